@@ -1,0 +1,483 @@
+"""Benchmark: chi0 + Sigma_c on one B200 (GFLOP/s), plain FP64 vs split FP16.
+
+One step = the hot path over one batch of synthetic input:
+  * chi0(q, iw) of the GaAs-like configuration (N=600, nk=216, nocc=9,
+    nunocc U{100..300} per k, 24 imaginary frequencies), all k and all iw in
+    one call (qsgw_chi0_lorentz_d), and
+  * the Sigma_c band sum of 64 tasks (one per q of W_c), each N=600,
+    40 target x 400 intermediate states, 24 iw + w=0 and the real-axis pole
+    part on a 50-point mesh (qsgw_sxcf_correlation_d per task).
+Inputs are seeded synthetic data with the configurations' shapes and value
+distributions; W_c(q, iw) is built by this library's own chi0 -> W path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|split]
+    python bench.py --impl reference ...   # the reference's CPU path (oracle)
+
+N > 1 runs N independent replicas (the path needs no collective; the
+reference's q/k partitions are independent), timed as the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err <=1 meV"
+
+
+# ----------------------------------------------------------------------------- helpers
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------------------- workload
+def chi0_config():
+    from ecalj_b200 import synth
+    c = synth.CONFIGS["c1"]
+    rng = np.random.default_rng(c["seed"])
+    nocc, nun, eocc, eun = synth.chi0_spectrum(rng, c["nk"], c["nocc"], c["nun"])
+    mesh = synth.imag_mesh(c["niw"])
+    npair = int(np.sum(nocc * nun))
+    return dict(N=c["N"], nk=c["nk"], niw=c["niw"], nocc=nocc, nun=nun,
+                eocc_h=np.concatenate(eocc) * 0.5, eun_h=np.concatenate(eun) * 0.5,
+                npair=npair, seed=c["seed"], **mesh)
+
+
+def sigc_config():
+    from ecalj_b200 import synth
+    return dict(synth.CONFIGS["c2"])
+
+
+def device_normal_c128(n, seed, scale):
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    t = torch.empty(2 * n, dtype=torch.float64, device="cuda")
+    t.normal_(0.0, scale, generator=g)
+    return t.view(torch.complex128)
+
+
+def build_sigc_inputs(lib, c, log):
+    """W_c(q, iw) for every q from this library's chi0 -> W path (c0-style
+    pair model at N=600, iw = 0 plus the 24 Gauss-Legendre points), a real-axis
+    model on the 50-point mesh, and zmel per task.  All device-resident."""
+    import torch
+    from ecalj_b200 import synth
+    from ecalj_b200 import sched
+    N, niw, ntq, nm = c["N"], c["niw"], c["ntq"], c["nm"]
+    mesh = synth.imag_mesh(niw)
+    fr = synth.freq_r_mesh(c["nreal"])
+    freqs = np.concatenate([[0.0], mesh["freq_i"]])            # slot 0 = w = 0
+    nf = niw + 1
+    vsq, q = synth.coulomb(N, c["seed"] + 1)
+    m2e = lib.to_device(q)
+    tasks = []
+    t0 = time.time()
+    for iq in range(c["nq"]):
+        rng = np.random.default_rng(c["seed"] * 1000 + iq)
+        nocc_a, nun_a, eocc, eun = synth.chi0_spectrum(rng, c["chi_nk"], c["chi_nocc"], c["chi_nun"])
+        npair = int(np.sum(nocc_a * nun_a))
+        z = device_normal_c128(N * npair, c["seed"] * 7919 + iq, 1.0 / math.sqrt(N))
+        chi = torch.zeros(N * N * nf, dtype=torch.complex128, device="cuda")
+        lib.chi0_lorentz_d(chi, N, nf, freqs, c["chi_nk"], nocc_a, nun_a,
+                           np.concatenate(eocc) * 0.5, np.concatenate(eun) * 0.5, z)
+        del z
+        wi = torch.zeros(N * N * nf, dtype=torch.complex128, device="cuda")
+        lib.wvi_llw(chi, 2, vsq, m2e, True, True, 2, zw=wi, device=True, ngb=N, niw=nf)
+        del chi
+        g = torch.tensor(1.0 / (1.0 + (fr / 0.5) ** 2), dtype=torch.float64, device="cuda")
+        wr = (wi[:N * N].view(1, N * N) * g.view(-1, 1)).reshape(-1).contiguous()
+        trng = np.random.default_rng(c["seed"] * 31 + iq)
+        omega = np.sort(trng.uniform(-1.0, 1.0, ntq))
+        ekc = np.sort(trng.uniform(-1.0, 4.0, nm))
+        zmel = device_normal_c128(N * nm * ntq, c["seed"] * 104729 + iq, 1.0 / math.sqrt(N))
+        ef, esmr = 0.0, 0.01
+        nwxi, nwx, ntmax = sched.get_nwx(omega, ekc, fr, ef, esmr)
+        ns2r = min(nm, ntmax)
+        tasks.append(dict(wi=wi, wr=wr, zmel=zmel, omega=omega, ekc=ekc, ef=ef, esmr=esmr,
+                          nwxi=nwxi, nwx=nwx, ns2r=ns2r))
+    lib.synchronize()
+    log(f"sigc inputs: {c['nq']} W stacks built on the GPU in {time.time() - t0:.1f}s")
+    return dict(tasks=tasks, mesh=mesh, fr=fr, N=N, niw=niw, ntq=ntq, nm=nm, wkkr=1.0 / c["nq"])
+
+
+def sigc_flops(lib, s):
+    """Algorithmic FLOPs of the Sigma_c step, counted as the reference's GEMMs
+    execute them: 8 N^2 (nm ntq) per iw (0..niw), 8 N^2 per pole column and
+    real bin, 8 ntq^2 N nm for the final contraction."""
+    from ecalj_b200 import sched
+    N, nm, ntq, niw = s["N"], s["nm"], s["ntq"], s["niw"]
+    f_imag = 8.0 * N * N * nm * ntq * (niw + 1)
+    f_fin = 8.0 * ntq * ntq * N * nm
+    tot_pole = 0.0
+    for t in s["tasks"]:
+        ent, _ = sched.pole_bins(t["omega"], t["ekc"], s["fr"], t["ef"], t["esmr"], t["nwxi"], t["nwx"],
+                                 t["ns2r"], nm, ntq)
+        nb = sum(1 for _, x in ent for j in range(3) if t["nwxi"] <= x - 1 + j <= t["nwx"])
+        tot_pole += 8.0 * N * N * nb
+    return len(s["tasks"]) * (f_imag + f_fin) + tot_pole, len(s["tasks"]) * f_imag + tot_pole
+
+
+def run_sigc(lib, s, host=None):
+    m = s["mesh"]
+    for i, t in enumerate(s["tasks"]):
+        src = host["tasks"][i] if host else t
+        lib.sxcf_correlation(src["zsec"], src["zmel"], 1, s["nm"], t["ns2r"], t["nwxi"], t["nwx"], s["ntq"],
+                             src["wi"], src["wr"], t["omega"], t["ekc"], 0, t["ef"], t["esmr"], s["wkkr"],
+                             m["ua"], m["x"], m["wx"], m["expa"], s["fr"], nblochpmx=s["N"],
+                             device=host is None, ngb=s["N"], ntq=s["ntq"])
+
+
+# ----------------------------------------------------------------------------- reference arm
+def reference_arm(args, ws, rank):
+    """The reference's CPU path (the oracle restatement on numpy/OpenBLAS with
+    every host thread) on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    from threadpoolctl import threadpool_info
+    from oracle import sxcf as osx
+    from ecalj_b200 import synth
+    c1 = chi0_config()
+    N, niw = c1["N"], c1["niw"]
+    rng = np.random.default_rng(1)
+    P_s = 3000
+    z = synth.zmel_columns(rng, N, P_s)
+    de = rng.uniform(0.025, 2.0, P_s)
+    w = -2.0 * de[:, None] / (de[:, None] ** 2 + c1["freq_i"][None, :] ** 2) / c1["nk"]
+    c2 = sigc_config()
+    nm_s = 100
+    t = synth.sigc_task(c2["N"], c2["ntq"], nm_s, c2["niw"], c2["nreal"], seed=5, esmr=0.01, ef=0.0)
+    wi = synth.zmel_columns(rng, N, N * (c2["niw"] + 1)).reshape(N, N, c2["niw"] + 1, order="F") * 0.01
+    wr = synth.real_axis_model(wi[:, :, 0], t["freq_r"])
+    nt0p, nt0m = osx.nt0pm(t["ekc"], t["ef"], t["esmr"])
+    nwxi, nwx, ntmax = osx.get_nwx(t["omega"], c2["ntq"], nt0p, nt0m, nm_s, t["freq_r"], t["esmr"], t["ef"],
+                                   t["ekc"], 0)
+    fl_chi = 8.0 * N * N * P_s * niw
+    npole = len(osx.pole_table(t["omega"], t["ekc"], 0, 1, min(nm_s, ntmax), c2["ntq"], t["ef"], t["esmr"],
+                               1.0, t["freq_r"]))
+    fl_sig = 8.0 * N * N * nm_s * c2["ntq"] * (c2["niw"] + 1) + 8.0 * N * N * 3 * npole \
+        + 8.0 * c2["ntq"] ** 2 * N * nm_s
+
+    def step():
+        acc = np.zeros((N, N), complex)
+        zh = z.conj().T.copy()
+        for iw in range(niw):                       # x0gemm: one ZGEMM per bin
+            acc += zh.T @ (z.T * w[:, iw:iw + 1])
+        zs = np.zeros((c2["ntq"], c2["ntq"]), complex, order="F")
+        osx.correlation_block(zs, t["zmel"], 1, nm_s, min(nm_s, ntmax), nwxi, nwx, c2["ntq"], wi, wr, t["omega"],
+                              t["ekc"], 0, t["ef"], t["esmr"], 1.0, t["ua"], t["x"], t["wx"], t["expa"], t["freq_r"])
+        return acc, zs
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    gf = (fl_chi + fl_sig) / dt / 1e9
+    threads = max([d.get("num_threads", 1) for d in threadpool_info()] + [1])
+    sample = (f"chi0 {P_s} of {c1['npair']} pairs x {niw} iw at N={N}; Sigma_c 1 task with {nm_s} of "
+              f"{c2['nm']} intermediate states x {c2['ntq']} targets, {c2['niw']}+1 iw, {npole} pole columns")
+    cpu = {"value": round(gf, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port", "sample": sample}
+    line = {"metric": METRIC, "value": round(gf, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "c1 chi0 + c2 Sigma_c (bounded CPU sample)", "sample": sample},
+            "impl": "reference", "cpu_baseline": cpu,
+            "e2e": {"value": round(gf, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nq", type=int, default=None, help="Sigma_c tasks (default: the configuration's 64)")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    log = (lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
+    if args.impl == "reference":
+        reference_arm(args, ws, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from ecalj_b200 import lib
+    lib.load()
+    lib.init(local)
+    lib.set_stream(torch.cuda.current_stream().cuda_stream)
+    prec = args.precision
+    if prec == "auto":
+        prec = "fp64"
+    lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
+    peaks, peak_src = load_peaks()
+
+    # ---- workload set-up (untimed)
+    c1 = chi0_config()
+    N, niw = c1["N"], c1["niw"]
+    zc = device_normal_c128(N * c1["npair"], c1["seed"], 1.0 / math.sqrt(N))
+    chi = torch.zeros(N * N * niw, dtype=torch.complex128, device="cuda")
+    c2 = sigc_config()
+    if args.nq:
+        c2["nq"] = args.nq
+    s = build_sigc_inputs(lib, c2, log)
+    for t in s["tasks"]:
+        t["zsec"] = torch.zeros(s["ntq"] * s["ntq"], dtype=torch.complex128, device="cuda")
+    fl_chi = 8.0 * N * N * c1["npair"] * niw
+    fl_sig, fl_sig_seg = sigc_flops(lib, s)
+    flops = fl_chi + fl_sig
+
+    def step():
+        lib.chi0_lorentz_d(chi, N, niw, c1["freq_i"], c1["nk"], c1["nocc"], c1["nun"], c1["eocc_h"],
+                           c1["eun_h"], zc)
+        run_sigc(lib, s)
+
+    # ---- warm-up, then K timed steps bracketed by barrier + synchronize
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    lib.profile(True)
+    l0 = lib.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = lib.launch_count() - l0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    kt = {tag: lib.profile_get(tag) for tag in ("chi0_dmma", "sigc_seg_dmma", "gemm_dmma", "chi0_tc",
+                                               "sigc_seg_tc")}
+    lib.profile(False)
+    clocks = sampler.stop()
+    if ws > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    value = ws * flops / (ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel
+    if prec == "split":
+        dom_tag, dom_flops = "sigc_seg_tc", fl_sig_seg
+    else:
+        dom_tag, dom_flops = "sigc_seg_dmma", fl_sig_seg
+    k_ms, k_n = kt[dom_tag]
+    per_launch_ms = k_ms / max(k_n, 1)
+    achieved = (dom_flops * args.steps / max(k_n, 1)) / (per_launch_ms * 1e-3) / 1e12 if k_n else None
+    fp64_peak = measure_fp64_peak()
+    if prec == "split":
+        peak = peaks["bf16_tflops_sustained"] / 3.0
+        peak_note = (f"{peak_src} bf16 sustained {peaks['bf16_tflops_sustained']} TFLOP/s / 3 "
+                     f"(3 FP16 slice products per FP64-equivalent product)")
+    else:
+        peak = fp64_peak
+        peak_note = "cuBLAS ZGEMM (complex128, 4096^3) measured in this run; MEASURED_PEAKS.json has no FP64 figure"
+    roof = {"bound": "tensor", "achieved": round(achieved, 3) if achieved else None, "peak": round(peak, 3),
+            "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if achieved else None, "traffic": None,
+            "kernel": dom_tag, "launch_ms": round(per_launch_ms, 4), "peak_source": peak_note,
+            "algorithmic_flops_per_launch": dom_flops * args.steps / max(k_n, 1)}
+
+    # ---- end-to-end through the host-pointer entry points (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline()
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "c128" if prec == "fp64" else "c128 via split-f16",
+                "data": "synthetic",
+                "config": {"workload": "c1 chi0 (N=600, nk=216, nocc=9, nunocc U{100..300}, 24 iw, "
+                                       f"{c1['npair']} pairs) + c2 Sigma_c ({len(s['tasks'])} tasks, N=600, "
+                                       "40x400 states, 24+1 iw, 50-point real mesh)",
+                           "precision": prec, "parallelism": f"replicas x{ws}",
+                           "l2": "inputs exceed L2 (zmel columns 3.73 GB)",
+                           "flops_per_step": flops, "flops_chi0": fl_chi, "flops_sigc": fl_sig},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks, "kernel_ms": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]},
+                "fp64_peak_tflops": round(fp64_peak, 3)}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def measure_fp64_peak():
+    """cuBLAS complex128 GEMM throughput (8 n^3 flops), best of 3 -- the FP64
+    tensor-pipe denominator (a measurement only)."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.complex128, device="cuda")
+    b = torch.randn(n, n, dtype=torch.complex128, device="cuda")
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); torch.matmul(a, b); e1.record(); torch.cuda.synchronize()
+        best = max(best, 8.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist):
+    """Same step through the host-pointer C-ABI entry points: every step copies
+    its inputs from pinned host memory and reads the results back."""
+    N, niw = c1["N"], c1["niw"]
+    zc_h = torch.empty(zc.numel(), dtype=torch.complex128, pin_memory=True)
+    zc_h.copy_(zc)
+    chi_h = torch.empty(N * N * niw, dtype=torch.complex128, pin_memory=True)
+    host = {"tasks": []}
+    h2d = zc_h.numel() * 16
+    for t in s["tasks"]:
+        d = {}
+        for k in ("zmel", "wi", "wr"):
+            d[k] = torch.empty(t[k].numel(), dtype=torch.complex128, pin_memory=True)
+            d[k].copy_(t[k])
+        d["zsec"] = torch.zeros(s["ntq"] * s["ntq"], dtype=torch.complex128, pin_memory=True)
+        for k in ("zmel", "wi", "wr", "zsec"):
+            d[k] = d[k].numpy().reshape(-1)
+        d["zmel"] = d["zmel"].reshape((s["N"], s["nm"], s["ntq"]), order="F")
+        d["wi"] = d["wi"].reshape((s["N"], s["N"], s["niw"] + 1), order="F")
+        d["wr"] = d["wr"].reshape((s["N"], s["N"], len(s["fr"])), order="F")
+        d["zsec"] = d["zsec"].reshape((s["ntq"], s["ntq"]), order="F")
+        host["tasks"].append(d)
+        h2d += (t["zmel"].numel() + t["wi"].numel()) * 16 + 16 * s["ntq"] ** 2
+        h2d += 16 * N * N * n_real_records(t, s)
+    d2h = chi_h.numel() * 16 + len(s["tasks"]) * 16 * s["ntq"] ** 2
+    zc_np = zc_h.numpy()
+    chi_np = chi_h.numpy()
+
+    def step():
+        lib.chi0_lorentz_d(chi_np, N, niw, c1["freq_i"], c1["nk"], c1["nocc"], c1["nun"], c1["eocc_h"],
+                           c1["eun_h"], zc_np, host=True)
+        run_sigc(lib, s, host=host)
+
+    step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    nst = max(1, min(args.steps, 2))
+    for _ in range(nst):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / nst
+    if ws > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    del host
+    return {"value": round(ws * flops / (ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(ms, 3),
+            "steps": nst, "api": "qsgw_chi0_lorentz + qsgw_sxcf_correlation (host pointers)"}
+
+
+def n_real_records(t, s):
+    from ecalj_b200 import sched
+    return len(sched.pole_bins(t["omega"], t["ekc"], s["fr"], t["ef"], t["esmr"], t["nwxi"], t["nwx"],
+                               t["ns2r"], s["nm"], s["ntq"])[1])
+
+
+def cpu_baseline():
+    """The oracle (numpy/OpenBLAS, all host threads) on a bounded sample,
+    run in a child process so its threads do not share this process."""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1"], capture_output=True, text=True, env={**os.environ, "WORLD_SIZE": "1",
+                                                                              "RANK": "0"})
+    for ln in r.stdout.splitlines():
+        if ln.startswith("{"):
+            return json.loads(ln)["cpu_baseline"]
+    return {"value": None, "unit": "GFLOP/s", "cores": None, "kind": "port", "sample": r.stderr[-300:]}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,376 @@
+// chi0 rank-k accumulation.
+//   qsgw_x0gemm / qsgw_x0gemm_d : drop-in for x0gemm (x0gemm.f90:2-97).
+//   qsgw_chi0_lorentz_d          : every k and every iw in one launch, with
+//                                  the Lorentzian pair weights built on the
+//                                  GPU in FP64.
+// The host builds the (jpm, iw) bin lists in the reference's icoun order
+// (x0gemm.f90:37-64); the GPU never materialises zw / wzw: the pair gather
+// and the weight are folded into the operand loads of the DMMA engine.
+#include <vector>
+#include "zgemm_f64.cuh"
+#include "split_f16.cuh"
+
+namespace qsgw {
+
+static DevBuf g_x0_idx, g_x0_w, g_x0_bins, g_x0_zm, g_x0_rc;
+
+struct BinTables {
+  std::vector<int> colidx;
+  std::vector<double> wts;
+  std::vector<int> cnt, slab;
+  std::vector<long long> off;
+  int maxcnt = 0;
+};
+
+// Returns the number of chunks of the longest bin.
+static int upload_bins(const BinTables& bt, ZParams& p, cudaStream_t s, int& rc) {
+  const size_t nb = bt.cnt.size();
+  const size_t ni = bt.colidx.size();
+  rc = g_x0_idx.ensure(std::max<size_t>(ni, 1) * sizeof(int));
+  if (rc) return 0;
+  rc = g_x0_w.ensure(std::max<size_t>(ni, 1) * sizeof(double));
+  if (rc) return 0;
+  const size_t bin_bytes = nb * (2 * sizeof(int) + sizeof(long long));
+  rc = g_x0_bins.ensure(std::max<size_t>(bin_bytes, 64));
+  if (rc) return 0;
+  std::vector<unsigned char> hb(bin_bytes);
+  memcpy(hb.data(), bt.off.data(), nb * sizeof(long long));
+  memcpy(hb.data() + nb * sizeof(long long), bt.cnt.data(), nb * sizeof(int));
+  memcpy(hb.data() + nb * (sizeof(long long) + sizeof(int)), bt.slab.data(), nb * sizeof(int));
+  if (ni) {
+    rc = check_cuda(cudaMemcpyAsync(g_x0_idx.p, bt.colidx.data(), ni * sizeof(int), cudaMemcpyHostToDevice, s), "H2D pair columns");
+    if (rc) return 0;
+    rc = check_cuda(cudaMemcpyAsync(g_x0_w.p, bt.wts.data(), ni * sizeof(double), cudaMemcpyHostToDevice, s), "H2D pair weights");
+    if (rc) return 0;
+  }
+  rc = check_cuda(cudaMemcpyAsync(g_x0_bins.p, hb.data(), bin_bytes, cudaMemcpyHostToDevice, s), "H2D bins");
+  if (rc) return 0;
+  // the pageable copies above are staged before returning, hb may die now
+  unsigned char* base = g_x0_bins.as<unsigned char>();
+  p.bin_coff = reinterpret_cast<const long long*>(base);
+  p.bin_woff = reinterpret_cast<const long long*>(base);
+  p.bin_cnt = reinterpret_cast<const int*>(base + nb * sizeof(long long));
+  p.bin_slab = reinterpret_cast<const int*>(base + nb * (sizeof(long long) + sizeof(int)));
+  p.colidx = g_x0_idx.as<int>();
+  p.wts = g_x0_w.as<double>();
+  return (bt.maxcnt + ZG_BK - 1) / ZG_BK;
+}
+
+static int choose_splitk(int ntiles, int nbins, int maxch) {
+  const long long ctas = static_cast<long long>(ntiles) * nbins;
+  const long long slots = 2LL * ctx().sm_count;
+  if (ctas >= slots || maxch < 16) return 1;
+  int sk = static_cast<int>((slots + ctas - 1) / ctas);
+  return std::max(1, std::min(sk, maxch / 8));
+}
+
+static int x0gemm_device(double2* rcxq, int npr, int ipr_col, int npr_col, int nwhis, int npm,
+                         int ns1, int ns2, const double2* zmel, int nbb, int nm1, int nm2,
+                         int nqtot, int icounkmink, int icounkmaxk, const int* itc, const int* itpc,
+                         const int* jpmc, const int* iwini, const int* iwend, const int* icouini,
+                         const double* whwc, int ncount) {
+  cudaStream_t s = ctx().stream;
+  const int nmz = nm2 - nm1 + 1;
+  // ---- bin lists in icoun order (x0gemm.f90:37-64) ----
+  const int nbins_all = nwhis * npm;
+  std::vector<int> cnt(nbins_all, 0);
+  for (int icoun = icounkmink; icoun <= icounkmaxk; ++icoun) {
+    const int c = icoun - 1;
+    const int jpm = jpmc[c], it = itc[c], itp = itpc[c];
+    QSGW_ARG(jpm >= 1 && jpm <= npm, "x0gemm: jpmc(%d)=%d outside 1..npm", icoun, jpm);
+    if (it < ns1 || it > ns2) continue;
+    QSGW_ARG(it >= nm1 && it <= nm2, "x0gemm: itc(%d)=%d outside zmel bounds %d:%d", icoun, it, nm1, nm2);
+    QSGW_ARG(itp >= 1 && itp <= nqtot, "x0gemm: itpc(%d)=%d outside 1..nqtot", icoun, itp);
+    QSGW_ARG(iwini[c] >= 1 && iwend[c] <= nwhis, "x0gemm: bins %d..%d outside 1..nwhis", iwini[c], iwend[c]);
+    QSGW_ARG(icouini[c] >= 1 && icouini[c] + (iwend[c] - iwini[c]) <= ncount,
+             "x0gemm: icouini(%d)=%d outside whwc", icoun, icouini[c]);
+    for (int iw = iwini[c]; iw <= iwend[c]; ++iw) cnt[(jpm - 1) * nwhis + (iw - 1)]++;
+  }
+  BinTables bt;
+  std::vector<long long> start(nbins_all, 0);
+  long long tot = 0;
+  for (int jpm = 1; jpm <= npm; ++jpm)
+    for (int iw = 1; iw <= nwhis; ++iw) {
+      const int b = (jpm - 1) * nwhis + (iw - 1);
+      start[b] = tot;
+      if (cnt[b] > 0) {
+        bt.cnt.push_back(cnt[b]);
+        bt.off.push_back(tot);
+        bt.slab.push_back(iw * (3 - 2 * jpm) - (1 - npm) * nwhis);
+        bt.maxcnt = std::max(bt.maxcnt, cnt[b]);
+      }
+      tot += cnt[b];
+    }
+  if (bt.cnt.empty()) return QSGW_OK;
+  bt.colidx.resize(tot);
+  bt.wts.resize(tot);
+  std::vector<long long> fill(start);
+  for (int icoun = icounkmink; icoun <= icounkmaxk; ++icoun) {
+    const int c = icoun - 1;
+    const int jpm = jpmc[c], it = itc[c], itp = itpc[c];
+    if (it < ns1 || it > ns2) continue;
+    const int col = (it - nm1) + nmz * (itp - 1);
+    for (int iw = iwini[c]; iw <= iwend[c]; ++iw) {
+      const int b = (jpm - 1) * nwhis + (iw - 1);
+      bt.colidx[fill[b]] = col;
+      bt.wts[fill[b]] = whwc[iw - iwini[c] + icouini[c] - 1];   // x0gemm.f90:62
+      fill[b]++;
+    }
+  }
+  ZParams p{};
+  p.M = npr; p.N = npr_col;
+  p.A = zmel; p.a_rs = 1; p.a_ks = nbb; p.a_conj = 1;               // zw^H   (:76, :88 opA=C)
+  p.B = zmel + (ipr_col - 1); p.b_rs = 1; p.b_ks = nbb; p.b_conj = 0;  // wzw   (:84)
+  p.C = rcxq; p.ldc = npr; p.c_bs = static_cast<long long>(npr) * npr_col;
+  p.ntm = (npr + ZG_BM - 1) / ZG_BM; p.ntn = (npr_col + ZG_BN - 1) / ZG_BN;
+  int rc = 0;
+  const int maxch = upload_bins(bt, p, s, rc);
+  if (rc) return rc;
+  const int herm = (ipr_col == 1 && npr_col == npr) ? 1 : 0;
+  const int ntiles = herm ? p.ntm * (p.ntm + 1) / 2 : p.ntm * p.ntn;
+  const int nbins = static_cast<int>(bt.cnt.size());
+  const int sk = choose_splitk(ntiles, nbins, maxch);
+  p.kch_per_split = (maxch + sk - 1) / sk;
+  rc = zgemm_chi0_launch(p, nbins, herm, sk, s);
+  if (rc) return rc;
+  // host vectors must outlive the async copies from pageable memory: they do,
+  // because pageable cudaMemcpyAsync stages the data before returning.
+  return QSGW_OK;
+}
+
+static int x0gemm_check(int npr, int ipr_col, int npr_col, int nwhis, int npm, int nbb, int nm1,
+                        int nm2, int nqtot, int icounkmink, int icounkmaxk, int ncount,
+                        const void* rcxq, const void* zmel) {
+  QSGW_ARG(npr >= 1 && npr_col >= 1 && ipr_col >= 1, "x0gemm: bad npr=%d npr_col=%d ipr_col=%d", npr, npr_col, ipr_col);
+  QSGW_ARG(npr <= nbb && ipr_col - 1 + npr_col <= nbb, "x0gemm: product-basis range exceeds nbb=%d", nbb);
+  QSGW_ARG(npm == 1 || npm == 2, "x0gemm: npm=%d", npm);
+  QSGW_ARG(nwhis >= 1, "x0gemm: nwhis=%d", nwhis);
+  QSGW_ARG(nm2 >= nm1 && nqtot >= 1, "x0gemm: zmel bounds %d:%d nqtot=%d", nm1, nm2, nqtot);
+  QSGW_ARG(icounkmink >= 1 && icounkmaxk >= icounkmink - 1, "x0gemm: icoun range %d..%d", icounkmink, icounkmaxk);
+  QSGW_ARG(ncount >= 0, "x0gemm: ncount=%d", ncount);
+  QSGW_ARG(rcxq && zmel, "x0gemm: null array");
+  QSGW_ARG((reinterpret_cast<uintptr_t>(rcxq) & 15) == 0 && (reinterpret_cast<uintptr_t>(zmel) & 15) == 0,
+           "x0gemm: complex arrays must be 16-byte aligned");
+  return QSGW_OK;
+}
+
+}  // namespace qsgw
+
+using namespace qsgw;
+
+extern "C" int qsgw_x0gemm_d(double* rcxq_d, int npr, int ipr_col, int npr_col, int nwhis, int npm,
+                             int ns1, int ns2, const double* zmel_d, int nbb, int nm1, int nm2,
+                             int nqtot, int icounkmink, int icounkmaxk, const int* itc,
+                             const int* itpc, const int* jpmc, const int* iwini, const int* iwend,
+                             const int* icouini, const double* whwc, int ncount) {
+  int rc = require_init();
+  if (rc) return rc;
+  rc = x0gemm_check(npr, ipr_col, npr_col, nwhis, npm, nbb, nm1, nm2, nqtot, icounkmink, icounkmaxk,
+                    ncount, rcxq_d, zmel_d);
+  if (rc) return rc;
+  if (icounkmaxk < icounkmink) return QSGW_OK;
+  QSGW_ARG(itc && itpc && jpmc && iwini && iwend && icouini && whwc, "x0gemm: null index table");
+  return x0gemm_device(reinterpret_cast<double2*>(rcxq_d), npr, ipr_col, npr_col, nwhis, npm, ns1,
+                       ns2, reinterpret_cast<const double2*>(zmel_d), nbb, nm1, nm2, nqtot,
+                       icounkmink, icounkmaxk, itc, itpc, jpmc, iwini, iwend, icouini, whwc, ncount);
+}
+
+extern "C" int qsgw_x0gemm(double* rcxq, int npr, int ipr_col, int npr_col, int nwhis, int npm,
+                           int ns1, int ns2, const double* zmel, int nbb, int nm1, int nm2,
+                           int nqtot, int icounkmink, int icounkmaxk, const int* itc,
+                           const int* itpc, const int* jpmc, const int* iwini, const int* iwend,
+                           const int* icouini, const double* whwc, int ncount) {
+  int rc = require_init();
+  if (rc) return rc;
+  rc = x0gemm_check(npr, ipr_col, npr_col, nwhis, npm, nbb, nm1, nm2, nqtot, icounkmink, icounkmaxk,
+                    ncount, rcxq, zmel);
+  if (rc) return rc;
+  if (icounkmaxk < icounkmink) return QSGW_OK;
+  cudaStream_t s = ctx().stream;
+  const size_t nslab = static_cast<size_t>(npm == 1 ? nwhis + 1 : 2 * nwhis + 1);
+  const size_t rc_bytes = static_cast<size_t>(npr) * npr_col * nslab * 16;
+  const size_t zm_bytes = static_cast<size_t>(nbb) * (nm2 - nm1 + 1) * nqtot * 16;
+  rc = g_x0_rc.ensure(rc_bytes); if (rc) return rc;
+  rc = g_x0_zm.ensure(zm_bytes); if (rc) return rc;
+  QSGW_CUDA(cudaMemcpyAsync(g_x0_rc.p, rcxq, rc_bytes, cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(g_x0_zm.p, zmel, zm_bytes, cudaMemcpyHostToDevice, s));
+  rc = qsgw_x0gemm_d(g_x0_rc.as<double>(), npr, ipr_col, npr_col, nwhis, npm, ns1, ns2,
+                     g_x0_zm.as<double>(), nbb, nm1, nm2, nqtot, icounkmink, icounkmaxk, itc, itpc,
+                     jpmc, iwini, iwend, icouini, whwc, ncount);
+  if (rc) return rc;
+  QSGW_CUDA(cudaMemcpyAsync(rcxq, g_x0_rc.p, rc_bytes, cudaMemcpyDeviceToHost, s));
+  QSGW_CUDA(cudaStreamSynchronize(s));
+  return QSGW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// All-k chi0 with Lorentzian weights built on the device.
+namespace qsgw {
+
+__global__ void lorentz_weight_kernel(double* __restrict__ w, const int* __restrict__ peo,
+                                      const int* __restrict__ peu, const double* __restrict__ eo,
+                                      const double* __restrict__ eu, const double* __restrict__ fi,
+                                      long long npair, int niw, double inv_nk) {
+  const long long total = npair * niw;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long pr = i % npair;
+    const int iw = static_cast<int>(i / npair);
+    const double de = eu[peu[pr]] - eo[peo[pr]];
+    const double om = fi[iw];
+    w[i] = -2.0 * de / (de * de + om * om) * inv_nk;   // chi0(iw) <= 0 (dpsion5.f90:218)
+  }
+}
+
+static DevBuf g_lz_map, g_lz_e, g_lz_w, g_lz_bins, g_lz_fi;
+
+int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc, const int* nun,
+                         const double* eocc, const double* eunocc, long long& npair, double*& w_d,
+                         cudaStream_t s) {
+  npair = 0;
+  long long no_tot = 0, nu_tot = 0;
+  for (int k = 0; k < nk; ++k) {
+    QSGW_ARG(nocc[k] >= 0 && nun[k] >= 0, "chi0: negative band count at k=%d", k);
+    npair += static_cast<long long>(nocc[k]) * nun[k];
+    no_tot += nocc[k];
+    nu_tot += nun[k];
+  }
+  std::vector<int> peo(npair), peu(npair);
+  long long c = 0, oo = 0, uo = 0;
+  for (int k = 0; k < nk; ++k) {
+    // column order of zcols: (it - 1) + nocc_k * (itp - 1), as zmel(:, it, itp)
+    for (int itp = 0; itp < nun[k]; ++itp)
+      for (int it = 0; it < nocc[k]; ++it) {
+        peo[c] = static_cast<int>(oo + it);
+        peu[c] = static_cast<int>(uo + itp);
+        ++c;
+      }
+    oo += nocc[k];
+    uo += nun[k];
+  }
+  int rc = g_lz_map.ensure(2 * std::max<long long>(npair, 1) * sizeof(int));
+  if (rc) return rc;
+  rc = g_lz_e.ensure((no_tot + nu_tot + 1) * sizeof(double));
+  if (rc) return rc;
+  rc = g_lz_w.ensure(std::max<long long>(npair, 1) * niw * sizeof(double));
+  if (rc) return rc;
+  rc = g_lz_fi.ensure(niw * sizeof(double));
+  if (rc) return rc;
+  int* dpeo = g_lz_map.as<int>();
+  int* dpeu = dpeo + npair;
+  double* deo = g_lz_e.as<double>();
+  double* deu = deo + no_tot;
+  QSGW_CUDA(cudaMemcpyAsync(dpeo, peo.data(), npair * sizeof(int), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(dpeu, peu.data(), npair * sizeof(int), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(deo, eocc, no_tot * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(deu, eunocc, nu_tot * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(g_lz_fi.p, freq_i, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  const long long tot = npair * niw;
+  const int blocks = static_cast<int>(std::min<long long>((tot + 255) / 256, 8LL * ctx().sm_count));
+  if (tot > 0) {
+    lorentz_weight_kernel<<<std::max(blocks, 1), 256, 0, s>>>(g_lz_w.as<double>(), dpeo, dpeu, deo, deu,
+                                                              g_lz_fi.as<double>(), npair, niw, 1.0 / nk);
+    count_launch();
+    QSGW_LAUNCH_CHECK("lorentz_weight_kernel");
+  }
+  w_d = g_lz_w.as<double>();
+  return QSGW_OK;
+}
+
+static DevBuf g_lz_ident;
+
+__global__ void iota_kernel(int* a, long long n) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x)
+    a[i] = static_cast<int>(i);
+}
+
+}  // namespace qsgw
+
+extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const double* freq_i, int nk,
+                                   const int* nocc, const int* nun, const double* eocc,
+                                   const double* eunocc, const double* zcols_d, int ldz) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(chi0_d && zcols_d && freq_i && nocc && nun && eocc && eunocc, "chi0_lorentz: null pointer");
+  QSGW_ARG(npr >= 1 && niw >= 1 && nk >= 1 && ldz >= npr, "chi0_lorentz: npr=%d niw=%d nk=%d ldz=%d", npr, niw, nk, ldz);
+  QSGW_ARG((reinterpret_cast<uintptr_t>(chi0_d) & 15) == 0 && (reinterpret_cast<uintptr_t>(zcols_d) & 15) == 0,
+           "chi0_lorentz: complex arrays must be 16-byte aligned");
+  cudaStream_t s = ctx().stream;
+  long long npair = 0;
+  double* w_d = nullptr;
+  rc = chi0_lorentz_weights(niw, freq_i, nk, nocc, nun, eocc, eunocc, npair, w_d, s);
+  if (rc) return rc;
+  QSGW_ARG(npair < (1LL << 31), "chi0_lorentz: %lld pairs exceed the 32-bit column index", npair);
+  const size_t cbytes = static_cast<size_t>(npr) * npr * niw * 16;
+  QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
+  if (npair == 0) return QSGW_OK;
+  if (ctx().prec_mode == QSGW_PREC_SPLIT_F16) {
+    return chi0_split_f16(reinterpret_cast<double2*>(chi0_d), npr, niw,
+                          reinterpret_cast<const double2*>(zcols_d), ldz, npair, w_d, s);
+  }
+  rc = g_lz_ident.ensure(npair * sizeof(int));
+  if (rc) return rc;
+  iota_kernel<<<static_cast<int>(std::min<long long>((npair + 255) / 256, 4096)), 256, 0, s>>>(
+      g_lz_ident.as<int>(), npair);
+  count_launch();
+  QSGW_LAUNCH_CHECK("iota_kernel");
+  // one bin per iw, all pairs in every bin, bin iw's weights at offset iw*npair
+  std::vector<long long> off(2 * niw);
+  std::vector<int> cs(2 * niw);
+  for (int iw = 0; iw < niw; ++iw) {
+    off[iw] = 0;                                  // column offsets (shared identity list)
+    off[niw + iw] = static_cast<long long>(iw) * npair;   // weight offsets
+    cs[iw] = static_cast<int>(npair);
+    cs[niw + iw] = iw;                            // slab
+  }
+  rc = g_lz_bins.ensure(2 * niw * (sizeof(long long) + sizeof(int)));
+  if (rc) return rc;
+  unsigned char* base = g_lz_bins.as<unsigned char>();
+  QSGW_CUDA(cudaMemcpyAsync(base, off.data(), 2 * niw * sizeof(long long), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(base + 2 * niw * sizeof(long long), cs.data(), 2 * niw * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  ZParams p{};
+  p.M = npr; p.N = npr;
+  p.A = reinterpret_cast<const double2*>(zcols_d); p.a_rs = 1; p.a_ks = ldz; p.a_conj = 1;
+  p.B = reinterpret_cast<const double2*>(zcols_d); p.b_rs = 1; p.b_ks = ldz; p.b_conj = 0;
+  p.C = reinterpret_cast<double2*>(chi0_d); p.ldc = npr; p.c_bs = static_cast<long long>(npr) * npr;
+  p.ntm = p.ntn = (npr + ZG_BM - 1) / ZG_BM;
+  p.bin_coff = reinterpret_cast<const long long*>(base);
+  p.bin_woff = reinterpret_cast<const long long*>(base) + niw;
+  p.bin_cnt = reinterpret_cast<const int*>(base + 2 * niw * sizeof(long long));
+  p.bin_slab = p.bin_cnt + niw;
+  p.colidx = g_lz_ident.as<int>();
+  p.wts = w_d;
+  const int maxch = static_cast<int>((npair + ZG_BK - 1) / ZG_BK);
+  const int ntiles = p.ntm * (p.ntm + 1) / 2;
+  const int sk = choose_splitk(ntiles, niw, maxch);
+  p.kch_per_split = (maxch + sk - 1) / sk;
+  return zgemm_chi0_launch(p, niw, 1, sk, s);
+}
+
+static qsgw::DevBuf g_lzh_z, g_lzh_c;
+
+extern "C" int qsgw_chi0_lorentz(double* chi0, int npr, int niw, const double* freq_i, int nk,
+                                 const int* nocc, const int* nun, const double* eocc,
+                                 const double* eunocc, const double* zcols, int ldz) {
+  using namespace qsgw;
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(chi0 && zcols && nocc && nun, "chi0_lorentz: null pointer");
+  QSGW_ARG(npr >= 1 && niw >= 1 && nk >= 1 && ldz >= npr, "chi0_lorentz: npr=%d niw=%d nk=%d ldz=%d", npr, niw, nk, ldz);
+  long long ncol = 0;
+  for (int k = 0; k < nk; ++k) ncol += static_cast<long long>(nocc[k]) * nun[k];
+  cudaStream_t s = ctx().stream;
+  const size_t zb = static_cast<size_t>(ldz) * ncol * 16;
+  const size_t cb = static_cast<size_t>(npr) * npr * niw * 16;
+  rc = g_lzh_z.ensure(zb); if (rc) return rc;
+  rc = g_lzh_c.ensure(cb); if (rc) return rc;
+  QSGW_CUDA(cudaMemcpyAsync(g_lzh_z.p, zcols, zb, cudaMemcpyHostToDevice, s));
+  rc = qsgw_chi0_lorentz_d(g_lzh_c.as<double>(), npr, niw, freq_i, nk, nocc, nun, eocc, eunocc,
+                           g_lzh_z.as<double>(), ldz);
+  if (rc) return rc;
+  QSGW_CUDA(cudaMemcpyAsync(chi0, g_lzh_c.p, cb, cudaMemcpyDeviceToHost, s));
+  QSGW_CUDA(cudaStreamSynchronize(s));
+  return QSGW_OK;
+}

@@ -1,0 +1,66 @@
+// Shared helpers for libqsgw_b200: error plumbing, the library context and
+// its device scratch buffers.  All entry points return 0 or a negative
+// qsgw_status code and never abort; qsgw_last_error() returns the text.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "qsgw_b200.h"
+
+namespace qsgw {
+
+struct Context {
+  bool initialized = false;
+  int device = -1;
+  cudaStream_t stream = nullptr;      // stream every entry point launches on
+  bool own_stream = false;
+  int prec_mode = QSGW_PREC_FP64;     // runtime precision switch
+  int nslices = 2;
+  int sm_count = 148;
+  int* d_flags = nullptr;             // device-side error/status words
+};
+
+Context& ctx();
+void set_error(const char* fmt, ...);
+int check_cuda(cudaError_t e, const char* what);
+
+// Grows-only device scratch buffer owned by the library.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t n);
+  void release();
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+int require_init();
+
+// Optional per-kernel timing with CUDA events on the launch stream
+// (qsgw_profile).  prof_begin returns -1 when profiling is off.
+int prof_begin(const char* tag, cudaStream_t s);
+void prof_end(int idx, cudaStream_t s);
+
+}  // namespace qsgw
+
+#define QSGW_CUDA(call)                                                   \
+  do {                                                                    \
+    int _rc = ::qsgw::check_cuda((call), #call);                          \
+    if (_rc != 0) return _rc;                                             \
+  } while (0)
+
+#define QSGW_LAUNCH_CHECK(what)                                           \
+  do {                                                                    \
+    int _rc = ::qsgw::check_cuda(cudaGetLastError(), what);               \
+    if (_rc != 0) return _rc;                                             \
+  } while (0)
+
+#define QSGW_ARG(cond, ...)                                               \
+  do {                                                                    \
+    if (!(cond)) {                                                        \
+      ::qsgw::set_error(__VA_ARGS__);                                     \
+      return QSGW_ERR_ARG;                                                \
+    }                                                                     \
+  } while (0)

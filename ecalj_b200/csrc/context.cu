@@ -1,0 +1,232 @@
+// Library context: device selection, launch stream, precision switch and
+// error text.  Replaces gpu_init (m_gpu.f90:14-68) and the cuBLAS/cuSOLVER
+// handle set-up/teardown (m_lapack.f90:230-255) of the reference.
+#include <cstdarg>
+#include <atomic>
+#include "common.cuh"
+
+namespace qsgw {
+
+static Context g_ctx;
+static char g_err[1024] = "";
+static std::atomic<long long> g_launches{0};
+
+Context& ctx() { return g_ctx; }
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+void count_launch(int n) { g_launches += n; }
+
+int check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return QSGW_OK;
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? QSGW_ERR_OOM : QSGW_ERR_CUDA;
+}
+
+int DevBuf::ensure(size_t n) {
+  if (n <= bytes && p) return QSGW_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  size_t want = n < 256 ? 256 : n;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    return check_cuda(e, "cudaMalloc(scratch)");
+  }
+  bytes = want;
+  return QSGW_OK;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+struct ProfRec {
+  std::string tag;
+  cudaEvent_t a, b;
+};
+static bool g_prof = false;
+static std::vector<ProfRec> g_prof_recs;
+static std::vector<cudaEvent_t> g_event_pool;
+
+static cudaEvent_t pool_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+static void prof_reset() {
+  for (auto& r : g_prof_recs) {
+    g_event_pool.push_back(r.a);
+    g_event_pool.push_back(r.b);
+  }
+  g_prof_recs.clear();
+}
+
+int prof_begin(const char* tag, cudaStream_t s) {
+  if (!g_prof) return -1;
+  ProfRec r{tag, pool_event(), pool_event()};
+  cudaEventRecord(r.a, s);
+  g_prof_recs.push_back(r);
+  return static_cast<int>(g_prof_recs.size()) - 1;
+}
+
+void prof_end(int idx, cudaStream_t s) {
+  if (idx < 0 || idx >= static_cast<int>(g_prof_recs.size())) return;
+  cudaEventRecord(g_prof_recs[idx].b, s);
+}
+
+int require_init() {
+  if (!g_ctx.initialized) {
+    set_error("qsgw_init has not been called");
+    return QSGW_ERR_NOTINIT;
+  }
+  cudaError_t e = cudaSetDevice(g_ctx.device);
+  return check_cuda(e, "cudaSetDevice");
+}
+
+}  // namespace qsgw
+
+using namespace qsgw;
+
+extern "C" int qsgw_init(int device) {
+  Context& c = ctx();
+  if (c.initialized) {
+    if (c.device == device) return QSGW_OK;
+    set_error("qsgw_init: already initialised on device %d", c.device);
+    return QSGW_ERR_ARG;
+  }
+  int ndev = 0;
+  QSGW_CUDA(cudaGetDeviceCount(&ndev));
+  QSGW_ARG(device >= 0 && device < ndev, "qsgw_init: device %d out of range (%d devices)", device, ndev);
+  QSGW_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  QSGW_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) {
+    set_error("qsgw_init: device %d is sm_%d%d; this library is built for sm_100a only",
+              device, prop.major, prop.minor);
+    return QSGW_ERR_UNSUPPORTED;
+  }
+  c.sm_count = prop.multiProcessorCount;
+  QSGW_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+  c.own_stream = true;
+  QSGW_CUDA(cudaMalloc(&c.d_flags, 64 * sizeof(int)));
+  QSGW_CUDA(cudaMemset(c.d_flags, 0, 64 * sizeof(int)));
+  c.device = device;
+  c.initialized = true;
+  g_launches = 0;
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_finalize(void) {
+  Context& c = ctx();
+  if (!c.initialized) return QSGW_OK;
+  cudaSetDevice(c.device);
+  cudaDeviceSynchronize();
+  if (c.d_flags) cudaFree(c.d_flags);
+  if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+  c = Context();
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_set_stream(void* stream) {
+  int rc = require_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  if (stream == nullptr) {
+    if (!c.own_stream) {
+      QSGW_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+      c.own_stream = true;
+    }
+    return QSGW_OK;
+  }
+  if (c.own_stream && c.stream) {
+    QSGW_CUDA(cudaStreamSynchronize(c.stream));
+    cudaStreamDestroy(c.stream);
+  }
+  c.stream = reinterpret_cast<cudaStream_t>(stream);
+  c.own_stream = false;
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_synchronize(void) {
+  int rc = require_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  QSGW_CUDA(cudaStreamSynchronize(c.stream));
+  int flag = 0;
+  QSGW_CUDA(cudaMemcpy(&flag, c.d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    QSGW_CUDA(cudaMemset(c.d_flags, 0, sizeof(int)));
+    set_error("a pivot block of the Hermitian inverse was singular or not finite");
+    return QSGW_ERR_NUMERIC;
+  }
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_set_precision(int mode, int nslices) {
+  QSGW_ARG(mode == QSGW_PREC_FP64 || mode == QSGW_PREC_SPLIT_F16,
+           "qsgw_set_precision: unknown mode %d", mode);
+  QSGW_ARG(mode == QSGW_PREC_FP64 || nslices == 2,
+           "qsgw_set_precision: SPLIT_F16 is built for 2 slices per operand (got %d)", nslices);
+  ctx().prec_mode = mode;
+  ctx().nslices = (mode == QSGW_PREC_FP64) ? 1 : nslices;
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_get_precision(int* mode, int* nslices) {
+  QSGW_ARG(mode && nslices, "qsgw_get_precision: null pointer");
+  *mode = ctx().prec_mode;
+  *nslices = ctx().nslices;
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_last_error(char* buf, int len) {
+  if (!buf || len <= 0) return QSGW_ERR_ARG;
+  strncpy(buf, g_err, static_cast<size_t>(len) - 1);
+  buf[len - 1] = '\0';
+  return QSGW_OK;
+}
+
+extern "C" long long qsgw_launch_count(void) { return g_launches.load(); }
+
+extern "C" int qsgw_profile(int enable) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_CUDA(cudaStreamSynchronize(ctx().stream));
+  prof_reset();
+  g_prof = enable != 0;
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_profile_get(const char* tag, double* ms, long long* launches) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(tag && ms && launches, "qsgw_profile_get: null pointer");
+  QSGW_CUDA(cudaStreamSynchronize(ctx().stream));
+  double tot = 0.0;
+  long long n = 0;
+  for (auto& r : g_prof_recs) {
+    if (r.tag != tag) continue;
+    float t = 0.f;
+    QSGW_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    tot += t;
+    ++n;
+  }
+  *ms = tot;
+  *launches = n;
+  return QSGW_OK;
+}

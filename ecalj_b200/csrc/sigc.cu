@@ -1,0 +1,464 @@
+// Correlation self-energy of one task: get_correlation_block of
+// sxcf_scz_correlation (m_sxcf_gemm.f90:407-612).
+//
+//   1. wgtim(0:niw, it, itp) on the GPU in FP64 (:432-458).
+//   2. Pole entries (it, itp) -> (ixs, wgt3) on the host, in the reference's
+//      loop order (:511-552, wfacx2/weavx2 of wfacx.f90:19-49).
+//   3. ONE launch of the segmented DMMA GEMM:
+//        czmelwc(:, c) = sum_{iw=0..niw} Wc_i(iw)^H (wgtim(iw, c) z_c)
+//                      + sum_{i=0..2}  Wsym(ixs_c-1+i)^H (wgt3_i(c) z_c)
+//      Columns are grouped by ixs so every 64-column tile shares one list of
+//      W matrices; every column is written once (no scatter races).
+//   4. zsec += czmelwc^H zmel (:599) with split-K, then Im zsec_ii <= 0 (:601-607).
+#include <cmath>
+#include <map>
+#include <vector>
+#include "zgemm_f64.cuh"
+#include "split_f16.cuh"
+
+namespace qsgw {
+
+static constexpr double kPi = 3.14159265358979323846264338327950288;
+
+__global__ void wgtim_kernel(double* __restrict__ wg, int niw, int ns1, int nm, int ntqxx, int nctot,
+                             const double* __restrict__ omega, const double* __restrict__ ekc,
+                             double esmr, double wkkr, double ua, const double* __restrict__ x,
+                             const double* __restrict__ wt, const double* __restrict__ expa) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nm * ntqxx) return;
+  const int itl = c % nm, itp = c / nm;
+  const int it = ns1 + itl;
+  const double pi = kPi;
+  const double we = 0.5 * (omega[itp] - ekc[it - 1]);
+  const double aw = fabs(ua * we), aw2 = aw * aw;
+  const double sig2 = 2.0 * (0.5 * esmr) * (0.5 * esmr);
+  const double sgn = signbit(we) ? -1.0 : 1.0;
+  double* out = wg + static_cast<long long>(c) * (niw + 1);
+  if (it <= nctot) {
+    double s0 = 0.0;
+    for (int i = 0; i < niw; ++i) {
+      const double cons = 1.0 / (we * we * x[i] * x[i] + (1.0 - x[i]) * (1.0 - x[i]));
+      const double w = we * cons * wt[i] * (-1.0 / pi);
+      out[1 + i] = wkkr * w;
+      s0 += w * expa[i];
+    }
+    double w0 = 0.0;
+    if (fabs(we) < 2.0 / ua) w0 = -s0 - 0.5 * sgn * exp(we * we * ua * ua) * erfc(ua * fabs(we));
+    out[0] = wkkr * w0;
+  } else {
+    double s0 = 0.0;
+    for (int i = 0; i < niw; ++i) {
+      const double omd = 1.0 / x[i] - 1.0;
+      const double omd2w = omd * omd + we * we;
+      const double r = omd2w / sig2;
+      double cons;
+      if (r > 5e-3) {
+        cons = (1.0 - exp(-r)) / omd2w;
+      } else {
+        cons = 1.0 / sig2 - omd2w / (sig2 * sig2) / 2.0 + omd2w * omd2w / (sig2 * sig2 * sig2) / 6.0 -
+               omd2w * omd2w * omd2w / (sig2 * sig2 * sig2 * sig2) / 24.0 +
+               omd2w * omd2w * omd2w * omd2w / (sig2 * sig2 * sig2 * sig2 * sig2) / 120.0 -
+               omd2w * omd2w * omd2w * omd2w * omd2w / (sig2 * sig2 * sig2 * sig2 * sig2 * sig2) / 720.0;
+      }
+      out[1 + i] = wkkr * (-we * cons * wt[i] / (x[i] * x[i]) / pi);
+      s0 += cons * expa[i] * wt[i] / (x[i] * x[i]);
+    }
+    const double w0 = we * s0 / pi + sgn * 0.5 * exp(aw2) * (erfc(sqrt(aw2 + we * we / sig2)) - erfc(aw));
+    out[0] = wkkr * w0;
+  }
+}
+
+// full Hermitian (ld = n) from a packed upper triangle, column order (j, i <= j) (:327-358, :468-474)
+__global__ void unpack_upper_kernel(double2* __restrict__ w, const double2* __restrict__ up, int n,
+                                    int nmat) {
+  const long long np = static_cast<long long>(n) * (n + 1) / 2;
+  const long long tot = static_cast<long long>(n) * n * nmat;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n);
+    const long long r = e / n;
+    const int j = static_cast<int>(r % n);
+    const long long m = r / n;
+    double2 v;
+    if (i <= j) {
+      v = up[m * np + static_cast<long long>(j) * (j + 1) / 2 + i];
+    } else {
+      const double2 u = up[m * np + static_cast<long long>(i) * (i + 1) / 2 + j];
+      v = make_double2(u.x, -u.y);
+    }
+    w[e] = v;
+  }
+}
+
+// (W + W^H)/2 of selected records (:573)
+__global__ void hermitize_kernel(double2* __restrict__ out, const double2* __restrict__ in,
+                                 const int* __restrict__ recs, int n, long long ld, int nrec) {
+  const long long tot = static_cast<long long>(n) * n * nrec;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n);
+    const long long r = e / n;
+    const int j = static_cast<int>(r % n);
+    const int q = static_cast<int>(r / n);
+    const double2* W = in + static_cast<long long>(recs[q]) * ld * ld;
+    const double2 a = W[i + j * ld], b = W[j + i * ld];
+    out[static_cast<long long>(q) * ld * ld + i + j * ld] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+  }
+}
+
+__global__ void clamp_diag_kernel(double2* zsec, int ntqxx, int ntq) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ntqxx) {
+    double2 v = zsec[i + static_cast<long long>(i) * ntq];
+    if (v.y > 0.0) v.y = 0.0;
+    zsec[i + static_cast<long long>(i) * ntq] = v;
+  }
+}
+
+// ---- host restatement of the pole weights (wfacx.f90:19-49, m_sxcf_gemm.f90:511-552)
+static double wfacx2_h(double e1, double e2, double ek, double esmr) {
+  const double el = std::min(e1, e2), eh = std::max(e1, e2);
+  if (eh - el < 1e-6) return 0.0;
+  if (esmr == 0.0) return (el <= ek && ek < eh) ? 1.0 : 0.0;
+  return 0.5 * std::erfc(-(eh - ek) / std::sqrt(2.0) / esmr) - 0.5 * std::erfc(-(el - ek) / std::sqrt(2.0) / esmr);
+}
+static double weavx2_h(double e1, double e2, double ek, double esmr) {
+  const double el = std::min(e1, e2), eh = std::max(e1, e2);
+  const double wtt = 0.5 * std::erfc(-(eh - ek) / std::sqrt(2.0) / esmr) -
+                     0.5 * std::erfc(-(el - ek) / std::sqrt(2.0) / esmr);
+  const double sig2 = 2.0 * esmr * esmr;
+  const double pi = 3.1415926535897932;
+  return ek + esmr / std::sqrt(2.0 * pi) * (-std::exp(-(eh - ek) * (eh - ek) / sig2) +
+                                            std::exp(-(el - ek) * (el - ek) / sig2)) / wtt;
+}
+static void inverse33_h(const double m[3][3], double inv[3][3]) {
+  // columns of the cofactor matrix (m_sxcf_gemm.f90:658-668), then transpose / det
+  double c[3][3];
+  auto cross = [](const double* a, const double* b, double* r) {
+    r[0] = a[1] * b[2] - a[2] * b[1];
+    r[1] = a[2] * b[0] - a[0] * b[2];
+    r[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  double col[3][3];
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) col[j][i] = m[i][j];
+  cross(col[1], col[2], c[0]);
+  cross(col[2], col[0], c[1]);
+  cross(col[0], col[1], c[2]);
+  const double det = col[0][0] * c[0][0] + col[0][1] * c[0][1] + col[0][2] * c[0][2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) inv[i][j] = c[i][j] / det;   // inv = transpose(cof) / det
+}
+
+struct PoleEntry { int col; int ixs; double w3[3]; };
+
+static int pole_table_h(const qsgw_sxcf_args& a, std::vector<PoleEntry>& out) {
+  const int nm = a.ns2 - a.ns1 + 1;
+  int nt0p = 0, nt0m = 0;
+  for (int i = 0; i < a.nekc; ++i) {
+    if (a.ekc[i] < a.ef + 10.0 * a.esmr) ++nt0p;
+    if (a.ekc[i] < a.ef - 10.0 * a.esmr) ++nt0m;
+  }
+  for (int itp = 1; itp <= a.ntqxx; ++itp) {
+    const double omg = a.omega[itp - 1];
+    const int itini = omg >= a.ef ? std::max(a.ns1, nt0m + 1) : a.ns1;
+    const int itend = omg >= a.ef ? a.ns2r : std::min(nt0p, a.ns2r);
+    for (int it = itini; it <= itend; ++it) {
+      double wf = wfacx2_h(omg, a.ef, a.ekc[it - 1], it <= a.nctot ? 0.0 : a.esmr);
+      if (wf < 1e-8) continue;
+      wf = wf * a.wkkr * (std::signbit(omg - a.ef) ? -1.0 : 1.0);
+      const double we = 0.5 * std::fabs(omg - weavx2_h(omg, a.ef, a.ekc[it - 1], a.esmr));
+      int ixs = 0;
+      for (int i = 1; i <= a.nw; ++i)
+        if (a.freq_r[i] > we) { ixs = i; break; }
+      if (ixs == 0 || ixs + 1 > a.nw) {
+        set_error("sxcf: pole frequency %g outside the real-axis mesh (freq_r(nw)=%g)", we, a.freq_r[a.nw]);
+        return QSGW_ERR_ARG;
+      }
+      double am[3][3], inv[3][3];
+      for (int r = 0; r < 3; ++r) {
+        const double xi = a.freq_r[ixs - 1 + r];
+        am[r][0] = 1.0; am[r][1] = xi * xi; am[r][2] = xi * xi * xi * xi;
+      }
+      inverse33_h(am, inv);
+      const double v[3] = {1.0, we * we, we * we * we * we};
+      PoleEntry e;
+      e.col = (it - a.ns1) + nm * (itp - 1);
+      e.ixs = ixs;
+      for (int j = 0; j < 3; ++j) e.w3[j] = wf * (v[0] * inv[0][j] + v[1] * inv[1][j] + v[2] * inv[2][j]);
+      out.push_back(e);
+    }
+  }
+  return QSGW_OK;
+}
+
+static DevBuf g_sc_wg, g_sc_w3, g_sc_cz, g_sc_wi, g_sc_wr, g_sc_tabs, g_sc_recs, g_sc_tmp;
+static DevBuf g_sc_host_z, g_sc_host_wi, g_sc_host_wr, g_sc_host_zs;
+
+static int grid_for(long long n) {
+  return static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 16LL * ctx().sm_count)));
+}
+
+static int sxcf_check(const qsgw_sxcf_args* a) {
+  QSGW_ARG(a, "sxcf: null args");
+  QSGW_ARG(a->ngb >= 1 && a->ntqxx >= 0 && a->ntq >= a->ntqxx && a->niw >= 1 && a->nw >= 2,
+           "sxcf: ngb=%d ntqxx=%d ntq=%d niw=%d nw=%d", a->ngb, a->ntqxx, a->ntq, a->niw, a->nw);
+  QSGW_ARG(a->keepwv || a->nblochpmx >= a->ngb, "sxcf: nblochpmx=%d < ngb", a->nblochpmx);
+  QSGW_ARG(a->ns1 >= 1 && a->ns2 <= a->nekc && a->ns2r <= a->ns2, "sxcf: middle states %d..%d (pole ..%d) vs nekc=%d",
+           a->ns1, a->ns2, a->ns2r, a->nekc);
+  QSGW_ARG(a->nwxi >= 0 && a->nwx <= a->nw, "sxcf: real window %d..%d, nw=%d", a->nwxi, a->nwx, a->nw);
+  QSGW_ARG(a->omega && a->ekc && a->freqx && a->wwx && a->expa && a->freq_r, "sxcf: null table");
+  QSGW_ARG(a->zmel && a->wc_imag && a->wc_real && a->zsec, "sxcf: null array");
+  QSGW_ARG(a->ua > 0.0 && a->esmr > 0.0, "sxcf: ua=%g esmr=%g must be positive", a->ua, a->esmr);
+  return QSGW_OK;
+}
+
+int sxcf_device(const qsgw_sxcf_args& a) {
+  cudaStream_t s = ctx().stream;
+  if (a.ns1 > a.ns2 || a.ntqxx == 0) return QSGW_OK;   // :418
+  const int ngb = a.ngb, niw = a.niw, nm = a.ns2 - a.ns1 + 1;
+  const long long ncol = static_cast<long long>(nm) * a.ntqxx;
+  const double2* zmel = reinterpret_cast<const double2*>(a.zmel);
+  // ---- 1. imaginary-axis weights on the GPU
+  int rc = g_sc_tabs.ensure((4 * niw + a.ntq + a.nekc + 8) * sizeof(double));
+  if (rc) return rc;
+  double* dt = g_sc_tabs.as<double>();
+  double *d_x = dt, *d_wt = dt + niw, *d_ex = dt + 2 * niw, *d_om = dt + 3 * niw, *d_ekc = d_om + a.ntq;
+  QSGW_CUDA(cudaMemcpyAsync(d_x, a.freqx, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_wt, a.wwx, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_ex, a.expa, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_om, a.omega, a.ntq * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_ekc, a.ekc, a.nekc * sizeof(double), cudaMemcpyHostToDevice, s));
+  rc = g_sc_wg.ensure(ncol * (niw + 1) * sizeof(double));
+  if (rc) return rc;
+  wgtim_kernel<<<static_cast<int>((ncol + 127) / 128), 128, 0, s>>>(
+      g_sc_wg.as<double>(), niw, a.ns1, nm, a.ntqxx, a.nctot, d_om, d_ekc, a.esmr, a.wkkr, a.ua, d_x, d_wt, d_ex);
+  count_launch();
+  QSGW_LAUNCH_CHECK("wgtim_kernel");
+  // ---- 2. pole entries (host)
+  std::vector<PoleEntry> poles;
+  rc = pole_table_h(a, poles);
+  if (rc) return rc;
+  // ---- W operands
+  const long long ldw = a.keepwv ? ngb : a.nblochpmx;
+  const long long wsz = ldw * ldw;
+  const double2* wi = reinterpret_cast<const double2*>(a.wc_imag);
+  const double2* wr_src = reinterpret_cast<const double2*>(a.wc_real);
+  if (a.keepwv) {
+    rc = g_sc_wi.ensure(wsz * (niw + 1) * sizeof(double2));
+    if (rc) return rc;
+    unpack_upper_kernel<<<grid_for(wsz * (niw + 1)), 256, 0, s>>>(g_sc_wi.as<double2>(), wi, ngb, niw + 1);
+    count_launch();
+    QSGW_LAUNCH_CHECK("unpack_upper_kernel");
+    wi = g_sc_wi.as<double2>();
+  }
+  // bins needed by the pole entries, restricted to [nwxi, nwx] (:557)
+  std::map<int, int> bin_slot;
+  for (const auto& e : poles)
+    for (int i = 0; i < 3; ++i) {
+      const int b = e.ixs - 1 + i;
+      if (b >= a.nwxi && b <= a.nwx && !bin_slot.count(b)) bin_slot.emplace(b, 0);
+    }
+  std::vector<int> recs;
+  for (auto& kv : bin_slot) { kv.second = static_cast<int>(recs.size()); recs.push_back(kv.first); }
+  const int nrec = static_cast<int>(recs.size());
+  const double2* wr = nullptr;
+  if (nrec > 0) {
+    rc = g_sc_wr.ensure(wsz * nrec * sizeof(double2));
+    if (rc) return rc;
+    rc = g_sc_recs.ensure(nrec * sizeof(int));
+    if (rc) return rc;
+    if (a.keepwv) {
+      // packed records are already (W+W^H)/2; unpack only the used ones
+      const long long np = static_cast<long long>(ngb) * (ngb + 1) / 2;
+      for (int q = 0; q < nrec; ++q) {
+        unpack_upper_kernel<<<grid_for(wsz), 256, 0, s>>>(g_sc_wr.as<double2>() + q * wsz, wr_src + recs[q] * np, ngb, 1);
+        count_launch();
+        QSGW_LAUNCH_CHECK("unpack_upper_kernel");
+      }
+    } else {
+      QSGW_CUDA(cudaMemcpyAsync(g_sc_recs.p, recs.data(), nrec * sizeof(int), cudaMemcpyHostToDevice, s));
+      hermitize_kernel<<<grid_for(static_cast<long long>(ngb) * ngb * nrec), 256, 0, s>>>(
+          g_sc_wr.as<double2>(), wr_src, g_sc_recs.as<int>(), ngb, ldw, nrec);
+      count_launch();
+      QSGW_LAUNCH_CHECK("hermitize_kernel");
+    }
+    wr = g_sc_wr.as<double2>();
+  }
+  // ---- groups: key ixs (0 = no pole); per-column wgt3
+  std::vector<double> w3(static_cast<size_t>(ncol) * 3, 0.0);
+  std::vector<int> key(ncol, 0);
+  for (const auto& e : poles) {
+    key[e.col] = e.ixs;
+    for (int i = 0; i < 3; ++i) w3[static_cast<size_t>(e.col) * 3 + i] = e.w3[i];
+  }
+  rc = g_sc_w3.ensure(w3.size() * sizeof(double));
+  if (rc) return rc;
+  QSGW_CUDA(cudaMemcpyAsync(g_sc_w3.p, w3.data(), w3.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  std::map<int, std::vector<int>> groups;
+  for (long long c = 0; c < ncol; ++c) groups[key[c]].push_back(static_cast<int>(c));
+  std::vector<ZSeg> segs;
+  std::vector<int> gseg_off, gnseg, tile_group, tile_cols;
+  int gidx = 0;
+  for (auto& kv : groups) {
+    gseg_off.push_back(static_cast<int>(segs.size()));
+    for (int sgi = 0; sgi <= niw; ++sgi) {
+      ZSeg z{wi + sgi * wsz, g_sc_wg.as<double>() + sgi, niw + 1, 0};
+      segs.push_back(z);
+    }
+    if (kv.first > 0) {
+      for (int i = 0; i < 3; ++i) {
+        const int b = kv.first - 1 + i;
+        auto it = bin_slot.find(b);
+        if (it == bin_slot.end()) continue;
+        ZSeg z{wr + it->second * wsz, g_sc_w3.as<double>() + i, 3, 0};
+        segs.push_back(z);
+      }
+    }
+    gnseg.push_back(static_cast<int>(segs.size()) - gseg_off.back());
+    const auto& cols = kv.second;
+    for (size_t t0 = 0; t0 < cols.size(); t0 += ZG_BN) {
+      tile_group.push_back(gidx);
+      for (int j = 0; j < ZG_BN; ++j)
+        tile_cols.push_back(t0 + j < cols.size() ? cols[t0 + j] : -1);
+    }
+    ++gidx;
+  }
+  const int ntiles = static_cast<int>(tile_group.size());
+  const size_t tb = segs.size() * sizeof(ZSeg) + (gseg_off.size() + gnseg.size() + tile_group.size() +
+                                                  tile_cols.size()) * sizeof(int);
+  rc = g_sc_tmp.ensure(tb + 16 * 5);
+  if (rc) return rc;
+  unsigned char* tbase = g_sc_tmp.as<unsigned char>();
+  size_t off = 0;
+  int cprc = 0;
+  auto put = [&](const void* src, size_t n) -> const void* {
+    void* dst = tbase + off;
+    if (!cprc) cprc = check_cuda(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s), "H2D sxcf tables");
+    off += (n + 15) & ~size_t(15);
+    return dst;
+  };
+  ZParams p{};
+  p.segs = reinterpret_cast<const ZSeg*>(put(segs.data(), segs.size() * sizeof(ZSeg)));
+  p.group_seg_off = reinterpret_cast<const int*>(put(gseg_off.data(), gseg_off.size() * sizeof(int)));
+  p.group_nseg = reinterpret_cast<const int*>(put(gnseg.data(), gnseg.size() * sizeof(int)));
+  p.tile_group = reinterpret_cast<const int*>(put(tile_group.data(), tile_group.size() * sizeof(int)));
+  p.tile_cols = reinterpret_cast<const int*>(put(tile_cols.data(), tile_cols.size() * sizeof(int)));
+  if (cprc) return cprc;
+  rc = g_sc_cz.ensure(static_cast<size_t>(ngb) * ncol * sizeof(double2));
+  if (rc) return rc;
+  double2* cz = g_sc_cz.as<double2>();
+  // ---- 3. imaginary axis + poles in one launch
+  p.M = ngb; p.K = ngb;
+  p.a_rs = ldw; p.a_ks = 1; p.a_conj = 1;             // Wc^H (:492 opA = m_op_C)
+  p.B = zmel; p.b_rs = ngb; p.b_ks = 1; p.b_conj = 0;
+  p.C = cz; p.ldc = ngb; p.beta_zero = 1;
+  if (ctx().prec_mode == QSGW_PREC_SPLIT_F16) rc = sigc_seg_split_f16(p, ntiles, s);
+  else rc = zgemm_seg_launch(p, ntiles, s);
+  if (rc) return rc;
+  // ---- 4. zsec += czmelwc^H zmel (:599) and the Im clamp (:601-607)
+  const long long kk = static_cast<long long>(ngb) * nm;
+  rc = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,
+                 make_double2(1, 0), reinterpret_cast<double2*>(a.zsec), a.ntq, 0, 1, s);
+  if (rc) return rc;
+  clamp_diag_kernel<<<(a.ntqxx + 127) / 128, 128, 0, s>>>(reinterpret_cast<double2*>(a.zsec), a.ntqxx, a.ntq);
+  count_launch();
+  QSGW_LAUNCH_CHECK("clamp_diag_kernel");
+  return QSGW_OK;
+}
+
+}  // namespace qsgw
+
+using namespace qsgw;
+
+extern "C" int qsgw_sxcf_correlation_d(const qsgw_sxcf_args* args) {
+  int rc = require_init();
+  if (rc) return rc;
+  rc = sxcf_check(args);
+  if (rc) return rc;
+  QSGW_ARG((reinterpret_cast<uintptr_t>(args->zmel) & 15) == 0 &&
+               (reinterpret_cast<uintptr_t>(args->wc_imag) & 15) == 0 &&
+               (reinterpret_cast<uintptr_t>(args->wc_real) & 15) == 0 &&
+               (reinterpret_cast<uintptr_t>(args->zsec) & 15) == 0,
+           "sxcf: complex arrays must be 16-byte aligned");
+  return sxcf_device(*args);
+}
+
+extern "C" int qsgw_sxcf_correlation(const qsgw_sxcf_args* args) {
+  int rc = require_init();
+  if (rc) return rc;
+  rc = sxcf_check(args);
+  if (rc) return rc;
+  const qsgw_sxcf_args& a = *args;
+  cudaStream_t s = ctx().stream;
+  const int nm = std::max(0, a.ns2 - a.ns1 + 1);
+  const size_t zb = static_cast<size_t>(a.ngb) * nm * a.ntqxx * 16;
+  const size_t wrec = a.keepwv ? static_cast<size_t>(a.ngb) * (a.ngb + 1) / 2 * 16
+                               : static_cast<size_t>(a.nblochpmx) * a.nblochpmx * 16;
+  const size_t wib = wrec * (a.niw + 1), wrb = wrec * (a.nw + 1);
+  const size_t sb = static_cast<size_t>(a.ntq) * a.ntq * 16;
+  rc = g_sc_host_z.ensure(zb); if (rc) return rc;
+  rc = g_sc_host_wi.ensure(wib); if (rc) return rc;
+  rc = g_sc_host_wr.ensure(wrb); if (rc) return rc;
+  rc = g_sc_host_zs.ensure(sb); if (rc) return rc;
+  if (zb) QSGW_CUDA(cudaMemcpyAsync(g_sc_host_z.p, a.zmel, zb, cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(g_sc_host_wi.p, a.wc_imag, wib, cudaMemcpyHostToDevice, s));
+  // only the real-axis records the pole part reads travel (as the reference
+  // reads __WVR records by index, m_sxcf_gemm.f90:570)
+  {
+    std::vector<PoleEntry> poles;
+    if (a.ns1 <= a.ns2 && a.ntqxx > 0) {
+      rc = pole_table_h(a, poles);
+      if (rc) return rc;
+    }
+    std::vector<char> need(a.nw + 1, 0);
+    for (const auto& e : poles)
+      for (int i = 0; i < 3; ++i) {
+        const int b = e.ixs - 1 + i;
+        if (b >= a.nwxi && b <= a.nwx) need[b] = 1;
+      }
+    for (int b = 0; b <= a.nw; ++b)
+      if (need[b])
+        QSGW_CUDA(cudaMemcpyAsync(g_sc_host_wr.as<char>() + b * wrec, reinterpret_cast<const char*>(a.wc_real) + b * wrec,
+                                  wrec, cudaMemcpyHostToDevice, s));
+  }
+  QSGW_CUDA(cudaMemcpyAsync(g_sc_host_zs.p, a.zsec, sb, cudaMemcpyHostToDevice, s));
+  qsgw_sxcf_args d = a;
+  d.zmel = g_sc_host_z.as<double>();
+  d.wc_imag = g_sc_host_wi.as<double>();
+  d.wc_real = g_sc_host_wr.as<double>();
+  d.zsec = g_sc_host_zs.as<double>();
+  rc = sxcf_device(d);
+  if (rc) return rc;
+  QSGW_CUDA(cudaMemcpyAsync(a.zsec, g_sc_host_zs.p, sb, cudaMemcpyDeviceToHost, s));
+  QSGW_CUDA(cudaStreamSynchronize(s));
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_sxcf_wgtim_d(double* wgtim_d, int niw, int ns1, int ns2, int ntqxx, int nctot,
+                                 const double* omega, const double* ekc, int nekc, double esmr,
+                                 double wkkr, double ua, const double* freqx, const double* wwx,
+                                 const double* expa) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(wgtim_d && omega && ekc && freqx && wwx && expa, "sxcf_wgtim: null pointer");
+  QSGW_ARG(niw >= 1 && ns1 >= 1 && ns2 >= ns1 && ns2 <= nekc && ntqxx >= 1, "sxcf_wgtim: bad sizes");
+  QSGW_ARG(esmr > 0.0 && ua > 0.0, "sxcf_wgtim: esmr and ua must be positive");
+  cudaStream_t s = ctx().stream;
+  const int nm = ns2 - ns1 + 1;
+  rc = g_sc_tabs.ensure((4 * niw + ntqxx + nekc + 8) * sizeof(double));
+  if (rc) return rc;
+  double* dt = g_sc_tabs.as<double>();
+  double *d_x = dt, *d_wt = dt + niw, *d_ex = dt + 2 * niw, *d_om = dt + 3 * niw, *d_ekc = d_om + ntqxx;
+  QSGW_CUDA(cudaMemcpyAsync(d_x, freqx, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_wt, wwx, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_ex, expa, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_om, omega, ntqxx * sizeof(double), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(d_ekc, ekc, nekc * sizeof(double), cudaMemcpyHostToDevice, s));
+  const long long ncol = static_cast<long long>(nm) * ntqxx;
+  wgtim_kernel<<<static_cast<int>((ncol + 127) / 128), 128, 0, s>>>(wgtim_d, niw, ns1, nm, ntqxx, nctot, d_om, d_ekc,
+                                                                    esmr, wkkr, ua, d_x, d_wt, d_ex);
+  count_launch();
+  QSGW_LAUNCH_CHECK("wgtim_kernel");
+  return QSGW_OK;
+}

@@ -1,0 +1,171 @@
+// Host side of the FP64 complex GEMM engine and the ZGEMM entry points that
+// replace the reference's BLAS shim zmm_h / zmm_d (m_blas.f90:198-228,
+// 469-498).
+#include "zgemm_f64.cuh"
+
+namespace qsgw {
+
+template <int MODE, bool A_RC, bool B_RC>
+static int launch_kernel(const ZParams& p, dim3 grid, cudaStream_t s) {
+  auto kern = zgemm_f64_kernel<MODE, A_RC, B_RC>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    QSGW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(sizeof(ZSmem))));
+    attr_done = true;
+  }
+  const char* tag = MODE == ZM_CHI0 ? "chi0_dmma" : (MODE == ZM_SEG ? "sigc_seg_dmma" : "gemm_dmma");
+  const int pi = prof_begin(tag, s);
+  kern<<<grid, ZG_THREADS, sizeof(ZSmem), s>>>(p);
+  prof_end(pi, s);
+  count_launch();
+  QSGW_LAUNCH_CHECK("zgemm_f64_kernel");
+  return QSGW_OK;
+}
+
+__global__ void zscale_kernel(double2* C, long long ldc, long long c_bs, int m, int n,
+                              double2 beta, int beta_zero) {
+  const long long b = blockIdx.y;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+       idx < static_cast<long long>(m) * n; idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long i = idx % m, j = idx / m;
+    double2* d = C + b * c_bs + i + j * ldc;
+    if (beta_zero) {
+      *d = make_double2(0.0, 0.0);
+    } else {
+      const double2 o = *d;
+      *d = make_double2(beta.x * o.x - beta.y * o.y, beta.x * o.y + beta.y * o.x);
+    }
+  }
+}
+
+int zgemm_f64(int opa, int opb, int m, int n, int k, double2 alpha,
+              const double2* A, long long lda, long long a_bs,
+              const double2* B, long long ldb, long long b_bs, double2 beta,
+              double2* C, long long ldc, long long c_bs, int nbatch, cudaStream_t s) {
+  if (m <= 0 || n <= 0 || nbatch <= 0) return QSGW_OK;
+  ZParams p{};
+  p.M = m; p.N = n; p.K = k;
+  p.A = A; p.a_bs = a_bs; p.a_conj = (opa == 2);
+  if (opa == 0) { p.a_rs = 1; p.a_ks = lda; } else { p.a_rs = lda; p.a_ks = 1; }
+  p.B = B; p.b_bs = b_bs; p.b_conj = (opb == 2);
+  if (opb == 0) { p.b_rs = ldb; p.b_ks = 1; } else { p.b_rs = 1; p.b_ks = ldb; }
+  p.C = C; p.ldc = ldc; p.c_bs = c_bs;
+  p.alpha = alpha; p.beta = beta;
+  p.beta_zero = (beta.x == 0.0 && beta.y == 0.0);
+  p.ntm = (m + ZG_BM - 1) / ZG_BM; p.ntn = (n + ZG_BN - 1) / ZG_BN;
+  if (k <= 0) {  // C = beta C
+    dim3 g(static_cast<unsigned>(std::min<long long>((static_cast<long long>(m) * n + 255) / 256, 4096)),
+           nbatch);
+    zscale_kernel<<<g, 256, 0, s>>>(C, ldc, c_bs, m, n, beta, p.beta_zero);
+    count_launch();
+    QSGW_LAUNCH_CHECK("zscale_kernel");
+    return QSGW_OK;
+  }
+  const int nch = (k + ZG_BK - 1) / ZG_BK;
+  const long long tiles = static_cast<long long>(p.ntm) * p.ntn * nbatch;
+  const int slots = 2 * ctx().sm_count;
+  int splitk = 1;
+  if (tiles < slots && nch >= 8) {
+    splitk = static_cast<int>((slots + tiles - 1) / tiles);
+    splitk = std::min(splitk, nch / 4);
+    splitk = std::max(splitk, 1);
+  }
+  p.kch_per_split = (nch + splitk - 1) / splitk;
+  splitk = (nch + p.kch_per_split - 1) / p.kch_per_split;
+  p.splitk = splitk;
+  if (splitk > 1) {
+    // beta applied up front; the tiles then add alpha*acc atomically
+    dim3 g(static_cast<unsigned>(std::min<long long>((static_cast<long long>(m) * n + 255) / 256, 4096)),
+           nbatch);
+    zscale_kernel<<<g, 256, 0, s>>>(C, ldc, c_bs, m, n, beta, p.beta_zero);
+    count_launch();
+    QSGW_LAUNCH_CHECK("zscale_kernel");
+  }
+  dim3 grid(static_cast<unsigned>(p.ntm * p.ntn), nbatch, splitk);
+  const bool arc = (opa == 0), brc = (opb != 0);
+  if (arc && brc) return launch_kernel<ZM_GEMM, true, true>(p, grid, s);
+  if (arc && !brc) return launch_kernel<ZM_GEMM, true, false>(p, grid, s);
+  if (!arc && brc) return launch_kernel<ZM_GEMM, false, true>(p, grid, s);
+  return launch_kernel<ZM_GEMM, false, false>(p, grid, s);
+}
+
+int zgemm_chi0_launch(ZParams p, int nbins, int herm, int splitk, cudaStream_t s) {
+  p.herm = herm;
+  p.splitk = splitk;
+  const int ntiles = herm ? p.ntm * (p.ntm + 1) / 2 : p.ntm * p.ntn;
+  dim3 grid(static_cast<unsigned>(ntiles), nbins, splitk);
+  return launch_kernel<ZM_CHI0, true, true>(p, grid, s);
+}
+
+int zgemm_seg_launch(ZParams p, int ncol_tiles, cudaStream_t s) {
+  if (ncol_tiles > 65535) {
+    set_error("segmented GEMM: %d column tiles exceed the grid limit", ncol_tiles);
+    return QSGW_ERR_UNSUPPORTED;
+  }
+  p.ntm = (p.M + ZG_BM - 1) / ZG_BM;
+  p.splitk = 1;
+  dim3 grid(static_cast<unsigned>(p.ntm), ncol_tiles, 1);
+  // A = op(W): 'C' / 'T' -> k-contiguous rows, 'N' -> row-contiguous
+  if (p.a_rs == 1) return launch_kernel<ZM_SEG, true, false>(p, grid, s);
+  return launch_kernel<ZM_SEG, false, false>(p, grid, s);
+}
+
+}  // namespace qsgw
+
+using namespace qsgw;
+
+static int zmm_check(int m, int n, int k, int opa, int opb, int lda, int ldb, int ldc) {
+  QSGW_ARG(m >= 0 && n >= 0 && k >= 0, "qsgw_zmm: negative size m=%d n=%d k=%d", m, n, k);
+  QSGW_ARG(opa >= 0 && opa <= 2 && opb >= 0 && opb <= 2, "qsgw_zmm: op must be 0 (N), 1 (T) or 2 (C)");
+  QSGW_ARG(lda >= std::max(1, opa == 0 ? m : k), "qsgw_zmm: lda=%d too small", lda);
+  QSGW_ARG(ldb >= std::max(1, opb == 0 ? k : n), "qsgw_zmm: ldb=%d too small", ldb);
+  QSGW_ARG(ldc >= std::max(1, m), "qsgw_zmm: ldc=%d too small", ldc);
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_zmm_d(const double* a, const double* b, double* c, int m, int n, int k,
+                          int opa, int opb, const double* alpha, const double* beta,
+                          int lda, int ldb, int ldc) {
+  int rc = require_init();
+  if (rc) return rc;
+  rc = zmm_check(m, n, k, opa, opb, lda, ldb, ldc);
+  if (rc) return rc;
+  QSGW_ARG(alpha && beta, "qsgw_zmm: alpha/beta must point to (re, im) pairs");
+  return zgemm_f64(opa, opb, m, n, k, make_double2(alpha[0], alpha[1]),
+                   reinterpret_cast<const double2*>(a), lda, 0,
+                   reinterpret_cast<const double2*>(b), ldb, 0,
+                   make_double2(beta[0], beta[1]), reinterpret_cast<double2*>(c), ldc, 0, 1,
+                   ctx().stream);
+}
+
+extern "C" int qsgw_zmm(const double* a, const double* b, double* c, int m, int n, int k,
+                        int opa, int opb, const double* alpha, const double* beta,
+                        int lda, int ldb, int ldc) {
+  int rc = require_init();
+  if (rc) return rc;
+  rc = zmm_check(m, n, k, opa, opb, lda, ldb, ldc);
+  if (rc) return rc;
+  QSGW_ARG(alpha && beta, "qsgw_zmm: alpha/beta must point to (re, im) pairs");
+  cudaStream_t s = ctx().stream;
+  const size_t na = static_cast<size_t>(lda) * (opa == 0 ? k : m);
+  const size_t nb = static_cast<size_t>(ldb) * (opb == 0 ? n : k);
+  const size_t nc = static_cast<size_t>(ldc) * n;
+  DevBuf da, db, dc;
+  rc = da.ensure(na * 16); if (rc) return rc;
+  rc = db.ensure(nb * 16); if (rc) { da.release(); return rc; }
+  rc = dc.ensure(nc * 16); if (rc) { da.release(); db.release(); return rc; }
+  auto done = [&](int r) { da.release(); db.release(); dc.release(); return r; };
+  if (na) { rc = check_cuda(cudaMemcpyAsync(da.p, a, na * 16, cudaMemcpyHostToDevice, s), "H2D a"); if (rc) return done(rc); }
+  if (nb) { rc = check_cuda(cudaMemcpyAsync(db.p, b, nb * 16, cudaMemcpyHostToDevice, s), "H2D b"); if (rc) return done(rc); }
+  rc = check_cuda(cudaMemcpyAsync(dc.p, c, nc * 16, cudaMemcpyHostToDevice, s), "H2D c");
+  if (rc) return done(rc);
+  rc = zgemm_f64(opa, opb, m, n, k, make_double2(alpha[0], alpha[1]), da.as<double2>(), lda, 0,
+                 db.as<double2>(), ldb, 0, make_double2(beta[0], beta[1]), dc.as<double2>(), ldc, 0,
+                 1, s);
+  if (rc) return done(rc);
+  rc = check_cuda(cudaMemcpyAsync(c, dc.p, nc * 16, cudaMemcpyDeviceToHost, s), "D2H c");
+  if (rc) return done(rc);
+  rc = check_cuda(cudaStreamSynchronize(s), "qsgw_zmm sync");
+  return done(rc);
+}

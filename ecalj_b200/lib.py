@@ -1,0 +1,300 @@
+"""ctypes binding of libqsgw_b200.so, mirroring the reference routines the
+C ABI replaces (names, argument meaning, 1-based Fortran indices).
+
+Host-array calls take numpy arrays (complex128 / float64 / int32, Fortran
+order where the reference array is multi-dimensional).  Device calls take
+torch CUDA tensors.  Every failure raises ``QSGWError`` with the library's
+status code and message; there is no CPU fallback: if the shared library is
+missing the import of this module fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_PKG, "libqsgw_b200.so")
+
+c_int = ctypes.c_int
+c_dbl = ctypes.c_double
+c_vp = ctypes.c_void_p
+c_ip = ctypes.POINTER(ctypes.c_int)
+c_dp = ctypes.POINTER(ctypes.c_double)
+
+STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_OOM", -4: "ERR_NOTINIT",
+          -5: "ERR_NUMERIC", -6: "ERR_TIMEOUT", -7: "ERR_UNSUPPORTED"}
+PREC_FP64 = 0
+PREC_SPLIT_F16 = 1
+
+
+class QSGWError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class SxcfArgs(ctypes.Structure):
+    """Mirror of ``qsgw_sxcf_args`` (include/qsgw_b200.h)."""
+    _fields_ = [("ngb", c_int), ("nblochpmx", c_int), ("ns1", c_int), ("ns2", c_int),
+                ("ns2r", c_int), ("ntqxx", c_int), ("ntq", c_int), ("niw", c_int),
+                ("nw", c_int), ("nwxi", c_int), ("nwx", c_int), ("nctot", c_int),
+                ("nekc", c_int), ("keepwv", c_int),
+                ("ef", c_dbl), ("esmr", c_dbl), ("wkkr", c_dbl), ("ua", c_dbl),
+                ("omega", c_vp), ("ekc", c_vp), ("freqx", c_vp), ("wwx", c_vp),
+                ("expa", c_vp), ("freq_r", c_vp),
+                ("zmel", c_vp), ("wc_imag", c_vp), ("wc_real", c_vp), ("zsec", c_vp)]
+
+
+_SIGS = {
+    "qsgw_init": [c_int],
+    "qsgw_finalize": [],
+    "qsgw_set_stream": [c_vp],
+    "qsgw_synchronize": [],
+    "qsgw_set_precision": [c_int, c_int],
+    "qsgw_get_precision": [c_ip, c_ip],
+    "qsgw_last_error": [ctypes.c_char_p, c_int],
+    "qsgw_profile": [c_int],
+    "qsgw_profile_get": [ctypes.c_char_p, c_dp, ctypes.POINTER(ctypes.c_longlong)],
+    "qsgw_zmm": [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_dp, c_dp, c_int, c_int, c_int],
+    "qsgw_zmm_d": [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_dp, c_dp, c_int, c_int, c_int],
+    "qsgw_zminv_hpd_batched_d": [c_vp, c_int, c_int, c_int],
+    "qsgw_x0gemm": [c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_int, c_int,
+                    c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int],
+    "qsgw_x0gemm_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_int, c_int,
+                      c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int],
+    "qsgw_chi0_lorentz_d": [c_vp, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_int],
+    "qsgw_chi0_lorentz": [c_vp, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_int],
+    "qsgw_wvi_llw": [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_int],
+    "qsgw_wvi_llw_d": [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_int],
+    "qsgw_sxcf_correlation": [ctypes.POINTER(SxcfArgs)],
+    "qsgw_sxcf_correlation_d": [ctypes.POINTER(SxcfArgs)],
+    "qsgw_sxcf_wgtim_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_dbl, c_dbl,
+                          c_dbl, c_vp, c_vp, c_vp],
+}
+
+
+def exported_symbols():
+    """Names the header declares (kept in sync with include/qsgw_b200.h)."""
+    return sorted(list(_SIGS) + ["qsgw_launch_count"])
+
+
+_lib = None
+
+
+def load(build_if_missing=False):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        if build_if_missing:
+            _build.build()
+        else:
+            raise ImportError(f"{LIBPATH} is missing: run `python -m ecalj_b200.build`")
+    lib = ctypes.CDLL(LIBPATH)
+    for name, args in _SIGS.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = c_int
+    lib.qsgw_launch_count.argtypes = []
+    lib.qsgw_launch_count.restype = ctypes.c_longlong
+    _lib = lib
+    return lib
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(1024)
+    load().qsgw_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def _chk(rc):
+    if rc != 0:
+        raise QSGWError(rc, last_error())
+    return rc
+
+
+def _p(a):
+    """Pointer of a numpy array or torch tensor (None passes NULL)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def _host_c128(a):
+    a = np.asarray(a)
+    if a.dtype != np.complex128 or not a.flags.f_contiguous:
+        raise ValueError("expected a Fortran-ordered complex128 array")
+    return a
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+# ---------------------------------------------------------------- context
+def init(device=0):
+    _chk(load().qsgw_init(device))
+
+
+def finalize():
+    _chk(load().qsgw_finalize())
+
+
+def set_stream(stream_handle):
+    _chk(load().qsgw_set_stream(stream_handle))
+
+
+def synchronize():
+    _chk(load().qsgw_synchronize())
+
+
+def set_precision(mode, nslices=2):
+    _chk(load().qsgw_set_precision(mode, nslices))
+
+
+def get_precision():
+    m, n = c_int(), c_int()
+    _chk(load().qsgw_get_precision(ctypes.byref(m), ctypes.byref(n)))
+    return m.value, n.value
+
+
+def launch_count():
+    return int(load().qsgw_launch_count())
+
+
+def profile(enable=True):
+    """Start (clearing old records) or stop per-kernel event timing."""
+    _chk(load().qsgw_profile(int(enable)))
+
+
+def profile_get(tag):
+    """(milliseconds, launches) summed over the recorded launches of ``tag``."""
+    ms, n = c_dbl(), ctypes.c_longlong()
+    _chk(load().qsgw_profile_get(tag.encode(), ctypes.byref(ms), ctypes.byref(n)))
+    return ms.value, n.value
+
+
+# ---------------------------------------------------------------- BLAS shim
+def _alpha(x):
+    x = complex(x)
+    return (c_dbl * 2)(x.real, x.imag)
+
+
+def zmm(a, b, c, m, n, k, opa=0, opb=0, alpha=1.0, beta=0.0, lda=None, ldb=None, ldc=None, device=False):
+    """m_blas.f90 zmm_h / zmm_d: c = alpha op(a) op(b) + beta c (c updated in place)."""
+    lda = lda or (m if opa == 0 else k)
+    ldb = ldb or (k if opb == 0 else n)
+    ldc = ldc or m
+    f = load().qsgw_zmm_d if device else load().qsgw_zmm
+    _chk(f(_p(a), _p(b), _p(c), m, n, k, opa, opb, _alpha(alpha), _alpha(beta), lda, ldb, ldc))
+    return c
+
+
+def zminv_hpd_batched_d(a, n, lda, nbatch):
+    _chk(load().qsgw_zminv_hpd_batched_d(_p(a), n, lda, nbatch))
+
+
+# ---------------------------------------------------------------- chi0
+def x0gemm(rcxq, npr, ipr_col, npr_col, nwhis, npm, ns1, ns2, zmel, nm1,
+           icounkmink, icounkmaxk, itc, itpc, jpmc, iwini, iwend, icouini, whwc,
+           zmel_shape=None, device=False):
+    """x0gemm.f90:2-97.  Host: rcxq (npr, npr_col, nslab) and zmel (nbb, nm,
+    nqtot) Fortran-ordered complex128 numpy arrays, rcxq updated in place.
+    Device: flat torch tensors holding the same column-major memory, with
+    ``zmel_shape = (nbb, nm, nqtot)``."""
+    if device:
+        nbb, nmz, nqtot = zmel_shape
+    else:
+        rcxq = _host_c128(rcxq)
+        zmel = _host_c128(zmel)
+        nbb, nmz, nqtot = zmel.shape
+    t = [_i32(itc), _i32(itpc), _i32(jpmc), _i32(iwini), _i32(iwend), _i32(icouini)]
+    w = _f64(whwc)
+    f = load().qsgw_x0gemm_d if device else load().qsgw_x0gemm
+    _chk(f(_p(rcxq), npr, ipr_col, npr_col, nwhis, npm, ns1, ns2, _p(zmel), nbb, nm1, nm1 + nmz - 1,
+           nqtot, icounkmink, icounkmaxk, *[_p(x) for x in t], _p(w), len(w)))
+    return rcxq
+
+
+def to_device(a):
+    """Flat torch CUDA tensor with the column-major memory of numpy array ``a``."""
+    import torch
+    return torch.from_numpy(np.asarray(a).reshape(-1, order='F').copy()).cuda()
+
+
+def from_device(t, shape):
+    """Inverse of ``to_device``: Fortran-ordered numpy array of ``shape``."""
+    return t.cpu().numpy().reshape(shape, order='F')
+
+
+def chi0_lorentz_d(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, zcols, ldz=None, host=False):
+    """All-k chi0 with device-built Lorentzian weights (include/qsgw_b200.h).
+    host=True: chi0/zcols are host arrays (numpy, column-major memory)."""
+    fi, no, nu = _f64(freq_i), _i32(nocc), _i32(nun)
+    eo, eu = _f64(eocc), _f64(eunocc)
+    f = load().qsgw_chi0_lorentz if host else load().qsgw_chi0_lorentz_d
+    _chk(f(_p(chi0), npr, niw, _p(fi), nk, _p(no), _p(nu), _p(eo), _p(eu), _p(zcols), ldz or npr))
+    return chi0
+
+
+# ---------------------------------------------------------------- W
+def wvi_llw(zxqi, nspin, vcousq, m2e, is_x0_m_basis, is_wc_m_basis, iq, nblochpmx=None,
+            zw=None, device=False, ngb=None, niw=None):
+    """m_llw.f90:265-376 (q /= 0 branch): returns zw (nblochpmx, nblochpmx, niw)."""
+    v = _f64(vcousq)
+    if device:
+        assert zw is not None and ngb is not None and niw is not None
+        nbl = nblochpmx or ngb
+        _chk(load().qsgw_wvi_llw_d(_p(zxqi), ngb, niw, nspin, _p(v), _p(m2e), int(is_x0_m_basis),
+                                   int(is_wc_m_basis), iq, _p(zw), nbl))
+        return zw
+    zxqi = _host_c128(zxqi)
+    ngb, _, niw = zxqi.shape
+    nbl = nblochpmx or ngb
+    if zw is None:
+        zw = np.zeros((nbl, nbl, niw), np.complex128, order='F')
+    m = None if m2e is None else _host_c128(m2e)
+    _chk(load().qsgw_wvi_llw(_p(zxqi), ngb, niw, nspin, _p(v), _p(m), int(is_x0_m_basis),
+                             int(is_wc_m_basis), iq, _p(zw), nbl))
+    return zw
+
+
+# ---------------------------------------------------------------- Sigma_c
+def sxcf_correlation(zsec, zmel, ns1, ns2, ns2r, nwxi, nwx, ntqxx, wc_imag, wc_real,
+                     omega, ekc, nctot, ef, esmr, wkkr, ua, freqx, wwx, expa, freq_r,
+                     keepwv=False, nblochpmx=None, device=False, ngb=None, ntq=None):
+    """get_correlation_block (m_sxcf_gemm.f90:407-612) for one task; zsec updated in place."""
+    tabs = dict(omega=_f64(omega), ekc=_f64(ekc), freqx=_f64(freqx), wwx=_f64(wwx),
+                expa=_f64(expa), freq_r=_f64(freq_r))
+    if device:
+        assert ngb is not None and ntq is not None
+    else:
+        zsec = _host_c128(zsec); zmel = _host_c128(zmel)
+        wc_imag = _host_c128(wc_imag); wc_real = _host_c128(wc_real)
+        ngb = zmel.shape[0]; ntq = zsec.shape[0]
+    niw = len(tabs['freqx']); nw = len(tabs['freq_r']) - 1
+    a = SxcfArgs(ngb=ngb, nblochpmx=nblochpmx or ngb, ns1=ns1, ns2=ns2, ns2r=ns2r, ntqxx=ntqxx,
+                 ntq=ntq, niw=niw, nw=nw, nwxi=nwxi, nwx=nwx, nctot=nctot,
+                 nekc=len(tabs['ekc']), keepwv=int(keepwv), ef=ef, esmr=esmr, wkkr=wkkr, ua=ua,
+                 omega=_p(tabs['omega']), ekc=_p(tabs['ekc']), freqx=_p(tabs['freqx']),
+                 wwx=_p(tabs['wwx']), expa=_p(tabs['expa']), freq_r=_p(tabs['freq_r']),
+                 zmel=_p(zmel), wc_imag=_p(wc_imag), wc_real=_p(wc_real), zsec=_p(zsec))
+    f = load().qsgw_sxcf_correlation_d if device else load().qsgw_sxcf_correlation
+    _chk(f(ctypes.byref(a)))
+    return zsec
+
+
+def sxcf_wgtim_d(out, niw, ns1, ns2, ntqxx, nctot, omega, ekc, esmr, wkkr, ua, freqx, wwx, expa):
+    o, e = _f64(omega), _f64(ekc)
+    x, w, ex = _f64(freqx), _f64(wwx), _f64(expa)
+    _chk(load().qsgw_sxcf_wgtim_d(_p(out), niw, ns1, ns2, ntqxx, nctot, _p(o), _p(e), len(e), esmr,
+                                  wkkr, ua, _p(x), _p(w), _p(ex)))
+    return out

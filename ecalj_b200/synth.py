@@ -1,0 +1,112 @@
+"""Seeded synthetic inputs with the shapes and value distributions of the
+benchmark configurations (the reference publishes no datasets for this path).
+
+Energies are generated in Ry as the configurations state them and handed to
+the kernels in the unit the reference uses there: Hartree for the chi0
+weights and the imaginary-axis mesh (x0kf / m_freq work in a.u.), Ry for the
+Sigma_c energies (omega, ekc, ef, esmr), with we = (omega - e)/2 in Hartree
+inside the weights (m_sxcf_gemm.f90:436).
+"""
+import math
+
+import numpy as np
+
+CONFIGS = {
+    # plain FP64 chi0 + W, Si-diamond-like size
+    "c0": dict(N=260, nk=64, nocc=4, nun=(40, 60), niw=12, seed=20260),
+    # split chi0, GaAs-like shape
+    "c1": dict(N=600, nk=216, nocc=9, nun=(100, 300), niw=24, seed=20261),
+    # Sigma_c band sum
+    "c2": dict(N=600, nq=64, niw=24, ntq=40, nm=400, nreal=50, seed=20262,
+               chi_nk=64, chi_nocc=4, chi_nun=(40, 60)),
+}
+
+
+def gauss_legendre01(n):
+    """Gauss-Legendre nodes/weights on (0,1), ascending (the nodes the
+    reference's tabulated ``gauss`` returns, mate.f90:1-206)."""
+    t, w = np.polynomial.legendre.leggauss(n)
+    return (t + 1.0) * 0.5, w * 0.5
+
+
+def imag_mesh(niw, ua=1.0):
+    """freq01 (m_freq.f90:164-186): x, wx, freq_i = (1-x)/x (Hartree), expa."""
+    x, wx = gauss_legendre01(niw)
+    fi = (1.0 - x) / x
+    return dict(x=x, wx=wx, freq_i=fi, expa=np.exp(-ua * ua * fi * fi), ua=ua)
+
+
+def chi0_spectrum(rng, nk, nocc, nun_range):
+    """Band counts and energies (Ry) per k: occupied U[-0.9, 0], unoccupied U[0.05, 4]."""
+    nun = rng.integers(nun_range[0], nun_range[1] + 1, size=nk)
+    nocc_a = np.full(nk, nocc, dtype=np.int64)
+    eocc = [rng.uniform(-0.9, 0.0, nocc) for _ in range(nk)]
+    eun = [rng.uniform(0.05, 4.0, int(n)) for n in nun]
+    return nocc_a, nun, eocc, eun
+
+
+def zmel_columns(rng, N, ncol):
+    """complex128 (N, ncol), re and im ~ N(0,1)/sqrt(N), Fortran order."""
+    s = 1.0 / math.sqrt(N)
+    z = np.empty((N, ncol), np.complex128, order='F')
+    z.real = rng.standard_normal((N, ncol)) * s
+    z.imag = rng.standard_normal((N, ncol)) * s
+    return z
+
+
+def chi0_problem(N, nk, nocc, nun, niw, seed):
+    """All inputs of one chi0(q, iw) evaluation (numpy, host)."""
+    rng = np.random.default_rng(seed)
+    nocc_a, nun_a, eocc, eun = chi0_spectrum(rng, nk, nocc, nun)
+    npair = int(np.sum(nocc_a * nun_a))
+    z = zmel_columns(rng, N, npair)
+    mesh = imag_mesh(niw)
+    return dict(N=N, nk=nk, niw=niw, nocc=nocc_a, nun=nun_a,
+                eocc_ry=eocc, eun_ry=eun,
+                eocc_h=np.concatenate(eocc) * 0.5, eun_h=np.concatenate(eun) * 0.5,
+                zcols=z, npair=npair, **mesh)
+
+
+def coulomb(N, seed):
+    """v = Q diag(lam) Q^H, Q Haar unitary, lam log-uniform in [1e-2, 1e3].
+    Returns vcousq = sqrt(lam) and the M->E matrix Q (= zcousq)."""
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+    q, r = np.linalg.qr(g)
+    q = q * (np.diag(r) / np.abs(np.diag(r)))[None, :]
+    lam = 10.0 ** rng.uniform(-2.0, 3.0, N)
+    return np.sqrt(lam), np.asfortranarray(q.astype(np.complex128))
+
+
+def freq_r_mesh(nreal, wmax=2.0):
+    """Real-axis mesh of the reference's form (m_freq.f90:95-134):
+    frhis(i) = bb (exp(aa (i-1)) - 1), freq_r(0) = 0,
+    freq_r(i) = (frhis(i) + frhis(i+1))/2, with aa, bb chosen so that nreal
+    points reach wmax (Hartree)."""
+    nw = nreal - 1
+    aa = 0.08
+    bb = wmax / (math.exp(aa * nw) - 1.0)
+    frhis = bb * (np.exp(aa * np.arange(nw + 1)) - 1.0)
+    fr = np.zeros(nw + 1)
+    fr[1:] = 0.5 * (frhis[:nw] + frhis[1:nw + 1])
+    return fr
+
+
+def sigc_task(N, ntq, nm, niw, nreal, seed, nctot=0, esmr=0.01, ef=0.0):
+    """Energies and zmel of one Sigma_c task (Ry).  Target energies
+    omega = eq(1:ntq) in [-1, 1] Ry; intermediate energies U[-1, 4] Ry."""
+    rng = np.random.default_rng(seed)
+    omega = np.sort(rng.uniform(-1.0, 1.0, ntq))
+    ekc = np.sort(rng.uniform(-1.0, 4.0, nctot + nm))
+    z = zmel_columns(rng, N, nm * ntq).reshape(N, nm, ntq, order='F')
+    mesh = imag_mesh(niw)
+    fr = freq_r_mesh(nreal)
+    return dict(omega=omega, ekc=ekc, zmel=np.asfortranarray(z), ef=ef, esmr=esmr,
+                nctot=nctot, freq_r=fr, **mesh)
+
+
+def real_axis_model(wc0, freq_r, wp=0.5):
+    """Synthetic Hermitian W_c on the real mesh (the configurations give W
+    only on the imaginary axis): W_c(w) = W_c(0) / (1 + (w/wp)^2)."""
+    g = 1.0 / (1.0 + (np.asarray(freq_r) / wp) ** 2)
+    return np.asfortranarray(wc0[:, :, None] * g[None, None, :])

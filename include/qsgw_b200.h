@@ -1,0 +1,192 @@
+/*
+ * libqsgw_b200 -- C ABI of the B200 implementation of ecalj's QSGW inner
+ * loops (chi0 -> W -> Sigma_c).  Every entry point replaces one routine of
+ * tkotani/ecalj (Fortran) at its call site and keeps that routine's argument
+ * layout:
+ *
+ *   - complex(8) arrays are interleaved (re, im) doubles, column-major, with
+ *     the Fortran leading dimensions passed explicitly;
+ *   - Fortran lower bounds (ns1:ns2, (1-npm)*nwhis:nwhis, 0:niw ...) are
+ *     passed explicitly and indices are 1-based where the reference's are;
+ *   - accumulated outputs (rcxq, zsec) are read-modify-write, as the
+ *     reference's beta = CONE GEMMs are.
+ *
+ * Functions without a suffix take HOST pointers and copy in and out.  The
+ * "_d" variants take DEVICE pointers for the large arrays (the reference
+ * passes those under `host_data use_device`); small tables stay on the host.
+ * "_d" calls are ordered on the library stream (qsgw_set_stream) and return
+ * before the GPU finishes; qsgw_synchronize() waits and reports any deferred
+ * device-side status.
+ *
+ * Return value: 0 on success, a negative qsgw_status on failure; the
+ * library never aborts.  qsgw_last_error() gives the message.  The library is
+ * not re-entrant: one caller thread per process (one MPI rank per GPU in the
+ * reference, m_gpu.f90:44).
+ */
+#ifndef QSGW_B200_H
+#define QSGW_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum qsgw_status {
+  QSGW_OK = 0,
+  QSGW_ERR_ARG = -1,         /* bad shape / bound / pointer */
+  QSGW_ERR_CUDA = -2,        /* CUDA runtime error */
+  QSGW_ERR_OOM = -3,         /* device allocation failed */
+  QSGW_ERR_NOTINIT = -4,     /* qsgw_init not called */
+  QSGW_ERR_NUMERIC = -5,     /* non-finite value or non-positive pivot */
+  QSGW_ERR_TIMEOUT = -6,     /* a bounded device wait ran out */
+  QSGW_ERR_UNSUPPORTED = -7  /* mode not built for this shape */
+};
+
+enum qsgw_precision {
+  QSGW_PREC_FP64 = 0,        /* complex FP64 on the FP64 tensor pipe (DMMA) */
+  QSGW_PREC_SPLIT_F16 = 1    /* split-FP16 slices on tcgen05, FP32 accumulate */
+};
+
+/* ---- context (replaces m_gpu.f90:14-68 gpu_init / cuBLAS+cuSOLVER handles,
+ *      m_lapack.f90:230-255 cusolver_init/cusolver_finalize) ---------------- */
+int qsgw_init(int device);
+int qsgw_finalize(void);
+/* Launch stream for every later call (a cudaStream_t; 0 = library stream). */
+int qsgw_set_stream(void *stream);
+int qsgw_synchronize(void);
+/* Runtime precision switch; the reference's is the compile-time -D__MP
+ * (m_kind.f90:3-11).  nslices: FP16 slices per operand for SPLIT_F16 (2). */
+int qsgw_set_precision(int mode, int nslices);
+int qsgw_get_precision(int *mode, int *nslices);
+/* Copies the last error message (NUL-terminated, truncated to len). */
+int qsgw_last_error(char *buf, int len);
+/* Number of kernels this library has launched since qsgw_init. */
+long long qsgw_launch_count(void);
+/* Per-kernel timing (replaces the reference's m_stopwatch laps,
+ * m_stopwatch.f90:1-133): enable != 0 clears the record and starts putting
+ * CUDA events around every hot kernel on the launch stream; qsgw_profile_get
+ * waits for the stream and returns the summed milliseconds and the launch
+ * count of one kernel tag ("chi0_dmma", "sigc_seg_dmma", "gemm_dmma",
+ * "chi0_tc", "sigc_seg_tc").                                              */
+int qsgw_profile(int enable);
+int qsgw_profile_get(const char *tag, double *ms, long long *launches);
+
+/* ---- BLAS shim: ZGEMM (m_blas.f90:198 zmm_h, :469 zmm_d) ----------------
+ * C = alpha op(A) op(B) + beta C; op = 0 'N', 1 'T', 2 'C' (m_op_n/t/c).
+ * alpha/beta are complex given as (re, im) pairs.  Always FP64.            */
+int qsgw_zmm(const double *a, const double *b, double *c, int m, int n, int k,
+             int opa, int opb, const double *alpha, const double *beta,
+             int lda, int ldb, int ldc);
+int qsgw_zmm_d(const double *a, const double *b, double *c, int m, int n,
+               int k, int opa, int opb, const double *alpha,
+               const double *beta, int lda, int ldb, int ldc);
+
+/* ---- Inverse of a batch of Hermitian positive definite matrices in place
+ * (replaces zminv_d, m_lapack.f90:108-176, on the imaginary axis where
+ * eps~ = 1 - v^1/2 chi0 v^1/2 is HPD because chi0(iw) <= 0).  Blocked
+ * Gauss-Jordan, FP64.  a: device, nbatch matrices at stride lda*n.
+ * Returns QSGW_ERR_NUMERIC (after the batch completes) if a pivot block is
+ * not invertible.                                                          */
+int qsgw_zminv_hpd_batched_d(double *a, int n, int lda, int nbatch);
+
+/* ---- chi0 rank-k accumulation: drop-in for x0gemm (x0gemm.f90:2-97) ----
+ * rcxq(npr, npr_col, (1-npm)*nwhis : nwhis) += sum over pairs of
+ *   conj(zmel(:,it,itp)) * whw * zmel(ipr_col-1+:, it, itp)^T
+ * per (jpm, iw) bin, the bin landing in slab iw*(3-2*jpm).
+ * zmel(nbb, nm1:nm2, nqtot) as get_zmel_init_gemm leaves it (conjugated).
+ * Pair tables are m_x0kf's (x0kf_v4h.f90:40-41,118-133), 1-based, read in
+ * icoun = icounkmink..icounkmaxk; only pairs with ns1 <= it <= ns2 count.
+ * whwc has ncount entries.  Index tables are host arrays in both variants. */
+int qsgw_x0gemm(double *rcxq, int npr, int ipr_col, int npr_col, int nwhis,
+                int npm, int ns1, int ns2, const double *zmel, int nbb,
+                int nm1, int nm2, int nqtot, int icounkmink, int icounkmaxk,
+                const int *itc, const int *itpc, const int *jpmc,
+                const int *iwini, const int *iwend, const int *icouini,
+                const double *whwc, int ncount);
+int qsgw_x0gemm_d(double *rcxq_d, int npr, int ipr_col, int npr_col,
+                  int nwhis, int npm, int ns1, int ns2, const double *zmel_d,
+                  int nbb, int nm1, int nm2, int nqtot, int icounkmink,
+                  int icounkmaxk, const int *itc, const int *itpc,
+                  const int *jpmc, const int *iwini, const int *iwend,
+                  const int *icouini, const double *whwc, int ncount);
+
+/* ---- chi0 for all k-points and all imaginary frequencies in one call
+ * (the k-loop of x0kf_zxq, x0kf_v4h.f90:233-290, with the direct iw
+ * Lorentzian weights that stand in for the tetrahedron weights):
+ *   chi0(:,:,iw) = sum_k sum_{pairs of k} w(pair,iw) conj(z) z^T,
+ *   w = -2 de / (de^2 + freq_i(iw)^2) / nk,   de = e_unocc - e_occ.
+ * zcols_d: device, complex (npr, ncol) = the zmel columns of every k
+ * (zmel(:, it, itp) of k stored at column col0[k] + (it-1) + nocc_k*(itp-1)).
+ * eocc/eunocc: host, concatenated per k (offsets by prefix sums of nocc/nun).
+ * chi0_d: device complex (npr, npr, niw), overwritten.  The weights are
+ * formed on the GPU in FP64.  Uses the precision set by qsgw_set_precision. */
+int qsgw_chi0_lorentz_d(double *chi0_d, int npr, int niw, const double *freq_i,
+                        int nk, const int *nocc, const int *nun,
+                        const double *eocc, const double *eunocc,
+                        const double *zcols_d, int ldz);
+/* Same with host chi0 / zcols (copied in and out inside the call). */
+int qsgw_chi0_lorentz(double *chi0, int npr, int niw, const double *freq_i,
+                      int nk, const int *nocc, const int *nun,
+                      const double *eocc, const double *eunocc,
+                      const double *zcols, int ldz);
+
+/* ---- W - v on the imaginary axis: drop-in for the per-iw block of
+ * WVIllwI (m_llw.f90:265-376, q /= 0 branch, iq <= nqibz):
+ *   chi *= 2 if nspin == 1 (in place, :299-303); chi -> m2e^H chi m2e if
+ *   is_x0_m_basis; eps~ = 1 - v^1/2 chi v^1/2; zw = v^1/2 (eps~^-1 - 1)
+ *   v^1/2; zw -> m2e zw m2e^H if is_wc_m_basis and iq /= 1.
+ * iq == 1 skips the head row/column (ix = 1).  zw(nblochpmx,nblochpmx,niw)
+ * is overwritten (rows/cols beyond ngb zero).  All iw in one batch.        */
+int qsgw_wvi_llw(double *zxqi, int ngb, int niw, int nspin,
+                 const double *vcousq, const double *m2e, int is_x0_m_basis,
+                 int is_wc_m_basis, int iq, double *zw, int nblochpmx);
+int qsgw_wvi_llw_d(double *zxqi_d, int ngb, int niw, int nspin,
+                   const double *vcousq, const double *m2e_d,
+                   int is_x0_m_basis, int is_wc_m_basis, int iq,
+                   double *zw_d, int nblochpmx);
+
+/* ---- Sigma_c band sum: drop-in for get_correlation_block of
+ * sxcf_scz_correlation (m_sxcf_gemm.f90:407-612) for one task
+ * (kx, irot, ip, isp, icount).                                            */
+typedef struct qsgw_sxcf_args {
+  int ngb;          /* product-basis size = nbb (zmel rows)                 */
+  int nblochpmx;    /* leading dimension of the W records                   */
+  int ns1, ns2;     /* middle states [ns1, ns2] (nstti/nstte)               */
+  int ns2r;         /* last middle state of the pole part (nstte2)          */
+  int ntqxx, ntq;   /* target states used; leading dimension of zsec        */
+  int niw, nw;      /* imaginary points; real-axis records 0..nw            */
+  int nwxi, nwx;    /* real-axis window (nwxic, nwxc)                       */
+  int nctot;        /* core states at the head of ekc                       */
+  int nekc;         /* length of ekc (nctot + nband)                        */
+  int keepwv;       /* 1: W given as packed upper triangles (--keepwv)      */
+  double ef, esmr, wkkr, ua;
+  const double *omega;   /* host (ntq): eq(1:ntq), Ry                       */
+  const double *ekc;     /* host (nekc): [ecore; e(q-k)], Ry                */
+  const double *freqx;   /* host (niw): Gauss points x in (0,1)             */
+  const double *wwx;     /* host (niw): their weights                       */
+  const double *expa;    /* host (niw): exp(-ua^2 w^2)                      */
+  const double *freq_r;  /* host (nw+1): real-axis mesh, freq_r(0) = 0      */
+  const double *zmel;    /* complex (ngb, ns2-ns1+1, ntqxx), M basis        */
+  const double *wc_imag; /* complex (nblochpmx,nblochpmx,niw+1): slot 0 is
+                            W(w=0)-v (first __WVR record), 1..niw __WVI; with
+                            keepwv: (ngb(ngb+1)/2, niw+1) packed upper      */
+  const double *wc_real; /* complex (nblochpmx,nblochpmx,nw+1) __WVR records;
+                            with keepwv: packed (ngb(ngb+1)/2, nw+1) of the
+                            already symmetrised (W+W^H)/2                   */
+  double *zsec;          /* complex (ntq, ntq), accumulated                 */
+} qsgw_sxcf_args;
+/* Host pointers for every array. */
+int qsgw_sxcf_correlation(const qsgw_sxcf_args *args);
+/* zmel, wc_imag, wc_real, zsec are device pointers; the tables stay host. */
+int qsgw_sxcf_correlation_d(const qsgw_sxcf_args *args);
+
+/* Imaginary-axis weights wgtim(0:niw, ns1:ns2, ntqxx), FP64 on the GPU
+ * (m_sxcf_gemm.f90:432-458, npm = 1).  wgtim_d: device (niw+1, nm, ntqxx). */
+int qsgw_sxcf_wgtim_d(double *wgtim_d, int niw, int ns1, int ns2, int ntqxx,
+                      int nctot, const double *omega, const double *ekc,
+                      int nekc, double esmr, double wkkr, double ua,
+                      const double *freqx, const double *wwx,
+                      const double *expa);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QSGW_B200_H */

@@ -1,0 +1,57 @@
+"""The C-ABI library loads and exports every entry point that
+include/qsgw_b200.h declares; argument checks that run before any CUDA call
+behave (no GPU needed)."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from ecalj_b200 import lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "qsgw_b200.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(qsgw_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def so():
+    if not os.path.exists(lib.LIBPATH):
+        from ecalj_b200 import build
+        build.build()
+    return lib.load()
+
+
+def test_header_lists_entry_points():
+    names = _declared()
+    assert "qsgw_x0gemm" in names and "qsgw_sxcf_correlation_d" in names
+    assert set(names) == set(lib.exported_symbols()), set(names) ^ set(lib.exported_symbols())
+
+
+def test_library_exports_every_declared_symbol(so):
+    out = subprocess.run(["nm", "-D", "--defined-only", lib.LIBPATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (qsgw_\w+)", out))
+    missing = [n for n in _declared() if n not in exported]
+    assert not missing, missing
+    for n in _declared():
+        assert hasattr(so, n)
+
+
+def test_calls_before_init_fail_cleanly(so):
+    assert so.qsgw_synchronize() == -4
+    assert "qsgw_init" in lib.last_error()
+    assert so.qsgw_x0gemm(None, 1, 1, 1, 1, 1, 1, 1, None, 1, 1, 1, 1, 1, 1,
+                          None, None, None, None, None, None, None, 0) == -4
+
+
+def test_precision_switch_validates(so):
+    assert so.qsgw_set_precision(7, 2) == -1
+    assert so.qsgw_set_precision(1, 3) == -1
+    assert so.qsgw_set_precision(1, 2) == 0
+    assert lib.get_precision() == (1, 2)
+    assert so.qsgw_set_precision(0, 1) == 0
