@@ -80,8 +80,13 @@ __global__ void unpack_upper_kernel(double2* __restrict__ w, const double2* __re
     const int j = static_cast<int>(r % n);
     const long long m = r / n;
     double2 v;
-    if (i <= j) {
+    if (i < j) {
       v = up[m * np + static_cast<long long>(j) * (j + 1) / 2 + i];
+    } else if (i == j) {
+      // wc(i,j) = up then wc(j,i) = conjg(up) in the same iteration: the
+      // diagonal ends up conjugated (m_sxcf_gemm.f90:470-473)
+      const double2 u = up[m * np + static_cast<long long>(j) * (j + 1) / 2 + i];
+      v = make_double2(u.x, -u.y);
     } else {
       const double2 u = up[m * np + static_cast<long long>(i) * (i + 1) / 2 + j];
       v = make_double2(u.x, -u.y);
@@ -297,14 +302,17 @@ int sxcf_device(const qsgw_sxcf_args& a) {
   QSGW_CUDA(cudaMemcpyAsync(g_sc_w3.p, w3.data(), w3.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   std::map<int, std::vector<int>> groups;
   for (long long c = 0; c < ncol; ++c) groups[key[c]].push_back(static_cast<int>(c));
+  const bool split = ctx().prec_mode == QSGW_PREC_SPLIT_F16;
+  const int tilew = split ? 128 : ZG_BN;       // column tile of the split / FP64 kernel
   std::vector<ZSeg> segs;
-  std::vector<int> gseg_off, gnseg, tile_group, tile_cols;
+  std::vector<int> gseg_off, gnseg, tile_group, tile_cols, seg_slot;
   int gidx = 0;
   for (auto& kv : groups) {
     gseg_off.push_back(static_cast<int>(segs.size()));
     for (int sgi = 0; sgi <= niw; ++sgi) {
       ZSeg z{wi + sgi * wsz, g_sc_wg.as<double>() + sgi, niw + 1, 0};
       segs.push_back(z);
+      seg_slot.push_back(sgi);
     }
     if (kv.first > 0) {
       for (int i = 0; i < 3; ++i) {
@@ -313,49 +321,66 @@ int sxcf_device(const qsgw_sxcf_args& a) {
         if (it == bin_slot.end()) continue;
         ZSeg z{wr + it->second * wsz, g_sc_w3.as<double>() + i, 3, 0};
         segs.push_back(z);
+        seg_slot.push_back(niw + 1 + it->second);
       }
     }
     gnseg.push_back(static_cast<int>(segs.size()) - gseg_off.back());
     const auto& cols = kv.second;
-    for (size_t t0 = 0; t0 < cols.size(); t0 += ZG_BN) {
+    for (size_t t0 = 0; t0 < cols.size(); t0 += tilew) {
       tile_group.push_back(gidx);
-      for (int j = 0; j < ZG_BN; ++j)
+      for (int j = 0; j < tilew; ++j)
         tile_cols.push_back(t0 + j < cols.size() ? cols[t0 + j] : -1);
     }
     ++gidx;
   }
   const int ntiles = static_cast<int>(tile_group.size());
-  const size_t tb = segs.size() * sizeof(ZSeg) + (gseg_off.size() + gnseg.size() + tile_group.size() +
-                                                  tile_cols.size()) * sizeof(int);
-  rc = g_sc_tmp.ensure(tb + 16 * 5);
-  if (rc) return rc;
-  unsigned char* tbase = g_sc_tmp.as<unsigned char>();
-  size_t off = 0;
-  int cprc = 0;
-  auto put = [&](const void* src, size_t n) -> const void* {
-    void* dst = tbase + off;
-    if (!cprc) cprc = check_cuda(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s), "H2D sxcf tables");
-    off += (n + 15) & ~size_t(15);
-    return dst;
-  };
-  ZParams p{};
-  p.segs = reinterpret_cast<const ZSeg*>(put(segs.data(), segs.size() * sizeof(ZSeg)));
-  p.group_seg_off = reinterpret_cast<const int*>(put(gseg_off.data(), gseg_off.size() * sizeof(int)));
-  p.group_nseg = reinterpret_cast<const int*>(put(gnseg.data(), gnseg.size() * sizeof(int)));
-  p.tile_group = reinterpret_cast<const int*>(put(tile_group.data(), tile_group.size() * sizeof(int)));
-  p.tile_cols = reinterpret_cast<const int*>(put(tile_cols.data(), tile_cols.size() * sizeof(int)));
-  if (cprc) return cprc;
   rc = g_sc_cz.ensure(static_cast<size_t>(ngb) * ncol * sizeof(double2));
   if (rc) return rc;
   double2* cz = g_sc_cz.as<double2>();
-  // ---- 3. imaginary axis + poles in one launch
-  p.M = ngb; p.K = ngb;
-  p.a_rs = ldw; p.a_ks = 1; p.a_conj = 1;             // Wc^H (:492 opA = m_op_C)
-  p.B = zmel; p.b_rs = ngb; p.b_ks = 1; p.b_conj = 0;
-  p.C = cz; p.ldc = ngb; p.beta_zero = 1;
-  if (ctx().prec_mode == QSGW_PREC_SPLIT_F16) rc = sigc_seg_split_f16(p, ntiles, s);
-  else rc = zgemm_seg_launch(p, ntiles, s);
-  if (rc) return rc;
+  if (split) {
+    // ---- 3'. the same contraction in split FP16 on tcgen05
+    SigcSplitArgs sa;
+    sa.ngb = ngb; sa.ldw = ldw;
+    sa.wi = wi; sa.nimag = niw + 1;
+    sa.wr = wr; sa.nreal = nrec;
+    sa.zmel = zmel; sa.ncol = ncol;
+    sa.wgt = g_sc_wg.as<double>(); sa.nwgt = ncol * (niw + 1);
+    sa.w3 = g_sc_w3.as<double>(); sa.nw3 = poles.empty() ? 0 : ncol * 3;
+    sa.tile_cols = std::move(tile_cols); sa.tile_group = std::move(tile_group);
+    sa.group_seg_off = std::move(gseg_off); sa.group_nseg = std::move(gnseg);
+    sa.seg_slot = std::move(seg_slot); sa.segs = std::move(segs);
+    sa.out = cz;
+    rc = sigc_split_f16(sa, s);
+    if (rc) return rc;
+  } else {
+    const size_t tb = segs.size() * sizeof(ZSeg) + (gseg_off.size() + gnseg.size() + tile_group.size() +
+                                                    tile_cols.size()) * sizeof(int);
+    rc = g_sc_tmp.ensure(tb + 16 * 5);
+    if (rc) return rc;
+    unsigned char* tbase = g_sc_tmp.as<unsigned char>();
+    size_t off = 0;
+    int cprc = 0;
+    auto put = [&](const void* src, size_t n) -> const void* {
+      void* dst = tbase + off;
+      if (!cprc) cprc = check_cuda(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s), "H2D sxcf tables");
+      off += (n + 15) & ~size_t(15);
+      return dst;
+    };
+    ZParams p{};
+    p.segs = reinterpret_cast<const ZSeg*>(put(segs.data(), segs.size() * sizeof(ZSeg)));
+    p.group_seg_off = reinterpret_cast<const int*>(put(gseg_off.data(), gseg_off.size() * sizeof(int)));
+    p.group_nseg = reinterpret_cast<const int*>(put(gnseg.data(), gnseg.size() * sizeof(int)));
+    p.tile_group = reinterpret_cast<const int*>(put(tile_group.data(), tile_group.size() * sizeof(int)));
+    p.tile_cols = reinterpret_cast<const int*>(put(tile_cols.data(), tile_cols.size() * sizeof(int)));
+    if (cprc) return cprc;
+    // ---- 3. imaginary axis + poles in one launch
+    p.M = ngb; p.K = ngb;
+    p.a_rs = ldw; p.a_ks = 1; p.a_conj = 1;             // Wc^H (:492 opA = m_op_C)
+    p.B = zmel; p.b_rs = ngb; p.b_ks = 1; p.b_conj = 0;
+    p.C = cz; p.ldc = ngb; p.beta_zero = 1;
+    rc = zgemm_seg_launch(p, ntiles, s);
+    if (rc) return rc;
+  }
   // ---- 4. zsec += czmelwc^H zmel (:599) and the Im clamp (:601-607)
   const long long kk = static_cast<long long>(ngb) * nm;
   rc = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,

@@ -1,16 +1,762 @@
-// Split-FP16 tcgen05 path (placeholder until the kernel lands).
+// Split-FP16 complex contractions on the 5th-generation tensor cores
+// (tcgen05.mma kind::f16, FP32 accumulators in TMEM, TMA-fed shared memory).
+//
+// A complex product C = A B is run as one real GEMM with the M dimension
+// doubled and K interleaved (k' = 2k + {re, im}):
+//     rows (m, re) of A' = [Re a, -Im a],   rows (m, im) of A' = [Im a, Re a]
+//     row n of B'       = [Re b,  Im b]   (K-major)
+// so lanes 0..63 of a 128-lane accumulator hold Re C and lanes 64..127 Im C.
+// Every FP64 operand is split into two scaled FP16 slices x = hi + lo
+// (22 significant bits); the product keeps hi*hi + hi*lo + lo*hi (the lo*lo
+// term, ~2^-22 relative, is dropped) and accumulates in FP32.
+//
+// The weight that differs per frequency (chi0, x0gemm.f90:84) or per
+// segment and column (Sigma_c, m_sxcf_gemm.f90:485) multiplies B.  A' and
+// the B source are pre-split once into HBM and streamed by TMA; four
+// converter warps apply the weight to the B source in shared memory and
+// re-split it into B' for every frequency / segment, while one thread issues
+// the MMAs.  Warp roles (192 threads, one CTA per SM):
+//     warp 0      TMA producer
+//     warp 1      TMEM owner and MMA issuer
+//     warps 2..5  B' converters, then the epilogue (TMEM -> FP64 atomics)
+// Every mbarrier wait is bounded; on time-out the CTA records an error,
+// drains its own TMA and MMA work, frees TMEM and exits.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <vector>
 #include "split_f16.cuh"
 
 namespace qsgw {
+namespace tc {
 
-int chi0_split_f16(double2*, int, int, const double2*, int, long long, const double*, cudaStream_t) {
-  set_error("split-FP16 chi0 is not built yet");
-  return QSGW_ERR_UNSUPPORTED;
+constexpr int BM2 = 128;                 // real accumulator rows (64 complex x {re, im})
+constexpr int BMC = 64;                  // complex rows per tile
+constexpr int NC = 128;                  // complex columns per tile (UMMA N)
+constexpr int KC = 64;                   // FP16 elements per chunk along K' (32 complex k)
+constexpr int NSTAGE = 2;
+constexpr int NTHREADS = 192;
+constexpr int NCONV = 128;               // converter threads (warps 2..5)
+constexpr int SLICE_A = BM2 * KC * 2;    // 16 KB
+constexpr int SLICE_S = NC * KC * 2;     // 16 KB
+constexpr int SLICE_B = NC * KC * 2;     // 16 KB
+constexpr int OFF_A = 0;
+constexpr int OFF_S = OFF_A + NSTAGE * 2 * SLICE_A;
+constexpr int OFF_B = OFF_S + NSTAGE * 2 * SLICE_S;
+constexpr int OFF_W = OFF_B + 2 * 2 * SLICE_B;          // chi0 weights per B' buffer: 2 x 32 floats
+constexpr int OFF_BAR = OFF_W + 2 * 32 * 4;
+constexpr int NBAR = 2 * NSTAGE + 2 + 2 + 1;
+constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
+constexpr int SMEM_BYTES = OFF_MISC + 64 + 1024;        // + slack for 1024-B alignment
+constexpr long long WAIT_LIMIT = 1LL << 24;              // bounded spin (several seconds)
+
+enum { MODE_CHI0 = 0, MODE_SEG = 1 };
+
+struct Params {
+  int mode;
+  int M, N;                 // complex rows / columns of C
+  int ntm, ntn;
+  int J;                    // accumulators per CTA
+  int kch_total, kch_per_split, cps;
+  // chi0
+  const double* w;          // w[iw * npair + p]
+  long long npair;
+  int niw;
+  // seg
+  const int* tile_group;
+  const int* tile_cols;
+  const int* group_seg_off;
+  const int* group_nseg;
+  const int* seg_slot;      // A' slot of every segment
+  const ZSeg* segs;         // scale pointer / column stride of every segment
+  int tiles_per_slot;       // m-tiles of one A' slot
+  int lo_tile_off;          // tile offset of the lo slice in the A' map
+  int lo_row_off;           // row (2-D) / tile (4-D) offset of the lo slice in the S map
+  // output
+  double2* C;
+  long long ldc, c_bs;
+  const double* scales;     // [0] sigma_A, [1] sigma_S, [2 + j] sigma_B(j)
+  int* err;
+};
+
+// ------------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: returns false (and raises the CTA abort flag) on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+  for (long long i = 0; i < WAIT_LIMIT; ++i) {
+    if (mbar_try(b, parity)) return true;
+    if (*abort_flag) return false;
+    if (i > 64) __nanosleep(64);
+  }
+  *abort_flag = 1;
+  return false;
+}
+// Warp-uniform bounded wait: lane 0 polls, every lane gets the same answer.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+  int ok = 0;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(b, parity, abort_flag) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+// Bounded wait that ignores the abort flag: used only to drain the CTA's own
+// in-flight TMA / MMA work before it frees TMEM and exits.
+__device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
+  for (long long i = 0; i < WAIT_LIMIT; ++i) {
+    if (mbar_try(b, parity)) return;
+    if (i > 64) __nanosleep(64);
+  }
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2),
+        "r"(c3)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+      : "memory");
 }
 
-int sigc_seg_split_f16(const ZParams&, int, cudaStream_t) {
-  set_error("split-FP16 Sigma_c is not built yet");
-  return QSGW_ERR_UNSUPPORTED;
+// K-major, 128-byte swizzle UMMA shared-memory descriptor: rows of 128 B in
+// 8-row atoms (SBO = 1024 B), version 1, layout type SWIZZLE_128B.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
+  d |= static_cast<uint64_t>(1) << 16;                 // LBO (unused for swizzled K-major)
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;         // SBO
+  d |= static_cast<uint64_t>(1) << 46;                 // version
+  d |= static_cast<uint64_t>(2) << 61;                 // SWIZZLE_128B
+  return d;
+}
+// kind::f16, A = B = F16, D = F32, both K-major, M = 128, N = NC
+constexpr uint32_t IDESC = (1u << 4) | (static_cast<uint32_t>(NC >> 3) << 17) | (static_cast<uint32_t>(BM2 >> 4) << 24);
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// offset of the 16-byte chunk `c` of row `r` inside a 128B-swizzled tile
+__device__ __forceinline__ int sw128_off(int r, int c) { return r * 128 + ((c ^ (r & 7)) << 4); }
+
+// ------------------------------------------------------------------ the kernel
+__global__ void __launch_bounds__(NTHREADS, 1)
+    split_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapS,
+                      const Params p) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* sA = sm + OFF_A;
+  unsigned char* sS = sm + OFF_S;
+  unsigned char* sB = sm + OFF_B;
+
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
+  uint64_t* full = bar;                  // [NSTAGE]
+  uint64_t* empty = bar + NSTAGE;        // [NSTAGE]
+  uint64_t* bfull = bar + 2 * NSTAGE;    // [2]
+  uint64_t* bempty = bfull + 2;          // [2]
+  uint64_t* accfull = bempty + 2;        // [1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + OFF_MISC);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + OFF_MISC + 8);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // ---- work unit
+  const int tileid = blockIdx.x;
+  const int mt = tileid % p.ntm, nt = tileid / p.ntm;
+  const int jg = blockIdx.y;
+  const int split = blockIdx.z;
+  const int J = p.J;
+  const int c0 = split * p.kch_per_split;
+  const int c1 = min(p.kch_total, c0 + p.kch_per_split);
+  const int nch = c1 - c0;
+  int group = 0, nseg = 0, seg0 = 0;
+  if (p.mode == MODE_SEG) {
+    group = p.tile_group[nt];
+    nseg = p.group_nseg[group];
+    seg0 = p.group_seg_off[group];
+  }
+  const int nchunk = (p.mode == MODE_SEG) ? nseg * p.cps : nch;
+  const int cbeg = (p.mode == MODE_SEG) ? 0 : c0;
+
+  if (tid == 0) {
+    for (int i = 0; i < NSTAGE; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    for (int i = 0; i < 2; ++i) { mbar_init(&bfull[i], NCONV); mbar_init(&bempty[i], 1); }
+    mbar_init(accfull, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  const uint32_t ncols = (J * NC <= 128) ? 128 : (J * NC <= 256 ? 256 : 512);
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (nchunk > 0) {
+    if (warp == 0 && lane == 0) {
+      // ---------------- TMA producer
+      const uint32_t bytes = 2 * SLICE_A + 2 * SLICE_S;
+      int issued = 0;
+      for (int c = 0; c < nchunk; ++c) {
+        const int st = c % NSTAGE;
+        if (c >= NSTAGE && !mbar_wait(&empty[st], ((c / NSTAGE) - 1) & 1, abort_flag)) break;
+        issued = c + 1;
+        mbar_expect_tx(&full[st], bytes);
+        unsigned char* a = sA + st * 2 * SLICE_A;
+        unsigned char* s = sS + st * 2 * SLICE_S;
+        if (p.mode == MODE_CHI0) {
+          const int x = (cbeg + c) * KC;
+          tma_load_4d(a, &mapA, &full[st], x, 0, 0, mt);
+          tma_load_4d(a + SLICE_A, &mapA, &full[st], x, 0, 0, p.lo_tile_off + mt);
+          tma_load_4d(s, &mapS, &full[st], x, 0, 0, 2 * nt);
+          tma_load_4d(s + SLICE_S, &mapS, &full[st], x, 0, 0, p.lo_row_off + 2 * nt);
+        } else {
+          const int sg = c / p.cps;
+          const int x = (c - sg * p.cps) * KC;
+          const int t = p.seg_slot[seg0 + sg] * p.tiles_per_slot + mt;
+          tma_load_4d(a, &mapA, &full[st], x, 0, 0, t);
+          tma_load_4d(a + SLICE_A, &mapA, &full[st], x, 0, 0, p.lo_tile_off + t);
+          tma_load_2d(s, &mapS, &full[st], x, nt * NC);
+          tma_load_2d(s + SLICE_S, &mapS, &full[st], x, p.lo_row_off + nt * NC);
+        }
+      }
+      // every issued copy has landed before the CTA may exit
+      for (int c = max(0, issued - NSTAGE); c < issued; ++c) mbar_drain(&full[c % NSTAGE], (c / NSTAGE) & 1);
+    } else if (warp == 1 && lane == 0) {
+      // ---------------- MMA issuer
+      int it = 0;
+      for (int c = 0; c < nchunk && !*abort_flag; ++c) {
+        const int st = c % NSTAGE;
+        if (!mbar_wait(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
+        const uint32_t a_hi = smem_u32(sA + st * 2 * SLICE_A), a_lo = a_hi + SLICE_A;
+        bool ok = true;
+        for (int j = 0; j < J; ++j, ++it) {
+          const int b = it & 1;
+          if (!mbar_wait(&bfull[b], (it >> 1) & 1, abort_flag)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t b_hi = smem_u32(sB + b * 2 * SLICE_B), b_lo = b_hi + SLICE_B;
+          const uint32_t d = tmem + static_cast<uint32_t>(j * NC);
+#pragma unroll
+          for (int kk = 0; kk < KC / 16; ++kk) {
+            const uint32_t ko = kk * 32;   // 16 FP16 = 32 B along K
+            const uint32_t acc0 = (c == 0 && kk == 0) ? 0u : 1u;
+            umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_hi + ko), acc0);
+            umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_lo + ko), 1u);
+            umma_f16(d, sw128_desc(a_lo + ko), sw128_desc(b_hi + ko), 1u);
+          }
+          umma_commit(&bempty[b]);
+        }
+        if (!ok) break;
+        umma_commit(&empty[st]);
+      }
+      umma_commit(accfull);
+      mbar_drain(accfull, 0);      // all issued MMAs retired
+    } else if (warp >= 2) {
+      // ---------------- converters: B'_j = weight_j * (S_hi + S_lo), re-split
+      const int ct = tid - 64;                 // 0..127 = row n of the tile
+      int it = 0;
+      double rowscale_seg = 0.0;
+      for (int c = 0; c < nchunk; ++c) {
+        const int st = c % NSTAGE;
+        if (!mbar_wait_warp(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
+        const unsigned char* s_hi = sS + st * 2 * SLICE_S;
+        const unsigned char* s_lo = s_hi + SLICE_S;
+        if (p.mode == MODE_SEG) {
+          const int sg = c / p.cps;
+          const int col = p.tile_cols[nt * NC + ct];
+          const ZSeg zs = p.segs[seg0 + sg];
+          rowscale_seg = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
+        }
+        bool ok = true;
+        for (int j = 0; j < J; ++j, ++it) {
+          const int b = it & 1;
+          if (it >= 2 && !mbar_wait_warp(&bempty[b], ((it >> 1) - 1) & 1, abort_flag)) { ok = false; break; }
+          float wl = 0.f, rs = 1.f;
+          if (p.mode == MODE_CHI0) {
+            // lane i holds the weight of complex k = i of this chunk; shuffled below
+            const int iw = jg * J + j;
+            const long long pr = static_cast<long long>(cbeg + c) * 32 + lane;
+            if (iw < p.niw && pr < p.npair)
+              wl = static_cast<float>(p.w[static_cast<long long>(iw) * p.npair + pr] * p.scales[2 + iw]);
+          } else {
+            rs = static_cast<float>(rowscale_seg * p.scales[2]);
+          }
+          unsigned char* d_hi = sB + b * 2 * SLICE_B;
+          unsigned char* d_lo = d_hi + SLICE_B;
+#pragma unroll
+          for (int ch = 0; ch < 8; ++ch) {
+            const int off = sw128_off(ct, ch);
+            const uint4 vh = *reinterpret_cast<const uint4*>(s_hi + off);
+            const uint4 vl = *reinterpret_cast<const uint4*>(s_lo + off);
+            const __half2* h2 = reinterpret_cast<const __half2*>(&vh);
+            const __half2* l2 = reinterpret_cast<const __half2*>(&vl);
+            uint4 oh, ol;
+            __half2* oh2 = reinterpret_cast<__half2*>(&oh);
+            __half2* ol2 = reinterpret_cast<__half2*>(&ol);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              // the pair (re, im) of complex k = 4*ch + q
+              const float2 fh = __half22float2(h2[q]);
+              const float2 fl = __half22float2(l2[q]);
+              const float wk = __shfl_sync(0xffffffffu, wl, ch * 4 + q);
+              const float f = (p.mode == MODE_CHI0) ? wk : rs;
+              const float v0 = (fh.x + fl.x) * f, v1 = (fh.y + fl.y) * f;
+              const __half2 hi = __floats2half2_rn(v0, v1);
+              const float2 fb = __half22float2(hi);
+              oh2[q] = hi;
+              ol2[q] = __floats2half2_rn(v0 - fb.x, v1 - fb.y);
+            }
+            *reinterpret_cast<uint4*>(d_hi + off) = oh;
+            *reinterpret_cast<uint4*>(d_lo + off) = ol;
+          }
+          fence_async_smem();
+          mbar_arrive(&bfull[b]);
+        }
+        if (!ok) break;
+      }
+      // ---------------- epilogue: TMEM -> FP64 atomics
+      if (mbar_wait_warp(accfull, 0, abort_flag)) {
+        tc_fence_after();
+        const int quad = warp & 3;            // TMEM lanes 32*quad .. 32*quad+31
+        const int row = quad * 32 + lane;     // accumulator row: 0..63 re, 64..127 im
+        const int m = mt * BMC + (row & 63);
+        const bool im_part = row >= 64;
+        const double inv_as = 1.0 / (p.scales[0] * p.scales[1]);
+        for (int j = 0; j < J; ++j) {
+          double inv;
+          double2* Cj;
+          if (p.mode == MODE_CHI0) {
+            const int iw = jg * J + j;
+            if (iw >= p.niw) break;
+            inv = inv_as / p.scales[2 + iw];
+            Cj = p.C + static_cast<long long>(iw) * p.c_bs;
+          } else {
+            inv = inv_as / p.scales[2];
+            Cj = p.C;
+          }
+          for (int cb = 0; cb < NC / 32; ++cb) {
+            float v[32];
+            tmem_ld32(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(j * NC + cb * 32), v);
+            if (m >= p.M) continue;
+#pragma unroll 4
+            for (int i = 0; i < 32; ++i) {
+              const int nloc = cb * 32 + i;
+              long long col;
+              if (p.mode == MODE_CHI0) {
+                col = nt * NC + nloc;
+                if (col >= p.N) continue;
+              } else {
+                col = p.tile_cols[nt * NC + nloc];
+                if (col < 0) continue;
+              }
+              double* dst = reinterpret_cast<double*>(Cj + m + col * p.ldc) + (im_part ? 1 : 0);
+              atomicAdd(dst, static_cast<double>(v[i]) * inv);
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  if (*abort_flag && tid == 0) atomicExch(p.err, 2);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+  }
+}
+
+// ------------------------------------------------------------------ pre-split kernels
+__device__ __forceinline__ void split2(double x, double sig, __half& hi, __half& lo) {
+  const double v = x * sig;
+  hi = __double2half(v);
+  lo = __double2half(v - static_cast<double>(__half2float(hi)));
+}
+
+// max |re|, |im| over a strided complex set -> atomicMax on the bit pattern
+__global__ void absmax_c128_kernel(const double2* __restrict__ a, long long rows, long long cols, long long ld,
+                                   unsigned long long* out) {
+  double m = 0.0;
+  const long long tot = rows * cols;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long r = e % rows, c = e / rows;
+    const double2 v = a[r + c * ld];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __double_as_longlong(m));
+}
+__global__ void absmax_f64_rows_kernel(const double* __restrict__ a, long long n, long long stride, int nrow,
+                                       unsigned long long* out) {
+  // out[r] = max_i |a[r*stride + i]| for i < n
+  const int r = blockIdx.y;
+  double m = 0.0;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x)
+    m = fmax(m, fabs(a[r * stride + i]));
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && r < nrow) atomicMax(out + r, __double_as_longlong(m));
+}
+// power-of-two scales: sigma = 2^(target - ceil(log2(max)))
+__global__ void make_scales_kernel(const unsigned long long* mx, double* scales, int n, int target0, int target_rest) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double m = __longlong_as_double(static_cast<long long>(mx[i]));
+  const int t = (i < 2) ? target0 : target_rest;
+  int e = 0;
+  if (m > 0.0 && isfinite(m)) { frexp(m, &e); }      // m = f * 2^e, f in [0.5, 1)
+  scales[i] = ldexp(1.0, t - e);
+}
+
+// A' of the M-doubled real GEMM from a complex getter, into
+// [slice][slot*T + t][half][64][Kp] FP16 (slice 0 = hi, 1 = lo).
+// getter 0 (chi0): a(m, k) = conj(Z[m + k*ld]);  getter 1 (Sigma_c): a(m, k) = conj(W_slot[k + m*ld]).
+template <int GET>
+__global__ void presplit_a_kernel(__half* __restrict__ out, const double2* __restrict__ src, long long ld,
+                                  long long slot_stride, int M, long long K, int T, int nslot, long long Kp,
+                                  const double* __restrict__ scales, long long slice_elems, int slot_out0 = 0) {
+  const double sig = scales[0];
+  const long long per_slot = static_cast<long long>(T) * 64 * (Kp / 2);
+  const long long tot = per_slot * nslot;      // one thread per (slot, t, mm, k)
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    long long r = e;
+    const long long k = r % (Kp / 2); r /= (Kp / 2);
+    const int mm = static_cast<int>(r % 64); r /= 64;
+    const int t = static_cast<int>(r % T);
+    const int slot = static_cast<int>(r / T);
+    const int m = t * 64 + mm;
+    double ar = 0.0, ai = 0.0;
+    if (m < M && k < K) {
+      double2 v;
+      if (GET == 0) v = src[m + k * ld];
+      else v = src[slot * slot_stride + k + static_cast<long long>(m) * ld];
+      ar = v.x; ai = -v.y;     // a = conj(v)
+    }
+    const long long row0 = ((static_cast<long long>(slot + slot_out0) * T + t) * 2 + 0) * 64 + mm;
+    const long long row1 = row0 + 64;
+    __half h, l;
+    // half 0: [Re a, -Im a]; half 1: [Im a, Re a]
+    split2(ar, sig, h, l); out[row0 * Kp + 2 * k] = h; out[slice_elems + row0 * Kp + 2 * k] = l;
+    split2(-ai, sig, h, l); out[row0 * Kp + 2 * k + 1] = h; out[slice_elems + row0 * Kp + 2 * k + 1] = l;
+    split2(ai, sig, h, l); out[row1 * Kp + 2 * k] = h; out[slice_elems + row1 * Kp + 2 * k] = l;
+    split2(ar, sig, h, l); out[row1 * Kp + 2 * k + 1] = h; out[slice_elems + row1 * Kp + 2 * k + 1] = l;
+  }
+}
+
+// B source rows (K-major): row r = column cols[r] of Z (k contiguous), [Re b, Im b] per k,
+// into [slice][rows_pad][Kp]; cols == nullptr means row r = column r.
+__global__ void presplit_s_kernel(__half* __restrict__ out, const double2* __restrict__ z, long long ld, long long K,
+                                  const int* __restrict__ cols, long long nrows, long long ncols_valid, long long Kp,
+                                  const double* __restrict__ scales, long long slice_elems) {
+  const double sig = scales[1];
+  const long long tot = nrows * (Kp / 2);
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long k = e % (Kp / 2), r = e / (Kp / 2);
+    const long long c = cols ? cols[r] : (r < ncols_valid ? r : -1);
+    double br = 0.0, bi = 0.0;
+    if (c >= 0 && k < K) {
+      const double2 v = z[k + c * ld];
+      br = v.x; bi = v.y;
+    }
+    __half h, l;
+    split2(br, sig, h, l); out[r * Kp + 2 * k] = h; out[slice_elems + r * Kp + 2 * k] = l;
+    split2(bi, sig, h, l); out[r * Kp + 2 * k + 1] = h; out[slice_elems + r * Kp + 2 * k + 1] = l;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
+static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides_bytes,
+                    const cuuint32_t* box) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return QSGW_ERR_CUDA;
+  }
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) {
+    set_error("tensor map base is not 16-byte aligned");
+    return QSGW_ERR_ARG;
+  }
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, rank, base, dims, strides_bytes, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", static_cast<int>(r));
+    return QSGW_ERR_CUDA;
+  }
+  return QSGW_OK;
+}
+
+static DevBuf g_a, g_s, g_mx, g_sc, g_tabs;
+static bool g_attr = false;
+
+static int launch_split(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s,
+                        const char* tag) {
+  if (!g_attr) {
+    QSGW_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    g_attr = true;
+  }
+  const int pi = prof_begin(tag, s);
+  split_gemm_kernel<<<grid, NTHREADS, SMEM_BYTES, s>>>(ma, ms, p);
+  prof_end(pi, s);
+  count_launch();
+  QSGW_LAUNCH_CHECK("split_gemm_kernel");
+  return QSGW_OK;
+}
+
+static int grid1(long long n) {
+  return static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 32LL * ctx().sm_count)));
+}
+
+}  // namespace tc
+
+using namespace tc;
+
+int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ldz, long long npair, const double* w,
+                   cudaStream_t s) {
+  const int T = (npr + BMC - 1) / BMC;             // 64-row tiles of the basis
+  const int Tn = (npr + NC - 1) / NC;              // 128-column tiles
+  const long long Kp = ((2 * npair + KC - 1) / KC) * KC;
+  // the S view reads pairs of A' tiles, so give A' an even tile count covering Tn*2
+  const int Ta = std::max(T, 2 * Tn);
+  const long long slice_elems = static_cast<long long>(Ta) * 128 * Kp;
+  int rc = g_a.ensure(2 * slice_elems * sizeof(__half));
+  if (rc) return rc;
+  rc = g_mx.ensure((2 + niw) * sizeof(unsigned long long));
+  if (rc) return rc;
+  rc = g_sc.ensure((2 + niw) * sizeof(double));
+  if (rc) return rc;
+  unsigned long long* mx = g_mx.as<unsigned long long>();
+  QSGW_CUDA(cudaMemsetAsync(mx, 0, (2 + niw) * sizeof(unsigned long long), s));
+  absmax_c128_kernel<<<grid1(static_cast<long long>(npr) * npair), 256, 0, s>>>(zcols, npr, npair, ldz, mx);
+  count_launch();
+  QSGW_LAUNCH_CHECK("absmax_c128_kernel");
+  QSGW_CUDA(cudaMemcpyAsync(mx + 1, mx, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s));
+  absmax_f64_rows_kernel<<<dim3(64, niw), 256, 0, s>>>(w, npair, npair, niw, mx + 2);
+  count_launch();
+  QSGW_LAUNCH_CHECK("absmax_f64_rows_kernel");
+  // A', S magnitudes <= 2^14; B' = S * w * sigma_B <= 2^15
+  make_scales_kernel<<<(2 + niw + 63) / 64, 64, 0, s>>>(mx, g_sc.as<double>(), 2 + niw, 14, 1);
+  count_launch();
+  QSGW_LAUNCH_CHECK("make_scales_kernel");
+  __half* a = g_a.as<__half>();
+  QSGW_CUDA(cudaMemsetAsync(a, 0, 2 * slice_elems * sizeof(__half), s));
+  presplit_a_kernel<0><<<grid1(static_cast<long long>(T) * 64 * (Kp / 2)), 256, 0, s>>>(
+      a, zcols, ldz, 0, npr, npair, T, 1, Kp, g_sc.as<double>(), slice_elems);
+  count_launch();
+  QSGW_LAUNCH_CHECK("presplit_a_kernel");
+  // maps: A' [Kp, 64, 2, 2*Ta] (hi tiles 0..Ta-1, lo tiles Ta..2Ta-1) box {64,64,2,1};
+  //       S  same memory, half 0 of two consecutive tiles: box {64,64,1,2}
+  CUtensorMap ma, ms;
+  const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(2 * Ta)};
+  const cuuint64_t str[3] = {static_cast<cuuint64_t>(Kp * 2), static_cast<cuuint64_t>(Kp * 2 * 64),
+                             static_cast<cuuint64_t>(Kp * 2 * 128)};
+  const cuuint32_t boxa[4] = {KC, 64, 2, 1};
+  const cuuint32_t boxs[4] = {KC, 64, 1, 2};
+  rc = make_map(&ma, a, 4, dims, str, boxa);
+  if (rc) return rc;
+  rc = make_map(&ms, a, 4, dims, str, boxs);
+  if (rc) return rc;
+  Params p{};
+  p.mode = MODE_CHI0;
+  p.M = npr; p.N = npr;
+  p.ntm = T; p.ntn = Tn;
+  p.tiles_per_slot = Ta;
+  p.lo_tile_off = Ta;                       // lo slice = tiles Ta..2Ta-1 of the same map
+  p.lo_row_off = Ta;
+  p.J = 4;
+  p.kch_total = static_cast<int>(Kp / KC);
+  p.w = w; p.npair = npair; p.niw = niw;
+  p.C = chi0; p.ldc = npr; p.c_bs = static_cast<long long>(npr) * npr;
+  p.scales = g_sc.as<double>();
+  p.err = ctx().d_flags + 1;
+  const int ngroups = (niw + p.J - 1) / p.J;
+  const long long units = static_cast<long long>(T) * Tn * ngroups;
+  const long long slots = ctx().sm_count;
+  // enough CTAs to fill the GPU, and at most ~1536 chunks accumulated in FP32 per CTA
+  int splitk = static_cast<int>(std::max<long long>(1, (4 * slots + units - 1) / units));
+  splitk = std::max(splitk, (p.kch_total + 1535) / 1536);
+  splitk = std::min(splitk, std::max(1, p.kch_total / 16));
+  p.kch_per_split = (p.kch_total + splitk - 1) / splitk;
+  splitk = (p.kch_total + p.kch_per_split - 1) / p.kch_per_split;
+  dim3 grid(static_cast<unsigned>(T * Tn), ngroups, splitk);
+  return launch_split(ma, ms, p, grid, s, "chi0_tc");
+}
+
+int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
+  const int ngb = a.ngb;
+  const int T = (ngb + BMC - 1) / BMC;
+  const long long Kp = ((2LL * ngb + KC - 1) / KC) * KC;
+  const int nslot = a.nimag + a.nreal;
+  const int ntiles = static_cast<int>(a.tile_group.size());
+  const long long nrows = static_cast<long long>(ntiles) * NC;
+  const long long slice_a = static_cast<long long>(nslot) * T * 128 * Kp;
+  const long long slice_s = nrows * Kp;
+  int rc = g_a.ensure(2 * slice_a * sizeof(__half));
+  if (rc) return rc;
+  rc = g_s.ensure(2 * slice_s * sizeof(__half));
+  if (rc) return rc;
+  rc = g_mx.ensure(3 * sizeof(unsigned long long));
+  if (rc) return rc;
+  rc = g_sc.ensure(3 * sizeof(double));
+  if (rc) return rc;
+  unsigned long long* mx = g_mx.as<unsigned long long>();
+  QSGW_CUDA(cudaMemsetAsync(mx, 0, 3 * sizeof(unsigned long long), s));
+  // magnitudes: W stack (sigma_A), zmel (sigma_S), every weight (sigma_B)
+  absmax_c128_kernel<<<grid1(static_cast<long long>(ngb) * ngb * a.nimag), 256, 0, s>>>(
+      a.wi, ngb, static_cast<long long>(ngb) * a.nimag, a.ldw, mx);
+  count_launch();
+  if (a.nreal > 0) {
+    absmax_c128_kernel<<<grid1(static_cast<long long>(ngb) * ngb * a.nreal), 256, 0, s>>>(
+        a.wr, ngb, static_cast<long long>(ngb) * a.nreal, a.ldw, mx);
+    count_launch();
+  }
+  absmax_c128_kernel<<<grid1(static_cast<long long>(ngb) * a.ncol), 256, 0, s>>>(a.zmel, ngb, a.ncol, ngb, mx + 1);
+  count_launch();
+  absmax_f64_rows_kernel<<<dim3(64, 1), 256, 0, s>>>(a.wgt, a.nwgt, 0, 1, mx + 2);
+  count_launch();
+  if (a.nw3 > 0) {
+    absmax_f64_rows_kernel<<<dim3(16, 1), 256, 0, s>>>(a.w3, a.nw3, 0, 1, mx + 2);
+    count_launch();
+  }
+  make_scales_kernel<<<1, 64, 0, s>>>(mx, g_sc.as<double>(), 3, 14, 1);
+  count_launch();
+  QSGW_LAUNCH_CHECK("sigc split scales");
+  // pre-split A' slots: imag W first, then the symmetrised real-axis records
+  __half* A = g_a.as<__half>();
+  presplit_a_kernel<1><<<grid1(static_cast<long long>(a.nimag) * T * 64 * (Kp / 2)), 256, 0, s>>>(
+      A, a.wi, a.ldw, a.ldw * a.ldw, ngb, ngb, T, a.nimag, Kp, g_sc.as<double>(), slice_a, 0);
+  count_launch();
+  if (a.nreal > 0) {
+    presplit_a_kernel<1><<<grid1(static_cast<long long>(a.nreal) * T * 64 * (Kp / 2)), 256, 0, s>>>(
+        A, a.wr, a.ldw, a.ldw * a.ldw, ngb, ngb, T, a.nreal, Kp, g_sc.as<double>(), slice_a, a.nimag);
+    count_launch();
+  }
+  // B source rows in tile order (tile_cols, -1 = zero row)
+  rc = g_tabs.ensure((a.tile_cols.size() + a.tile_group.size() + a.group_seg_off.size() + a.group_nseg.size() +
+                      a.seg_slot.size() + 16) * sizeof(int) + a.segs.size() * sizeof(ZSeg) + 256);
+  if (rc) return rc;
+  unsigned char* tb = g_tabs.as<unsigned char>();
+  size_t off = 0;
+  int cprc = 0;
+  auto put = [&](const void* src, size_t n) -> const void* {
+    void* dst = tb + off;
+    if (!cprc && n) cprc = check_cuda(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s), "H2D split tables");
+    off += (n + 15) & ~size_t(15);
+    return dst;
+  };
+  const ZSeg* d_segs = reinterpret_cast<const ZSeg*>(put(a.segs.data(), a.segs.size() * sizeof(ZSeg)));
+  const int* d_cols = reinterpret_cast<const int*>(put(a.tile_cols.data(), a.tile_cols.size() * sizeof(int)));
+  const int* d_tg = reinterpret_cast<const int*>(put(a.tile_group.data(), a.tile_group.size() * sizeof(int)));
+  const int* d_gso = reinterpret_cast<const int*>(put(a.group_seg_off.data(), a.group_seg_off.size() * sizeof(int)));
+  const int* d_gns = reinterpret_cast<const int*>(put(a.group_nseg.data(), a.group_nseg.size() * sizeof(int)));
+  const int* d_slot = reinterpret_cast<const int*>(put(a.seg_slot.data(), a.seg_slot.size() * sizeof(int)));
+  if (cprc) return cprc;
+  __half* S = g_s.as<__half>();
+  presplit_s_kernel<<<grid1(nrows * (Kp / 2)), 256, 0, s>>>(S, a.zmel, ngb, ngb, d_cols, nrows, 0, Kp,
+                                                            g_sc.as<double>(), slice_s);
+  count_launch();
+  QSGW_LAUNCH_CHECK("sigc presplit");
+  CUtensorMap ma, ms;
+  const cuuint64_t dima[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(2LL * nslot * T)};
+  const cuuint64_t stra[3] = {static_cast<cuuint64_t>(Kp * 2), static_cast<cuuint64_t>(Kp * 2 * 64),
+                              static_cast<cuuint64_t>(Kp * 2 * 128)};
+  const cuuint32_t boxa[4] = {KC, 64, 2, 1};
+  rc = make_map(&ma, A, 4, dima, stra, boxa);
+  if (rc) return rc;
+  const cuuint64_t dims_[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(2 * nrows)};
+  const cuuint64_t strs[1] = {static_cast<cuuint64_t>(Kp * 2)};
+  const cuuint32_t boxs[2] = {KC, NC};
+  rc = make_map(&ms, S, 2, dims_, strs, boxs);
+  if (rc) return rc;
+  Params p{};
+  p.mode = MODE_SEG;
+  p.M = ngb; p.N = 0;
+  p.ntm = T; p.ntn = ntiles;
+  p.J = 1;
+  p.cps = static_cast<int>(Kp / KC);
+  p.kch_total = 0; p.kch_per_split = 0;
+  p.tile_group = d_tg; p.tile_cols = d_cols; p.group_seg_off = d_gso; p.group_nseg = d_gns;
+  p.seg_slot = d_slot; p.segs = d_segs;
+  p.tiles_per_slot = T;
+  p.lo_tile_off = nslot * T;
+  p.lo_row_off = static_cast<int>(nrows);
+  p.C = a.out; p.ldc = ngb; p.c_bs = 0;
+  p.scales = g_sc.as<double>();
+  p.err = ctx().d_flags + 1;
+  QSGW_CUDA(cudaMemsetAsync(a.out, 0, static_cast<size_t>(ngb) * a.ncol * sizeof(double2), s));
+  dim3 grid(static_cast<unsigned>(T * ntiles), 1, 1);
+  return launch_split(ma, ms, p, grid, s, "sigc_seg_tc");
 }
 
 }  // namespace qsgw

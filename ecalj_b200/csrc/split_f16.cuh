@@ -1,5 +1,6 @@
 // Split-FP16 (Ozaki-style) complex contractions on the tcgen05 tensor cores.
 #pragma once
+#include <vector>
 #include "zgemm_f64.cuh"
 
 namespace qsgw {
@@ -9,8 +10,21 @@ namespace qsgw {
 int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ldz,
                    long long npair, const double* w, cudaStream_t s);
 
-// Sigma_c segmented contraction (same problem description as the FP64
-// ZM_SEG launch): C(:, col) = sum_seg op(A_seg) * s_seg(col) * Z(:, col).
-int sigc_seg_split_f16(const ZParams& p, int ncol_tiles, cudaStream_t s);
+// Sigma_c imaginary-axis + pole contraction (the segmented problem of the
+// FP64 ZM_SEG launch) in split FP16:  out(:, col) = sum over the segments of
+// the column's group of  W_slot^H (scale_seg(col) z_col).
+struct SigcSplitArgs {
+  int ngb;
+  long long ldw;                       // leading dimension of every W record
+  const double2* wi; int nimag;        // imaginary-axis stack (slots 0..nimag-1)
+  const double2* wr; int nreal;        // symmetrised real-axis records (slots nimag..)
+  const double2* zmel; long long ncol; // zmel columns (ngb each)
+  const double* wgt; long long nwgt;   // every imaginary weight (for the scale)
+  const double* w3; long long nw3;     // every pole weight
+  std::vector<int> tile_cols, tile_group, group_seg_off, group_nseg, seg_slot;  // 128-column tiles
+  std::vector<ZSeg> segs;
+  double2* out;                        // (ngb, ncol), overwritten
+};
+int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s);
 
 }  // namespace qsgw
