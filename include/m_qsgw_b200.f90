@@ -1,0 +1,76 @@
+! ISO_C_BINDING interface to libqsgw_b200 (include/qsgw_b200.h) for ecalj's
+! own drivers.  Selected in place of the m_blas / m_lapack aliases by a
+! -D__B200 build; every function returns 0 or a negative qsgw_status.
+module m_qsgw_b200
+  use, intrinsic :: iso_c_binding
+  implicit none
+  integer(c_int), parameter :: QSGW_PREC_FP64 = 0, QSGW_PREC_SPLIT_F16 = 1
+  type, bind(C) :: qsgw_sxcf_args
+    integer(c_int) :: ngb, nblochpmx, ns1, ns2, ns2r, ntqxx, ntq, niw, nw, nwxi, nwx, nctot, nekc, keepwv
+    real(c_double) :: ef, esmr, wkkr, ua
+    type(c_ptr) :: omega, ekc, freqx, wwx, expa, freq_r
+    type(c_ptr) :: zmel, wc_imag, wc_real, zsec
+  end type
+  interface
+    integer(c_int) function qsgw_init(device) bind(C, name='qsgw_init')
+      import :: c_int
+      integer(c_int), value :: device
+    end function
+    integer(c_int) function qsgw_finalize() bind(C, name='qsgw_finalize')
+      import :: c_int
+    end function
+    integer(c_int) function qsgw_synchronize() bind(C, name='qsgw_synchronize')
+      import :: c_int
+    end function
+    integer(c_int) function qsgw_set_precision(mode, nslices) bind(C, name='qsgw_set_precision')
+      import :: c_int
+      integer(c_int), value :: mode, nslices
+    end function
+    integer(c_int) function qsgw_last_error(buf, len) bind(C, name='qsgw_last_error')
+      import :: c_int, c_char
+      character(kind=c_char) :: buf(*)
+      integer(c_int), value :: len
+    end function
+    integer(c_int) function qsgw_zmm_d(a, b, c, m, n, k, opa, opb, alpha, beta, lda, ldb, ldc) &
+         bind(C, name='qsgw_zmm_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: a, b, c
+      integer(c_int), value :: m, n, k, opa, opb, lda, ldb, ldc
+      real(c_double), intent(in) :: alpha(2), beta(2)
+    end function
+    integer(c_int) function qsgw_zminv_hpd_batched_d(a, n, lda, nbatch) bind(C, name='qsgw_zminv_hpd_batched_d')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: a
+      integer(c_int), value :: n, lda, nbatch
+    end function
+    integer(c_int) function qsgw_x0gemm_d(rcxq, npr, ipr_col, npr_col, nwhis, npm, ns1, ns2, &
+         zmel, nbb, nm1, nm2, nqtot, icounkmink, icounkmaxk, itc, itpc, jpmc, iwini, iwend, &
+         icouini, whwc, ncount) bind(C, name='qsgw_x0gemm_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: rcxq, zmel
+      integer(c_int), value :: npr, ipr_col, npr_col, nwhis, npm, ns1, ns2, nbb, nm1, nm2, nqtot
+      integer(c_int), value :: icounkmink, icounkmaxk, ncount
+      integer(c_int), intent(in) :: itc(*), itpc(*), jpmc(*), iwini(*), iwend(*), icouini(*)
+      real(c_double), intent(in) :: whwc(*)
+    end function
+    integer(c_int) function qsgw_chi0_lorentz_d(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, &
+         zcols, ldz) bind(C, name='qsgw_chi0_lorentz_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: chi0, zcols
+      integer(c_int), value :: npr, niw, nk, ldz
+      real(c_double), intent(in) :: freq_i(*), eocc(*), eunocc(*)
+      integer(c_int), intent(in) :: nocc(*), nun(*)
+    end function
+    integer(c_int) function qsgw_wvi_llw_d(zxqi, ngb, niw, nspin, vcousq, m2e, is_x0_m_basis, &
+         is_wc_m_basis, iq, zw, nblochpmx) bind(C, name='qsgw_wvi_llw_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: zxqi, m2e, zw
+      integer(c_int), value :: ngb, niw, nspin, is_x0_m_basis, is_wc_m_basis, iq, nblochpmx
+      real(c_double), intent(in) :: vcousq(*)
+    end function
+    integer(c_int) function qsgw_sxcf_correlation_d(args) bind(C, name='qsgw_sxcf_correlation_d')
+      import :: c_int, qsgw_sxcf_args
+      type(qsgw_sxcf_args), intent(in) :: args
+    end function
+  end interface
+end module m_qsgw_b200
