@@ -122,6 +122,24 @@ int zminv_hpd_batched(double2* A, int n, long long lda, long long a_bs, int nbat
   return QSGW_OK;
 }
 
+// Same blocked Gauss-Jordan with caller-provided panel scratch (rb, qb: each
+// n*32*nbatch complex) and status word; allocates nothing.
+int zminv_hpd_batched_explicit(double2* A, int n, long long lda, long long a_bs, int nbatch, double2* rb,
+                               double2* qb, int* flag, cudaStream_t s) {
+  if (n <= 0 || nbatch <= 0) return QSGW_OK;
+  const dim3 pg((n + 63) / 64, nbatch);
+  for (int c0 = 0; c0 < n; c0 += GJ_NB) {
+    const int w = std::min(GJ_NB, n - c0);
+    gj_panel_kernel<<<pg, 256, 0, s>>>(A, n, lda, a_bs, rb, qb, c0, w, flag);
+    count_launch();
+    QSGW_LAUNCH_CHECK("gj_panel_kernel");
+    int rc = zgemm_f64(0, 0, n, n, w, make_double2(-1.0, 0.0), rb, n, static_cast<long long>(n) * GJ_NB, qb,
+                       GJ_NB, static_cast<long long>(n) * GJ_NB, make_double2(1.0, 0.0), A, lda, a_bs, nbatch, s);
+    if (rc) return rc;
+  }
+  return QSGW_OK;
+}
+
 // eps~(i,j) = delta_ij - v_i chi(i,j) v_j on the (ngb-ix) x (ngb-ix) block (m_llw.f90:341-348)
 __global__ void eps_build_kernel(double2* __restrict__ eps, const double2* __restrict__ chi,
                                  const double* __restrict__ v, int ngb, int ix, long long ldchi,

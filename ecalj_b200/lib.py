@@ -60,6 +60,7 @@ _SIGS = {
     "qsgw_zmm": [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_dp, c_dp, c_int, c_int, c_int],
     "qsgw_zmm_d": [c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int, c_dp, c_dp, c_int, c_int, c_int],
     "qsgw_zminv_hpd_batched_d": [c_vp, c_int, c_int, c_int],
+    "qsgw_zminv_hpd_batched_noalloc_d": [c_vp, c_int, c_int, c_int, c_vp],
     "qsgw_x0gemm": [c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_int, c_int,
                     c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int],
     "qsgw_x0gemm_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_int, c_int,
@@ -200,6 +201,12 @@ def zmm(a, b, c, m, n, k, opa=0, opb=0, alpha=1.0, beta=0.0, lda=None, ldb=None,
 
 def zminv_hpd_batched_d(a, n, lda, nbatch):
     _chk(load().qsgw_zminv_hpd_batched_d(_p(a), n, lda, nbatch))
+
+
+def zminv_hpd_batched_noalloc_d(a, n, lda, nbatch, stream=None):
+    """Allocation-free batched HPD inverse (static device scratch, n*nbatch <=
+    16384); synchronous on ``stream`` (a raw cudaStream_t handle, None = 0)."""
+    _chk(load().qsgw_zminv_hpd_batched_noalloc_d(_p(a), n, lda, nbatch, stream))
 
 
 # ---------------------------------------------------------------- chi0

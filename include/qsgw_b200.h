@@ -86,6 +86,22 @@ int qsgw_zmm_d(const double *a, const double *b, double *c, int m, int n,
  * Returns QSGW_ERR_NUMERIC (after the batch completes) if a pivot block is
  * not invertible.                                                          */
 int qsgw_zminv_hpd_batched_d(double *a, int n, int lda, int nbatch);
+/* The same inverse without any device allocation (no counterpart in the
+ * reference; it is an addition of this library).  For callers that cannot
+ * call cudaMalloc at this point: a driver that already keeps the device full
+ * with resident W(iw) stacks (the reference's --keepwv mode does this, and
+ * hvccfp0 sleeps and retries when device memory runs out), or a caller whose
+ * stream pipeline must not meet the implicit device synchronisation of
+ * cudaMalloc / cudaFree.  Needs no qsgw_init; runs on the current device and
+ * on `stream` (a cudaStream_t, 0 = default stream) and returns when the batch
+ * is done.  Limit: n * nbatch <= 16384 (larger sizes return QSGW_ERR_ARG).
+ * The Gauss-Jordan panels and the status word live in one static device
+ * array of 16 MiB that every GPU loading the library holds until exit; the
+ * first call on a device looks up that array's device address, so make the
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race and must not be issued concurrently.        */
+int qsgw_zminv_hpd_batched_noalloc_d(double *a, int n, int lda, int nbatch,
+                                     void *stream);
 
 /* ---- chi0 rank-k accumulation: drop-in for x0gemm (x0gemm.f90:2-97) ----
  * rcxq(npr, npr_col, (1-npm)*nwhis : nwhis) += sum over pairs of
