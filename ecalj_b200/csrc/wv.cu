@@ -324,6 +324,7 @@ extern "C" int qsgw_wvi_llw(double* zxqi, int ngb, int niw, int nspin, const dou
   QSGW_CUDA(cudaMemcpyAsync(&flag, ctx().d_flags, sizeof(int), cudaMemcpyDeviceToHost, s));
   QSGW_CUDA(cudaStreamSynchronize(s));
   if (flag) {
+    QSGW_CUDA(cudaMemset(ctx().d_flags, 0, sizeof(int)));   // reported here, not again by qsgw_synchronize
     set_error("wvi_llw: eps~ is not positive definite (singular pivot block)");
     return QSGW_ERR_NUMERIC;
   }
