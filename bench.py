@@ -101,9 +101,11 @@ def dist_setup():
 
 
 # ----------------------------------------------------------------------------- workload
-def chi0_config():
+def chi0_config(nk=None):
     from ecalj_b200 import synth
-    c = synth.CONFIGS["c1"]
+    c = dict(synth.CONFIGS["c1"])
+    if nk:
+        c["nk"] = nk
     rng = np.random.default_rng(c["seed"])
     nocc, nun, eocc, eun = synth.chi0_spectrum(rng, c["nk"], c["nocc"], c["nun"])
     mesh = synth.imag_mesh(c["niw"])
@@ -265,10 +267,13 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
+    ap.add_argument("--precision", default="split", choices=["split", "fp64"],
+                    help="headline precision; split also times the FP64 path for the comparison")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--nq", type=int, default=None, help="Sigma_c tasks (default: the configuration's 64)")
+    ap.add_argument("--nk", type=int, default=None, help="k-points of the chi0 part (profiling only)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     log = (lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
@@ -286,13 +291,11 @@ def main():
     lib.init(local)
     lib.set_stream(torch.cuda.current_stream().cuda_stream)
     prec = args.precision
-    if prec == "auto":
-        prec = "fp64"
-    lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
     peaks, peak_src = load_peaks()
 
     # ---- workload set-up (untimed)
-    c1 = chi0_config()
+    lib.set_precision(lib.PREC_FP64)
+    c1 = chi0_config(args.nk)
     N, niw = c1["N"], c1["niw"]
     zc = device_normal_c128(N * c1["npair"], c1["seed"], 1.0 / math.sqrt(N))
     chi = torch.zeros(N * N * niw, dtype=torch.complex128, device="cuda")
@@ -309,37 +312,63 @@ def main():
     def step():
         lib.chi0_lorentz_d(chi, N, niw, c1["freq_i"], c1["nk"], c1["nocc"], c1["nun"], c1["eocc_h"],
                            c1["eun_h"], zc)
+        for t in s["tasks"]:
+            t["zsec"].zero_()
         run_sigc(lib, s)
 
-    # ---- warm-up, then K timed steps bracketed by barrier + synchronize
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    lib.profile(True)
-    l0 = lib.launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    for _ in range(args.steps):
-        step()
-    ev1.record()
-    torch.cuda.synchronize()
-    launches = lib.launch_count() - l0
-    ms = ev0.elapsed_time(ev1) / args.steps
-    kt = {tag: lib.profile_get(tag) for tag in ("chi0_dmma", "sigc_seg_dmma", "gemm_dmma", "chi0_tc",
-                                               "sigc_seg_tc")}
-    lib.profile(False)
-    clocks = sampler.stop()
-    if ws > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-        dist.barrier()
+    def timed(mode, steps, warmup, sample_clocks):
+        lib.set_precision(lib.PREC_SPLIT_F16 if mode == "split" else lib.PREC_FP64)
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+        lib.profile(True)
+        l0 = lib.launch_count()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(steps):
+            step()
+        ev1.record()
+        torch.cuda.synchronize()
+        launches = lib.launch_count() - l0
+        ms = ev0.elapsed_time(ev1) / steps
+        kt = {tag: lib.profile_get(tag) for tag in ("chi0_dmma", "sigc_seg_dmma", "gemm_dmma", "chi0_tc",
+                                                   "sigc_seg_tc")}
+        lib.profile(False)
+        clocks = sampler.stop() if sampler else None
+        if ws > 1:
+            tt = torch.tensor([ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+            dist.barrier()
+        return ms, kt, launches, clocks
+
+    # ---- headline run
+    ms, kt, launches, clocks = timed(prec, args.steps, args.warmup, True)
     value = ws * flops / (ms * 1e-3) / 1e9
+    chi_main = chi.clone()
+    zsec_main = [t["zsec"].clone() for t in s["tasks"]]
+
+    # ---- the other precision, same workload, same run (the metric compares them)
+    compare = None
+    if prec == "split" and not args.no_compare:
+        ms64, kt64, _, _ = timed("fp64", max(1, min(args.steps, 2)), 1, False)
+        d_chi = float(torch.linalg.vector_norm(chi_main - chi) / torch.linalg.vector_norm(chi))
+        num = sum(float(torch.linalg.vector_norm(a - t["zsec"]) ** 2) for a, t in zip(zsec_main, s["tasks"]))
+        den = sum(float(torch.linalg.vector_norm(t["zsec"]) ** 2) for t in s["tasks"])
+        qp = max(float(torch.max(torch.abs(torch.real(a - t["zsec"]).view(s["ntq"], s["ntq"]).diagonal())))
+                 for a, t in zip(zsec_main, s["tasks"])) * 27211.386245988
+        compare = {"fp64_ms_per_step": round(ms64, 3), "fp64_value": round(ws * flops / (ms64 * 1e-3) / 1e9, 3),
+                   "speedup_split_vs_fp64": round(ms64 / ms, 3),
+                   "fp64_kernel_ms": {k: round(v[0] / max(1, min(args.steps, 2)), 3) for k, v in kt64.items() if v[1]},
+                   "chi0_rel_err_vs_fp64": d_chi, "sigc_rel_err_vs_fp64": math.sqrt(num / den),
+                   "qp_err_mev_max": qp}
+        lib.set_precision(lib.PREC_SPLIT_F16)
 
     # ---- roofline of the dominant kernel
     if prec == "split":
@@ -365,6 +394,7 @@ def main():
     # ---- end-to-end through the host-pointer entry points (pinned host buffers)
     e2e = None
     if not args.no_e2e:
+        lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
         e2e = run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist)
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -374,7 +404,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "c128" if prec == "fp64" else "c128 via split-f16",
                 "data": "synthetic",
-                "config": {"workload": "c1 chi0 (N=600, nk=216, nocc=9, nunocc U{100..300}, 24 iw, "
+                "config": {"workload": f"c1 chi0 (N=600, nk={c1['nk']}, nocc=9, nunocc U{{100..300}}, 24 iw, "
                                        f"{c1['npair']} pairs) + c2 Sigma_c ({len(s['tasks'])} tasks, N=600, "
                                        "40x400 states, 24+1 iw, 50-point real mesh)",
                            "precision": prec, "parallelism": f"replicas x{ws}",
@@ -382,7 +412,7 @@ def main():
                            "flops_per_step": flops, "flops_chi0": fl_chi, "flops_sigc": fl_sig},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "kernel_ms": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]},
-                "fp64_peak_tflops": round(fp64_peak, 3)}
+                "fp64_peak_tflops": round(fp64_peak, 3), "compare": compare}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
@@ -436,6 +466,8 @@ def run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist):
     def step():
         lib.chi0_lorentz_d(chi_np, N, niw, c1["freq_i"], c1["nk"], c1["nocc"], c1["nun"], c1["eocc_h"],
                            c1["eun_h"], zc_np, host=True)
+        for d in host["tasks"]:
+            d["zsec"][:] = 0
         run_sigc(lib, s, host=host)
 
     step()
