@@ -35,19 +35,22 @@ constexpr int BMC = 64;                  // complex rows per tile
 constexpr int NC = 128;                  // complex columns per tile (UMMA N)
 constexpr int KC = 64;                   // FP16 elements per chunk along K' (32 complex k)
 constexpr int NSTAGE = 2;
-constexpr int NTHREADS = 192;
+constexpr int NTHREADS = 320;            // warp 0 TMA, 1 MMA, 2..5 converters, 6..9 drain
 constexpr int NCONV = 128;               // converter threads (warps 2..5)
+constexpr int NDRAIN_WARPS = 4;          // drain warps 6..9 (TMEM lane quadrants 2,3,0,1)
+constexpr int DRAIN_PERIOD = 2;          // K chunks per FP32 accumulation run (24 MMAs)
 constexpr int SLICE_A = BM2 * KC * 2;    // 16 KB
 constexpr int SLICE_S = NC * KC * 2;     // 16 KB
 constexpr int SLICE_B = NC * KC * 2;     // 16 KB
 constexpr int OFF_A = 0;
 constexpr int OFF_S = OFF_A + NSTAGE * 2 * SLICE_A;
 constexpr int OFF_B = OFF_S + NSTAGE * 2 * SLICE_S;
-constexpr int OFF_W = OFF_B + 2 * 2 * SLICE_B;          // chi0 weights per B' buffer: 2 x 32 floats
-constexpr int OFF_BAR = OFF_W + 2 * 32 * 4;
-constexpr int NBAR = 2 * NSTAGE + 2 + 2 + 1;
+constexpr int OFF_BAR = OFF_B + 2 * 2 * SLICE_B;
+constexpr int NBAR = 2 * NSTAGE + 2 + 2 + 2 + 2 + 1;
 constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
 constexpr int SMEM_BYTES = OFF_MISC + 64 + 1024;        // + slack for 1024-B alignment
+constexpr uint32_t TMEM_COLS = 512;                      // acc0 [0,128) acc1 [128,256) FP64 sums [256,512)
+constexpr uint32_t FP64_COL = 256;
 constexpr long long WAIT_LIMIT = 1LL << 24;              // bounded spin (several seconds)
 
 enum { MODE_CHI0 = 0, MODE_SEG = 1 };
@@ -56,7 +59,6 @@ struct Params {
   int mode;
   int M, N;                 // complex rows / columns of C
   int ntm, ntn;
-  int J;                    // accumulators per CTA
   int kch_total, kch_per_split, cps;
   // chi0
   const double* w;          // w[iw * npair + p]
@@ -69,6 +71,7 @@ struct Params {
   const int* group_nseg;
   const int* seg_slot;      // A' slot of every segment
   const ZSeg* segs;         // scale pointer / column stride of every segment
+  int herm;                 // chi0: skip tiles above the diagonal, mirror the lower part
   int tiles_per_slot;       // m-tiles of one A' slot
   int lo_tile_off;          // tile offset of the lo slice in the A' map
   int lo_row_off;           // row (2-D) / tile (4-D) offset of the lo slice in the S map
@@ -183,10 +186,46 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};"
+      ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+        "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]),
+        "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]),
+        "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld32w(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // offset of the 16-byte chunk `c` of row `r` inside a 128B-swizzled tile
 __device__ __forceinline__ int sw128_off(int r, int c) { return r * 128 + ((c ^ (r & 7)) << 4); }
 
 // ------------------------------------------------------------------ the kernel
+// One CTA = one output tile (64 complex rows x 128 columns) of one frequency
+// (chi0) or of the Sigma_c column tile, over its K range.  FP32 accumulation
+// in the tensor core truncates, so its error grows with the run length; the
+// MMA thread therefore alternates two TMEM accumulators every DRAIN_PERIOD
+// chunks while four drain warps fold the finished one into FP64 sums kept in
+// TMEM (columns 256..511, two 32-bit words per value).
 __global__ void __launch_bounds__(NTHREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapS,
                       const Params p) {
@@ -195,13 +234,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   unsigned char* sA = sm + OFF_A;
   unsigned char* sS = sm + OFF_S;
   unsigned char* sB = sm + OFF_B;
-
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
-  uint64_t* full = bar;                  // [NSTAGE]
-  uint64_t* empty = bar + NSTAGE;        // [NSTAGE]
-  uint64_t* bfull = bar + 2 * NSTAGE;    // [2]
-  uint64_t* bempty = bfull + 2;          // [2]
-  uint64_t* accfull = bempty + 2;        // [1]
+  uint64_t* full = bar;                  // [NSTAGE] TMA -> MMA, converters
+  uint64_t* empty = bar + NSTAGE;        // [NSTAGE] MMA -> TMA
+  uint64_t* bfull = bar + 2 * NSTAGE;    // [2] converters -> MMA
+  uint64_t* bempty = bfull + 2;          // [2] MMA -> converters
+  uint64_t* accfull = bempty + 2;        // [2] MMA -> drain
+  uint64_t* accempty = accfull + 2;      // [2] drain -> MMA
+  uint64_t* done = accempty + 2;         // [1] every MMA of the CTA retired
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + OFF_MISC);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + OFF_MISC + 8);
 
@@ -209,32 +249,34 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   // ---- work unit
   const int tileid = blockIdx.x;
   const int mt = tileid % p.ntm, nt = tileid / p.ntm;
-  const int jg = blockIdx.y;
+  const int jw = blockIdx.y;                       // chi0: frequency index
   const int split = blockIdx.z;
-  const int J = p.J;
+  if (p.mode == MODE_CHI0 && p.herm && mt * BMC + BMC - 1 < nt * NC) return;   // strictly upper tile
   const int c0 = split * p.kch_per_split;
   const int c1 = min(p.kch_total, c0 + p.kch_per_split);
-  const int nch = c1 - c0;
-  int group = 0, nseg = 0, seg0 = 0;
+  int seg0 = 0, nseg = 0;
   if (p.mode == MODE_SEG) {
-    group = p.tile_group[nt];
+    const int group = p.tile_group[nt];
     nseg = p.group_nseg[group];
     seg0 = p.group_seg_off[group];
   }
-  const int nchunk = (p.mode == MODE_SEG) ? nseg * p.cps : nch;
+  const int nchunk = (p.mode == MODE_SEG) ? nseg * p.cps : max(0, c1 - c0);
   const int cbeg = (p.mode == MODE_SEG) ? 0 : c0;
+  const int nper = (nchunk + DRAIN_PERIOD - 1) / DRAIN_PERIOD;
 
   if (tid == 0) {
     for (int i = 0; i < NSTAGE; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
-    for (int i = 0; i < 2; ++i) { mbar_init(&bfull[i], NCONV); mbar_init(&bempty[i], 1); }
-    mbar_init(accfull, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&bfull[i], NCONV); mbar_init(&bempty[i], 1);
+      mbar_init(&accfull[i], 1); mbar_init(&accempty[i], NDRAIN_WARPS);
+    }
+    mbar_init(done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  const uint32_t ncols = (J * NC <= 128) ? 128 : (J * NC <= 256 ? 256 : 512);
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(ncols));
+                 "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -270,137 +312,154 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           tma_load_2d(s + SLICE_S, &mapS, &full[st], x, p.lo_row_off + nt * NC);
         }
       }
-      // every issued copy has landed before the CTA may exit
       for (int c = max(0, issued - NSTAGE); c < issued; ++c) mbar_drain(&full[c % NSTAGE], (c / NSTAGE) & 1);
     } else if (warp == 1 && lane == 0) {
       // ---------------- MMA issuer
-      int it = 0;
       for (int c = 0; c < nchunk && !*abort_flag; ++c) {
         const int st = c % NSTAGE;
+        const int per = c / DRAIN_PERIOD;
+        const int ab = per & 1;                      // accumulator of this period
+        const bool first_of_period = (c % DRAIN_PERIOD) == 0;
+        if (first_of_period && per >= 2 && !mbar_wait(&accempty[ab], ((per >> 1) - 1) & 1, abort_flag)) break;
         if (!mbar_wait(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
+        const int b = c & 1;                         // B' buffer
+        if (!mbar_wait(&bfull[b], (c >> 1) & 1, abort_flag)) break;
+        tc_fence_after();
         const uint32_t a_hi = smem_u32(sA + st * 2 * SLICE_A), a_lo = a_hi + SLICE_A;
-        bool ok = true;
-        for (int j = 0; j < J; ++j, ++it) {
-          const int b = it & 1;
-          if (!mbar_wait(&bfull[b], (it >> 1) & 1, abort_flag)) { ok = false; break; }
-          tc_fence_after();
-          const uint32_t b_hi = smem_u32(sB + b * 2 * SLICE_B), b_lo = b_hi + SLICE_B;
-          const uint32_t d = tmem + static_cast<uint32_t>(j * NC);
+        const uint32_t b_hi = smem_u32(sB + b * 2 * SLICE_B), b_lo = b_hi + SLICE_B;
+        const uint32_t d = tmem + static_cast<uint32_t>(ab * NC);
 #pragma unroll
-          for (int kk = 0; kk < KC / 16; ++kk) {
-            const uint32_t ko = kk * 32;   // 16 FP16 = 32 B along K
-            const uint32_t acc0 = (c == 0 && kk == 0) ? 0u : 1u;
-            umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_hi + ko), acc0);
-            umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_lo + ko), 1u);
-            umma_f16(d, sw128_desc(a_lo + ko), sw128_desc(b_hi + ko), 1u);
-          }
-          umma_commit(&bempty[b]);
+        for (int kk = 0; kk < KC / 16; ++kk) {
+          const uint32_t ko = kk * 32;               // 16 FP16 = 32 B along K
+          const uint32_t acc0 = (first_of_period && kk == 0) ? 0u : 1u;
+          umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_hi + ko), acc0);
+          umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_lo + ko), 1u);
+          umma_f16(d, sw128_desc(a_lo + ko), sw128_desc(b_hi + ko), 1u);
         }
-        if (!ok) break;
+        umma_commit(&bempty[b]);
         umma_commit(&empty[st]);
+        if ((c % DRAIN_PERIOD) == DRAIN_PERIOD - 1 || c == nchunk - 1) umma_commit(&accfull[ab]);
       }
-      umma_commit(accfull);
-      mbar_drain(accfull, 0);      // all issued MMAs retired
-    } else if (warp >= 2) {
-      // ---------------- converters: B'_j = weight_j * (S_hi + S_lo), re-split
+      // everything issued has retired before TMEM may be freed
+      umma_commit(done);
+      mbar_drain(done, 0);
+    } else if (warp >= 2 && warp < 6) {
+      // ---------------- converters: B' = weight * (S_hi + S_lo), re-split to FP16 hi/lo
       const int ct = tid - 64;                 // 0..127 = row n of the tile
-      int it = 0;
-      double rowscale_seg = 0.0;
       for (int c = 0; c < nchunk; ++c) {
         const int st = c % NSTAGE;
         if (!mbar_wait_warp(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
+        const int b = c & 1;
+        if (c >= 2 && !mbar_wait_warp(&bempty[b], ((c >> 1) - 1) & 1, abort_flag)) break;
         const unsigned char* s_hi = sS + st * 2 * SLICE_S;
         const unsigned char* s_lo = s_hi + SLICE_S;
-        if (p.mode == MODE_SEG) {
+        float wl = 0.f, rs = 1.f;
+        if (p.mode == MODE_CHI0) {
+          // lane i holds the weight of complex k = i of this chunk; shuffled below
+          const long long pr = static_cast<long long>(cbeg + c) * 32 + lane;
+          if (pr < p.npair) wl = static_cast<float>(p.w[static_cast<long long>(jw) * p.npair + pr] * p.scales[2 + jw]);
+        } else {
           const int sg = c / p.cps;
           const int col = p.tile_cols[nt * NC + ct];
           const ZSeg zs = p.segs[seg0 + sg];
-          rowscale_seg = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
+          const double sc = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
+          rs = static_cast<float>(sc * p.scales[2]);
         }
-        bool ok = true;
-        for (int j = 0; j < J; ++j, ++it) {
-          const int b = it & 1;
-          if (it >= 2 && !mbar_wait_warp(&bempty[b], ((it >> 1) - 1) & 1, abort_flag)) { ok = false; break; }
-          float wl = 0.f, rs = 1.f;
-          if (p.mode == MODE_CHI0) {
-            // lane i holds the weight of complex k = i of this chunk; shuffled below
-            const int iw = jg * J + j;
-            const long long pr = static_cast<long long>(cbeg + c) * 32 + lane;
-            if (iw < p.niw && pr < p.npair)
-              wl = static_cast<float>(p.w[static_cast<long long>(iw) * p.npair + pr] * p.scales[2 + iw]);
-          } else {
-            rs = static_cast<float>(rowscale_seg * p.scales[2]);
-          }
-          unsigned char* d_hi = sB + b * 2 * SLICE_B;
-          unsigned char* d_lo = d_hi + SLICE_B;
+        unsigned char* d_hi = sB + b * 2 * SLICE_B;
+        unsigned char* d_lo = d_hi + SLICE_B;
 #pragma unroll
-          for (int ch = 0; ch < 8; ++ch) {
-            const int off = sw128_off(ct, ch);
-            const uint4 vh = *reinterpret_cast<const uint4*>(s_hi + off);
-            const uint4 vl = *reinterpret_cast<const uint4*>(s_lo + off);
-            const __half2* h2 = reinterpret_cast<const __half2*>(&vh);
-            const __half2* l2 = reinterpret_cast<const __half2*>(&vl);
-            uint4 oh, ol;
-            __half2* oh2 = reinterpret_cast<__half2*>(&oh);
-            __half2* ol2 = reinterpret_cast<__half2*>(&ol);
+        for (int ch = 0; ch < 8; ++ch) {
+          const int off = sw128_off(ct, ch);
+          const uint4 vh = *reinterpret_cast<const uint4*>(s_hi + off);
+          const uint4 vl = *reinterpret_cast<const uint4*>(s_lo + off);
+          const __half2* h2 = reinterpret_cast<const __half2*>(&vh);
+          const __half2* l2 = reinterpret_cast<const __half2*>(&vl);
+          uint4 oh, ol;
+          __half2* oh2 = reinterpret_cast<__half2*>(&oh);
+          __half2* ol2 = reinterpret_cast<__half2*>(&ol);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              // the pair (re, im) of complex k = 4*ch + q
-              const float2 fh = __half22float2(h2[q]);
-              const float2 fl = __half22float2(l2[q]);
-              const float wk = __shfl_sync(0xffffffffu, wl, ch * 4 + q);
-              const float f = (p.mode == MODE_CHI0) ? wk : rs;
-              const float v0 = (fh.x + fl.x) * f, v1 = (fh.y + fl.y) * f;
-              const __half2 hi = __floats2half2_rn(v0, v1);
-              const float2 fb = __half22float2(hi);
-              oh2[q] = hi;
-              ol2[q] = __floats2half2_rn(v0 - fb.x, v1 - fb.y);
-            }
-            *reinterpret_cast<uint4*>(d_hi + off) = oh;
-            *reinterpret_cast<uint4*>(d_lo + off) = ol;
+          for (int q = 0; q < 4; ++q) {
+            // the pair (re, im) of complex k = 4*ch + q
+            const float wk = __shfl_sync(0xffffffffu, wl, ch * 4 + q);
+            const float f = (p.mode == MODE_CHI0) ? wk : rs;
+            const float2 fh = __half22float2(h2[q]);
+            const float2 fl = __half22float2(l2[q]);
+            const float v0 = (fh.x + fl.x) * f, v1 = (fh.y + fl.y) * f;
+            const __half2 hi = __floats2half2_rn(v0, v1);
+            const float2 fb = __half22float2(hi);
+            oh2[q] = hi;
+            ol2[q] = __floats2half2_rn(v0 - fb.x, v1 - fb.y);
           }
-          fence_async_smem();
-          mbar_arrive(&bfull[b]);
+          *reinterpret_cast<uint4*>(d_hi + off) = oh;
+          *reinterpret_cast<uint4*>(d_lo + off) = ol;
         }
-        if (!ok) break;
+        fence_async_smem();
+        mbar_arrive(&bfull[b]);
       }
-      // ---------------- epilogue: TMEM -> FP64 atomics
-      if (mbar_wait_warp(accfull, 0, abort_flag)) {
+    } else if (warp >= 6) {
+      // ---------------- drain: FP32 accumulator -> FP64 sums in TMEM, then the output
+      const int quad = warp & 3;                          // TMEM lanes 32*quad .. +31
+      const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
+      bool ok = true;
+      for (int per = 0; per < nper; ++per) {
+        const int ab = per & 1;
+        if (!mbar_wait_warp(&accfull[ab], (per >> 1) & 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
-        const int quad = warp & 3;            // TMEM lanes 32*quad .. 32*quad+31
-        const int row = quad * 32 + lane;     // accumulator row: 0..63 re, 64..127 im
+#pragma unroll 1
+        for (int cb = 0; cb < NC / 16; ++cb) {
+          uint32_t f32[16], f64[32];
+          tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + cb * 16), f32);
+          if (per > 0) tmem_ld32w(tmem + lane_base + FP64_COL + static_cast<uint32_t>(cb * 32), f64);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            double acc = (per > 0) ? __hiloint2double(static_cast<int>(f64[2 * i + 1]), static_cast<int>(f64[2 * i])) : 0.0;
+            acc += static_cast<double>(__uint_as_float(f32[i]));
+            f64[2 * i] = static_cast<uint32_t>(__double2loint(acc));
+            f64[2 * i + 1] = static_cast<uint32_t>(__double2hiint(acc));
+          }
+          tmem_st32(tmem + lane_base + FP64_COL + static_cast<uint32_t>(cb * 32), f64);
+        }
+        tmem_wait_st();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&accempty[ab]);
+      }
+      if (ok && !*abort_flag) {
+        tc_fence_after();
+        const int row = quad * 32 + lane;         // accumulator row: 0..63 re, 64..127 im
         const int m = mt * BMC + (row & 63);
         const bool im_part = row >= 64;
-        const double inv_as = 1.0 / (p.scales[0] * p.scales[1]);
-        for (int j = 0; j < J; ++j) {
-          double inv;
-          double2* Cj;
-          if (p.mode == MODE_CHI0) {
-            const int iw = jg * J + j;
-            if (iw >= p.niw) break;
-            inv = inv_as / p.scales[2 + iw];
-            Cj = p.C + static_cast<long long>(iw) * p.c_bs;
-          } else {
-            inv = inv_as / p.scales[2];
-            Cj = p.C;
-          }
-          for (int cb = 0; cb < NC / 32; ++cb) {
-            float v[32];
-            tmem_ld32(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(j * NC + cb * 32), v);
-            if (m >= p.M) continue;
+        double inv = 1.0 / (p.scales[0] * p.scales[1]);
+        double2* Cj = p.C;
+        if (p.mode == MODE_CHI0) {
+          inv /= p.scales[2 + jw];
+          Cj = p.C + static_cast<long long>(jw) * p.c_bs;
+        } else {
+          inv /= p.scales[2];
+        }
+#pragma unroll 1
+        for (int cb = 0; cb < NC / 16; ++cb) {
+          uint32_t f64[32];
+          tmem_ld32w(tmem + lane_base + FP64_COL + static_cast<uint32_t>(cb * 32), f64);
+          tmem_wait_ld();
+          if (m >= p.M) continue;
 #pragma unroll 4
-            for (int i = 0; i < 32; ++i) {
-              const int nloc = cb * 32 + i;
-              long long col;
-              if (p.mode == MODE_CHI0) {
-                col = nt * NC + nloc;
-                if (col >= p.N) continue;
-              } else {
-                col = p.tile_cols[nt * NC + nloc];
-                if (col < 0) continue;
-              }
-              double* dst = reinterpret_cast<double*>(Cj + m + col * p.ldc) + (im_part ? 1 : 0);
-              atomicAdd(dst, static_cast<double>(v[i]) * inv);
+          for (int i = 0; i < 16; ++i) {
+            const double v = __hiloint2double(static_cast<int>(f64[2 * i + 1]), static_cast<int>(f64[2 * i])) * inv;
+            const int nloc = cb * 16 + i;
+            if (p.mode == MODE_CHI0) {
+              const int n = nt * NC + nloc;
+              if (n >= p.N) continue;
+              if (p.herm && m < n) continue;                // upper part comes from the mirror
+              atomicAdd(reinterpret_cast<double*>(Cj + m + static_cast<long long>(n) * p.ldc) + (im_part ? 1 : 0), v);
+              if (p.herm && m > n)                         // chi0(n, m) = conj(chi0(m, n))
+                atomicAdd(reinterpret_cast<double*>(Cj + n + static_cast<long long>(m) * p.ldc) + (im_part ? 1 : 0),
+                          im_part ? -v : v);
+            } else {
+              const long long col = p.tile_cols[nt * NC + nloc];
+              if (col < 0) continue;
+              atomicAdd(reinterpret_cast<double*>(Cj + m + col * p.ldc) + (im_part ? 1 : 0), v);
             }
           }
         }
@@ -413,7 +472,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (*abort_flag && tid == 0) atomicExch(p.err, 2);
   if (warp == 1) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
   }
 }
 
@@ -634,22 +693,24 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   p.tiles_per_slot = Ta;
   p.lo_tile_off = Ta;                       // lo slice = tiles Ta..2Ta-1 of the same map
   p.lo_row_off = Ta;
-  p.J = 4;
+  p.herm = 1;                               // chi0(iw) is Hermitian: lower tiles + mirror
   p.kch_total = static_cast<int>(Kp / KC);
   p.w = w; p.npair = npair; p.niw = niw;
   p.C = chi0; p.ldc = npr; p.c_bs = static_cast<long long>(npr) * npr;
   p.scales = g_sc.as<double>();
   p.err = ctx().d_flags + 1;
-  const int ngroups = (niw + p.J - 1) / p.J;
-  const long long units = static_cast<long long>(T) * Tn * ngroups;
-  const long long slots = ctx().sm_count;
-  // enough CTAs to fill the GPU, and at most ~1536 chunks accumulated in FP32 per CTA
-  int splitk = static_cast<int>(std::max<long long>(1, (4 * slots + units - 1) / units));
-  splitk = std::max(splitk, (p.kch_total + 1535) / 1536);
-  splitk = std::min(splitk, std::max(1, p.kch_total / 16));
+  // one frequency per CTA; split K only when the tiles alone cannot fill the GPU
+  long long units = 0;
+  for (int nt = 0; nt < Tn; ++nt)
+    for (int mt = 0; mt < T; ++mt)
+      if (mt * BMC + BMC - 1 >= nt * NC) ++units;
+  units *= niw;
+  const long long slots = 2LL * ctx().sm_count;
+  int splitk = static_cast<int>(std::max<long long>(1, (slots + units - 1) / units));
+  splitk = std::min(splitk, std::max(1, p.kch_total / 8));
   p.kch_per_split = (p.kch_total + splitk - 1) / splitk;
   splitk = (p.kch_total + p.kch_per_split - 1) / p.kch_per_split;
-  dim3 grid(static_cast<unsigned>(T * Tn), ngroups, splitk);
+  dim3 grid(static_cast<unsigned>(T * Tn), niw, splitk);
   return launch_split(ma, ms, p, grid, s, "chi0_tc");
 }
 
@@ -743,7 +804,6 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   p.mode = MODE_SEG;
   p.M = ngb; p.N = 0;
   p.ntm = T; p.ntn = ntiles;
-  p.J = 1;
   p.cps = static_cast<int>(Kp / KC);
   p.kch_total = 0; p.kch_per_split = 0;
   p.tile_group = d_tg; p.tile_cols = d_cols; p.group_seg_off = d_gso; p.group_nseg = d_gns;
