@@ -15,10 +15,11 @@
 // the B source are pre-split once into HBM and streamed by TMA; four
 // converter warps apply the weight to the B source in shared memory and
 // re-split it into B' for every frequency / segment, while one thread issues
-// the MMAs.  Warp roles (192 threads, one CTA per SM):
-//     warp 0      TMA producer
-//     warp 1      TMEM owner and MMA issuer
-//     warps 2..5  B' converters, then the epilogue (TMEM -> FP64 atomics)
+// the MMAs.  Warp roles (448 threads, one CTA per SM):
+//     warp 0        TMA producer
+//     warp 1        TMEM owner and MMA issuer
+//     warps 2..9    B' converters (two threads per B' row)
+//     warps 10..13  drain: FP32 accumulators -> FP64 sums in TMEM -> output
 // Every mbarrier wait is bounded; on time-out the CTA records an error,
 // drains its own TMA and MMA work, frees TMEM and exits.
 #include <cuda.h>
@@ -35,9 +36,11 @@ constexpr int BMC = 64;                  // complex rows per tile
 constexpr int NC = 128;                  // complex columns per tile (UMMA N)
 constexpr int KC = 64;                   // FP16 elements per chunk along K' (32 complex k)
 constexpr int NSTAGE = 2;
-constexpr int NTHREADS = 320;            // warp 0 TMA, 1 MMA, 2..5 converters, 6..9 drain
-constexpr int NCONV = 128;               // converter threads (warps 2..5)
-constexpr int NDRAIN_WARPS = 4;          // drain warps 6..9 (TMEM lane quadrants 2,3,0,1)
+constexpr int NTHREADS = 448;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..13 drain
+constexpr int NCONV = 256;               // converter threads (warps 2..9), two per B' row
+constexpr int CONV_W0 = 2, DRAIN_W0 = 10;
+constexpr int NDRAIN_WARPS = 4;          // drain warps 10..13 (TMEM lane quadrants 2,3,0,1)
+constexpr int NBUF = 3;                  // B' buffers
 constexpr int DRAIN_PERIOD = 2;          // K chunks per FP32 accumulation run (24 MMAs)
 constexpr int SLICE_A = BM2 * KC * 2;    // 16 KB
 constexpr int SLICE_S = NC * KC * 2;     // 16 KB
@@ -45,8 +48,8 @@ constexpr int SLICE_B = NC * KC * 2;     // 16 KB
 constexpr int OFF_A = 0;
 constexpr int OFF_S = OFF_A + NSTAGE * 2 * SLICE_A;
 constexpr int OFF_B = OFF_S + NSTAGE * 2 * SLICE_S;
-constexpr int OFF_BAR = OFF_B + 2 * 2 * SLICE_B;
-constexpr int NBAR = 2 * NSTAGE + 2 + 2 + 2 + 2 + 1;
+constexpr int OFF_BAR = OFF_B + NBUF * 2 * SLICE_B;
+constexpr int NBAR = 2 * NSTAGE + 2 * NBUF + 2 + 2 + 1;
 constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
 constexpr int SMEM_BYTES = OFF_MISC + 64 + 1024;        // + slack for 1024-B alignment
 constexpr uint32_t TMEM_COLS = 512;                      // acc0 [0,128) acc1 [128,256) FP64 sums [256,512)
@@ -62,6 +65,8 @@ struct Params {
   int kch_total, kch_per_split, cps;
   // chi0
   const double* w;          // w[iw * npair + p]
+  const float* w32;         // w * sigma_B(iw) in FP32, rows of w32_ld (multiple of 32, zero padded)
+  long long w32_ld;
   long long npair;
   int niw;
   // seg
@@ -237,9 +242,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
   uint64_t* full = bar;                  // [NSTAGE] TMA -> MMA, converters
   uint64_t* empty = bar + NSTAGE;        // [NSTAGE] MMA -> TMA
-  uint64_t* bfull = bar + 2 * NSTAGE;    // [2] converters -> MMA
-  uint64_t* bempty = bfull + 2;          // [2] MMA -> converters
-  uint64_t* accfull = bempty + 2;        // [2] MMA -> drain
+  uint64_t* bfull = bar + 2 * NSTAGE;    // [NBUF] converters -> MMA
+  uint64_t* bempty = bfull + NBUF;       // [NBUF] MMA -> converters
+  uint64_t* accfull = bempty + NBUF;     // [2] MMA -> drain
   uint64_t* accempty = accfull + 2;      // [2] drain -> MMA
   uint64_t* done = accempty + 2;         // [1] every MMA of the CTA retired
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + OFF_MISC);
@@ -266,10 +271,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
   if (tid == 0) {
     for (int i = 0; i < NSTAGE; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
-    for (int i = 0; i < 2; ++i) {
-      mbar_init(&bfull[i], NCONV); mbar_init(&bempty[i], 1);
-      mbar_init(&accfull[i], 1); mbar_init(&accempty[i], NDRAIN_WARPS);
-    }
+    for (int i = 0; i < NBUF; ++i) { mbar_init(&bfull[i], NCONV); mbar_init(&bempty[i], 1); }
+    for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], NDRAIN_WARPS); }
     mbar_init(done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -322,8 +325,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const bool first_of_period = (c % DRAIN_PERIOD) == 0;
         if (first_of_period && per >= 2 && !mbar_wait(&accempty[ab], ((per >> 1) - 1) & 1, abort_flag)) break;
         if (!mbar_wait(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
-        const int b = c & 1;                         // B' buffer
-        if (!mbar_wait(&bfull[b], (c >> 1) & 1, abort_flag)) break;
+        const int b = c % NBUF;                      // B' buffer
+        if (!mbar_wait(&bfull[b], (c / NBUF) & 1, abort_flag)) break;
         tc_fence_after();
         const uint32_t a_hi = smem_u32(sA + st * 2 * SLICE_A), a_lo = a_hi + SLICE_A;
         const uint32_t b_hi = smem_u32(sB + b * 2 * SLICE_B), b_lo = b_hi + SLICE_B;
@@ -343,32 +346,50 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // everything issued has retired before TMEM may be freed
       umma_commit(done);
       mbar_drain(done, 0);
-    } else if (warp >= 2 && warp < 6) {
+    } else if (warp >= CONV_W0 && warp < DRAIN_W0) {
       // ---------------- converters: B' = weight * (S_hi + S_lo), re-split to FP16 hi/lo
-      const int ct = tid - 64;                 // 0..127 = row n of the tile
+      const int ctid = tid - 32 * CONV_W0;     // 0..255
+      const int ct = ctid >> 1;                // row n of the tile
+      const int h = ctid & 1;                  // which four of the eight 16-byte chunks
+      float4 wn[4];                            // chi0: this thread's 16 weights of the next chunk
+      auto load_w = [&](int c, float4 (&wv)[4]) {
+        const long long k0 = static_cast<long long>(cbeg + c) * 32 + h * 16;
+        const float4* src = reinterpret_cast<const float4*>(p.w32 + static_cast<long long>(jw) * p.w32_ld + k0);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) wv[i] = __ldg(src + i);
+      };
+      if (p.mode == MODE_CHI0) load_w(0, wn);
+      int seg_cached = -1;
+      float rs = 0.f;
       for (int c = 0; c < nchunk; ++c) {
         const int st = c % NSTAGE;
+        float4 wc[4];
+        if (p.mode == MODE_CHI0) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) wc[i] = wn[i];
+          if (c + 1 < nchunk) load_w(c + 1, wn);      // prefetch while this chunk converts
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) wc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+          const int sg = c / p.cps;
+          if (sg != seg_cached) {
+            const int col = p.tile_cols[nt * NC + ct];
+            const ZSeg zs = p.segs[seg0 + sg];
+            const double sc = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
+            rs = static_cast<float>(sc * p.scales[2]);
+            seg_cached = sg;
+          }
+        }
         if (!mbar_wait_warp(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
-        const int b = c & 1;
-        if (c >= 2 && !mbar_wait_warp(&bempty[b], ((c >> 1) - 1) & 1, abort_flag)) break;
+        const int b = c % NBUF;
+        if (c >= NBUF && !mbar_wait_warp(&bempty[b], ((c / NBUF) - 1) & 1, abort_flag)) break;
         const unsigned char* s_hi = sS + st * 2 * SLICE_S;
         const unsigned char* s_lo = s_hi + SLICE_S;
-        float wl = 0.f, rs = 1.f;
-        if (p.mode == MODE_CHI0) {
-          // lane i holds the weight of complex k = i of this chunk; shuffled below
-          const long long pr = static_cast<long long>(cbeg + c) * 32 + lane;
-          if (pr < p.npair) wl = static_cast<float>(p.w[static_cast<long long>(jw) * p.npair + pr] * p.scales[2 + jw]);
-        } else {
-          const int sg = c / p.cps;
-          const int col = p.tile_cols[nt * NC + ct];
-          const ZSeg zs = p.segs[seg0 + sg];
-          const double sc = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
-          rs = static_cast<float>(sc * p.scales[2]);
-        }
         unsigned char* d_hi = sB + b * 2 * SLICE_B;
         unsigned char* d_lo = d_hi + SLICE_B;
 #pragma unroll
-        for (int ch = 0; ch < 8; ++ch) {
+        for (int cc = 0; cc < 4; ++cc) {
+          const int ch = h * 4 + cc;
           const int off = sw128_off(ct, ch);
           const uint4 vh = *reinterpret_cast<const uint4*>(s_hi + off);
           const uint4 vl = *reinterpret_cast<const uint4*>(s_lo + off);
@@ -377,11 +398,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           uint4 oh, ol;
           __half2* oh2 = reinterpret_cast<__half2*>(&oh);
           __half2* ol2 = reinterpret_cast<__half2*>(&ol);
+          const float wq[4] = {wc[cc].x, wc[cc].y, wc[cc].z, wc[cc].w};
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             // the pair (re, im) of complex k = 4*ch + q
-            const float wk = __shfl_sync(0xffffffffu, wl, ch * 4 + q);
-            const float f = (p.mode == MODE_CHI0) ? wk : rs;
+            const float f = (p.mode == MODE_CHI0) ? wq[q] : rs;
             const float2 fh = __half22float2(h2[q]);
             const float2 fl = __half22float2(l2[q]);
             const float v0 = (fh.x + fl.x) * f, v1 = (fh.y + fl.y) * f;
@@ -396,7 +417,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         fence_async_smem();
         mbar_arrive(&bfull[b]);
       }
-    } else if (warp >= 6) {
+    } else if (warp >= DRAIN_W0) {
       // ---------------- drain: FP32 accumulator -> FP64 sums in TMEM, then the output
       const int quad = warp & 3;                          // TMEM lanes 32*quad .. +31
       const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
@@ -577,6 +598,18 @@ __global__ void presplit_s_kernel(__half* __restrict__ out, const double2* __res
   }
 }
 
+// w32[iw][p] = w[iw*npair + p] * sigma_B(iw) (FP32), zero beyond npair
+__global__ void scale_weights_kernel(float* __restrict__ w32, const double* __restrict__ w, long long npair,
+                                     long long ld, int niw, const double* __restrict__ scales) {
+  const long long tot = ld * niw;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long pr = e % ld;
+    const int iw = static_cast<int>(e / ld);
+    w32[e] = (pr < npair) ? static_cast<float>(w[iw * npair + pr] * scales[2 + iw]) : 0.f;
+  }
+}
+
 // ------------------------------------------------------------------ host side
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -616,7 +649,7 @@ static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* di
   return QSGW_OK;
 }
 
-static DevBuf g_a, g_s, g_mx, g_sc, g_tabs;
+static DevBuf g_a, g_s, g_mx, g_sc, g_tabs, g_w32;
 static bool g_attr = false;
 
 static int launch_split(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s,
@@ -668,6 +701,13 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   make_scales_kernel<<<(2 + niw + 63) / 64, 64, 0, s>>>(mx, g_sc.as<double>(), 2 + niw, 14, 1);
   count_launch();
   QSGW_LAUNCH_CHECK("make_scales_kernel");
+  const long long w32_ld = Kp / 2;
+  rc = g_w32.ensure(static_cast<size_t>(w32_ld) * niw * sizeof(float));
+  if (rc) return rc;
+  scale_weights_kernel<<<grid1(w32_ld * niw), 256, 0, s>>>(g_w32.as<float>(), w, npair, w32_ld, niw,
+                                                           g_sc.as<double>());
+  count_launch();
+  QSGW_LAUNCH_CHECK("scale_weights_kernel");
   __half* a = g_a.as<__half>();
   QSGW_CUDA(cudaMemsetAsync(a, 0, 2 * slice_elems * sizeof(__half), s));
   presplit_a_kernel<0><<<grid1(static_cast<long long>(T) * 64 * (Kp / 2)), 256, 0, s>>>(
@@ -696,6 +736,7 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   p.herm = 1;                               // chi0(iw) is Hermitian: lower tiles + mirror
   p.kch_total = static_cast<int>(Kp / KC);
   p.w = w; p.npair = npair; p.niw = niw;
+  p.w32 = g_w32.as<float>(); p.w32_ld = w32_ld;
   p.C = chi0; p.ldc = npr; p.c_bs = static_cast<long long>(npr) * npr;
   p.scales = g_sc.as<double>();
   p.err = ctx().d_flags + 1;
