@@ -19,7 +19,7 @@
 //     warp 0        TMA producer
 //     warp 1        TMEM owner and MMA issuer
 //     warps 2..9    B' converters (two threads per B' row)
-//     warps 10..13  drain: FP32 accumulators -> FP64 sums in TMEM -> output
+//     warps 10..17  drain: FP32 accumulators -> FP64 sums in TMEM -> output
 // Every mbarrier wait is bounded; on time-out the CTA records an error,
 // drains its own TMA and MMA work, frees TMEM and exits.
 #include <cuda.h>
@@ -36,10 +36,10 @@ constexpr int BMC = 64;                  // complex rows per tile
 constexpr int NC = 128;                  // complex columns per tile (UMMA N)
 constexpr int KC = 64;                   // FP16 elements per chunk along K' (32 complex k)
 constexpr int NSTAGE = 2;
-constexpr int NTHREADS = 448;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..13 drain
+constexpr int NTHREADS = 576;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..17 drain
 constexpr int NCONV = 256;               // converter threads (warps 2..9), two per B' row
 constexpr int CONV_W0 = 2, DRAIN_W0 = 10;
-constexpr int NDRAIN_WARPS = 4;          // drain warps 10..13 (TMEM lane quadrants 2,3,0,1)
+constexpr int NDRAIN_WARPS = 8;          // drain warps 10..17: two per TMEM lane quadrant, 64 columns each
 constexpr int NBUF = 3;                  // B' buffers
 constexpr int DRAIN_PERIOD = 2;          // K chunks per FP32 accumulation run (24 MMAs)
 constexpr int SLICE_A = BM2 * KC * 2;    // 16 KB
@@ -420,6 +420,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     } else if (warp >= DRAIN_W0) {
       // ---------------- drain: FP32 accumulator -> FP64 sums in TMEM, then the output
       const int quad = warp & 3;                          // TMEM lanes 32*quad .. +31
+      const int colh = (warp - DRAIN_W0) >> 2;            // columns 64*colh .. +63
       const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
       bool ok = true;
       for (int per = 0; per < nper; ++per) {
@@ -427,19 +428,25 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (!mbar_wait_warp(&accfull[ab], (per >> 1) & 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
 #pragma unroll 1
-        for (int cb = 0; cb < NC / 16; ++cb) {
-          uint32_t f32[16], f64[32];
-          tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + cb * 16), f32);
-          if (per > 0) tmem_ld32w(tmem + lane_base + FP64_COL + static_cast<uint32_t>(cb * 32), f64);
-          tmem_wait_ld();
+        for (int cp = 0; cp < 2; ++cp) {                  // two pairs of 16-column blocks
+          uint32_t f32a[16], f32b[16], f64w[32];
+          const int c0b = colh * 64 + cp * 32;
+          tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + c0b), f32a);
+          tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + c0b + 16), f32b);
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            double acc = (per > 0) ? __hiloint2double(static_cast<int>(f64[2 * i + 1]), static_cast<int>(f64[2 * i])) : 0.0;
-            acc += static_cast<double>(__uint_as_float(f32[i]));
-            f64[2 * i] = static_cast<uint32_t>(__double2loint(acc));
-            f64[2 * i + 1] = static_cast<uint32_t>(__double2hiint(acc));
+          for (int half = 0; half < 2; ++half) {
+            const uint32_t fcol = FP64_COL + static_cast<uint32_t>(2 * c0b + 32 * half);
+            if (per > 0) tmem_ld32w(tmem + lane_base + fcol, f64w);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              double a0 = (per > 0) ? __hiloint2double(static_cast<int>(f64w[2 * i + 1]), static_cast<int>(f64w[2 * i])) : 0.0;
+              a0 += static_cast<double>(__uint_as_float(half ? f32b[i] : f32a[i]));
+              f64w[2 * i] = static_cast<uint32_t>(__double2loint(a0));
+              f64w[2 * i + 1] = static_cast<uint32_t>(__double2hiint(a0));
+            }
+            tmem_st32(tmem + lane_base + fcol, f64w);
           }
-          tmem_st32(tmem + lane_base + FP64_COL + static_cast<uint32_t>(cb * 32), f64);
         }
         tmem_wait_st();
         tc_fence_before();
@@ -460,15 +467,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           inv /= p.scales[2];
         }
 #pragma unroll 1
-        for (int cb = 0; cb < NC / 16; ++cb) {
+        for (int cb = 0; cb < 4; ++cb) {
           uint32_t f64[32];
-          tmem_ld32w(tmem + lane_base + FP64_COL + static_cast<uint32_t>(cb * 32), f64);
+          const int cbase = colh * 64 + cb * 16;
+          tmem_ld32w(tmem + lane_base + FP64_COL + static_cast<uint32_t>(2 * cbase), f64);
           tmem_wait_ld();
           if (m >= p.M) continue;
 #pragma unroll 4
           for (int i = 0; i < 16; ++i) {
             const double v = __hiloint2double(static_cast<int>(f64[2 * i + 1]), static_cast<int>(f64[2 * i])) * inv;
-            const int nloc = cb * 16 + i;
+            const int nloc = cbase + i;
             if (p.mode == MODE_CHI0) {
               const int n = nt * NC + nloc;
               if (n >= p.N) continue;
