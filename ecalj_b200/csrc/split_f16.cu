@@ -19,7 +19,7 @@
 //     warp 0        TMA producer
 //     warp 1        TMEM owner and MMA issuer
 //     warps 2..9    B' converters (two threads per B' row)
-//     warps 10..13  drain: FP32 accumulators -> FP64 sums in TMEM -> output
+//     warps 10..17  drain: FP32 accumulators -> FP64 sums in TMEM -> output
 // Every mbarrier wait is bounded; on time-out the CTA records an error,
 // drains its own TMA and MMA work, frees TMEM and exits.
 #include <cuda.h>
@@ -35,17 +35,19 @@ constexpr int BM2 = 128;                 // real accumulator rows (64 complex x 
 constexpr int BMC = 64;                  // complex rows per tile
 constexpr int NC = 128;                  // complex columns per tile (UMMA N)
 constexpr int KC = 64;                   // FP16 elements per chunk along K' (32 complex k)
-constexpr int NSTAGE = 4;                // A' stages (TMA)
-constexpr int NTHREADS = 448;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..13 drain
+constexpr int NSTAGE = 2;
+constexpr int NTHREADS = 576;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..17 drain
 constexpr int NCONV = 256;               // converter threads (warps 2..9), two per B' row
 constexpr int CONV_W0 = 2, DRAIN_W0 = 10;
-constexpr int NDRAIN_WARPS = 4;          // drain warps 10..13, one per TMEM lane quadrant
+constexpr int NDRAIN_WARPS = 8;          // drain warps 10..17: two per TMEM lane quadrant, 64 columns each
 constexpr int NBUF = 3;                  // B' buffers
 constexpr int DRAIN_PERIOD = 2;          // K chunks per FP32 accumulation run (24 MMAs)
 constexpr int SLICE_A = BM2 * KC * 2;    // 16 KB
+constexpr int SLICE_S = NC * KC * 2;     // 16 KB
 constexpr int SLICE_B = NC * KC * 2;     // 16 KB
 constexpr int OFF_A = 0;
-constexpr int OFF_B = OFF_A + NSTAGE * 2 * SLICE_A;
+constexpr int OFF_S = OFF_A + NSTAGE * 2 * SLICE_A;
+constexpr int OFF_B = OFF_S + NSTAGE * 2 * SLICE_S;
 constexpr int OFF_BAR = OFF_B + NBUF * 2 * SLICE_B;
 constexpr int NBAR = 2 * NSTAGE + 2 * NBUF + 2 + 2 + 1;
 constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
@@ -77,11 +79,7 @@ struct Params {
   int herm;                 // chi0: skip tiles above the diagonal, mirror the lower part
   int tiles_per_slot;       // m-tiles of one A' slot
   int lo_tile_off;          // tile offset of the lo slice in the A' map
-  // B source: FP16 rows of s_ld elements, hi slice at s_base, lo slice at s_base + s_slice;
-  // chi0 rows live in the re-halves of the A' tiles (row of n = (n/64)*128 + n%64)
-  const __half* s_base;
-  long long s_slice, s_ld;
-  int s_tiled;
+  int lo_row_off;           // row (2-D) / tile (4-D) offset of the lo slice in the S map
   // output
   double2* C;
   long long ldc, c_bs;
@@ -145,6 +143,12 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
       "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
       ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2),
         "r"(c3)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
       : "memory");
 }
 
@@ -228,10 +232,12 @@ __device__ __forceinline__ int sw128_off(int r, int c) { return r * 128 + ((c ^ 
 // chunks while four drain warps fold the finished one into FP64 sums kept in
 // TMEM (columns 256..511, two 32-bit words per value).
 __global__ void __launch_bounds__(NTHREADS, 1)
-    split_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const Params p) {
+    split_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapS,
+                      const Params p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* sA = sm + OFF_A;
+  unsigned char* sS = sm + OFF_S;
   unsigned char* sB = sm + OFF_B;
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
   uint64_t* full = bar;                  // [NSTAGE] TMA -> MMA, converters
@@ -284,7 +290,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (nchunk > 0) {
     if (warp == 0 && lane == 0) {
       // ---------------- TMA producer
-      const uint32_t bytes = 2 * SLICE_A;
+      const uint32_t bytes = 2 * SLICE_A + 2 * SLICE_S;
       int issued = 0;
       for (int c = 0; c < nchunk; ++c) {
         const int st = c % NSTAGE;
@@ -292,16 +298,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         issued = c + 1;
         mbar_expect_tx(&full[st], bytes);
         unsigned char* a = sA + st * 2 * SLICE_A;
+        unsigned char* s = sS + st * 2 * SLICE_S;
         if (p.mode == MODE_CHI0) {
           const int x = (cbeg + c) * KC;
           tma_load_4d(a, &mapA, &full[st], x, 0, 0, mt);
           tma_load_4d(a + SLICE_A, &mapA, &full[st], x, 0, 0, p.lo_tile_off + mt);
+          tma_load_4d(s, &mapS, &full[st], x, 0, 0, 2 * nt);
+          tma_load_4d(s + SLICE_S, &mapS, &full[st], x, 0, 0, p.lo_row_off + 2 * nt);
         } else {
           const int sg = c / p.cps;
           const int x = (c - sg * p.cps) * KC;
           const int t = p.seg_slot[seg0 + sg] * p.tiles_per_slot + mt;
           tma_load_4d(a, &mapA, &full[st], x, 0, 0, t);
           tma_load_4d(a + SLICE_A, &mapA, &full[st], x, 0, 0, p.lo_tile_off + t);
+          tma_load_2d(s, &mapS, &full[st], x, nt * NC);
+          tma_load_2d(s + SLICE_S, &mapS, &full[st], x, p.lo_row_off + nt * NC);
         }
       }
       for (int c = max(0, issued - NSTAGE); c < issued; ++c) mbar_drain(&full[c % NSTAGE], (c / NSTAGE) & 1);
@@ -347,33 +358,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
         for (int i = 0; i < 4; ++i) wv[i] = __ldg(src + i);
       };
-      // this thread's 64-byte halves of the B-source row (hi and lo), one chunk ahead
-      const int n_tile = nt * NC + ct;
-      const long long srow = p.s_tiled ? (static_cast<long long>(n_tile >> 6) * 128 + (n_tile & 63)) : n_tile;
-      const __half* srow_hi = p.s_base + srow * p.s_ld + h * 32;
-      auto load_s = [&](int c, uint4 (&vh)[4], uint4 (&vl)[4]) {
-        const long long x = (p.mode == MODE_CHI0) ? static_cast<long long>(cbeg + c) * KC
-                                                  : static_cast<long long>(c - (c / p.cps) * p.cps) * KC;
-        const uint4* ph = reinterpret_cast<const uint4*>(srow_hi + x);
-        const uint4* pl = reinterpret_cast<const uint4*>(srow_hi + p.s_slice + x);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) { vh[i] = __ldg(ph + i); vl[i] = __ldg(pl + i); }
-      };
-      uint4 nh[4], nl[4];
-      load_s(0, nh, nl);
       if (p.mode == MODE_CHI0) load_w(0, wn);
       int seg_cached = -1;
       float rs = 0.f;
       for (int c = 0; c < nchunk; ++c) {
+        const int st = c % NSTAGE;
         float4 wc[4];
-        uint4 ch_hi[4], ch_lo[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) { ch_hi[i] = nh[i]; ch_lo[i] = nl[i]; }
-        if (c + 1 < nchunk) load_s(c + 1, nh, nl);        // prefetch while this chunk converts
         if (p.mode == MODE_CHI0) {
 #pragma unroll
           for (int i = 0; i < 4; ++i) wc[i] = wn[i];
-          if (c + 1 < nchunk) load_w(c + 1, wn);
+          if (c + 1 < nchunk) load_w(c + 1, wn);      // prefetch while this chunk converts
         } else {
 #pragma unroll
           for (int i = 0; i < 4; ++i) wc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -386,16 +380,19 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             seg_cached = sg;
           }
         }
+        if (!mbar_wait_warp(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
         const int b = c % NBUF;
         if (c >= NBUF && !mbar_wait_warp(&bempty[b], ((c / NBUF) - 1) & 1, abort_flag)) break;
+        const unsigned char* s_hi = sS + st * 2 * SLICE_S;
+        const unsigned char* s_lo = s_hi + SLICE_S;
         unsigned char* d_hi = sB + b * 2 * SLICE_B;
         unsigned char* d_lo = d_hi + SLICE_B;
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
           const int ch = h * 4 + cc;
           const int off = sw128_off(ct, ch);
-          const uint4 vh = ch_hi[cc];
-          const uint4 vl = ch_lo[cc];
+          const uint4 vh = *reinterpret_cast<const uint4*>(s_hi + off);
+          const uint4 vl = *reinterpret_cast<const uint4*>(s_lo + off);
           const __half2* h2 = reinterpret_cast<const __half2*>(&vh);
           const __half2* l2 = reinterpret_cast<const __half2*>(&vl);
           uint4 oh, ol;
@@ -423,6 +420,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     } else if (warp >= DRAIN_W0) {
       // ---------------- drain: FP32 accumulator -> FP64 sums in TMEM, then the output
       const int quad = warp & 3;                          // TMEM lanes 32*quad .. +31
+      const int colh = (warp - DRAIN_W0) >> 2;            // columns 64*colh .. +63
       const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
       bool ok = true;
       for (int per = 0; per < nper; ++per) {
@@ -430,9 +428,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (!mbar_wait_warp(&accfull[ab], (per >> 1) & 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
 #pragma unroll 1
-        for (int cp = 0; cp < NC / 32; ++cp) {            // pairs of 16-column blocks
+        for (int cp = 0; cp < 2; ++cp) {                  // two pairs of 16-column blocks
           uint32_t f32a[16], f32b[16], f64w[32];
-          const int c0b = cp * 32;
+          const int c0b = colh * 64 + cp * 32;
           tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + c0b), f32a);
           tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + c0b + 16), f32b);
 #pragma unroll
@@ -469,9 +467,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           inv /= p.scales[2];
         }
 #pragma unroll 1
-        for (int cb = 0; cb < NC / 16; ++cb) {
+        for (int cb = 0; cb < 4; ++cb) {
           uint32_t f64[32];
-          const int cbase = cb * 16;
+          const int cbase = colh * 64 + cb * 16;
           tmem_ld32w(tmem + lane_base + FP64_COL + static_cast<uint32_t>(2 * cbase), f64);
           tmem_wait_ld();
           if (m >= p.M) continue;
@@ -662,13 +660,14 @@ static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* di
 static DevBuf g_a, g_s, g_mx, g_sc, g_tabs, g_w32;
 static bool g_attr = false;
 
-static int launch_split(const CUtensorMap& ma, const Params& p, dim3 grid, cudaStream_t s, const char* tag) {
+static int launch_split(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s,
+                        const char* tag) {
   if (!g_attr) {
     QSGW_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     g_attr = true;
   }
   const int pi = prof_begin(tag, s);
-  split_gemm_kernel<<<grid, NTHREADS, SMEM_BYTES, s>>>(ma, p);
+  split_gemm_kernel<<<grid, NTHREADS, SMEM_BYTES, s>>>(ma, ms, p);
   prof_end(pi, s);
   count_launch();
   QSGW_LAUNCH_CHECK("split_gemm_kernel");
@@ -725,12 +724,15 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   QSGW_LAUNCH_CHECK("presplit_a_kernel");
   // maps: A' [Kp, 64, 2, 2*Ta] (hi tiles 0..Ta-1, lo tiles Ta..2Ta-1) box {64,64,2,1};
   //       S  same memory, half 0 of two consecutive tiles: box {64,64,1,2}
-  CUtensorMap ma;
+  CUtensorMap ma, ms;
   const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(2 * Ta)};
   const cuuint64_t str[3] = {static_cast<cuuint64_t>(Kp * 2), static_cast<cuuint64_t>(Kp * 2 * 64),
                              static_cast<cuuint64_t>(Kp * 2 * 128)};
   const cuuint32_t boxa[4] = {KC, 64, 2, 1};
+  const cuuint32_t boxs[4] = {KC, 64, 1, 2};
   rc = make_map(&ma, a, 4, dims, str, boxa);
+  if (rc) return rc;
+  rc = make_map(&ms, a, 4, dims, str, boxs);
   if (rc) return rc;
   Params p{};
   p.mode = MODE_CHI0;
@@ -738,7 +740,7 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   p.ntm = T; p.ntn = Tn;
   p.tiles_per_slot = Ta;
   p.lo_tile_off = Ta;                       // lo slice = tiles Ta..2Ta-1 of the same map
-  p.s_base = a; p.s_slice = slice_elems; p.s_ld = Kp; p.s_tiled = 1;
+  p.lo_row_off = Ta;
   p.herm = 1;                               // chi0(iw) is Hermitian: lower tiles + mirror
   p.kch_total = static_cast<int>(Kp / KC);
   p.w = w; p.npair = npair; p.niw = niw;
@@ -758,7 +760,7 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   p.kch_per_split = (p.kch_total + splitk - 1) / splitk;
   splitk = (p.kch_total + p.kch_per_split - 1) / p.kch_per_split;
   dim3 grid(static_cast<unsigned>(T * Tn), niw, splitk);
-  return launch_split(ma, p, grid, s, "chi0_tc");
+  return launch_split(ma, ms, p, grid, s, "chi0_tc");
 }
 
 int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
@@ -835,12 +837,17 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
                                                             g_sc.as<double>(), slice_s);
   count_launch();
   QSGW_LAUNCH_CHECK("sigc presplit");
-  CUtensorMap ma;
+  CUtensorMap ma, ms;
   const cuuint64_t dima[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(2LL * nslot * T)};
   const cuuint64_t stra[3] = {static_cast<cuuint64_t>(Kp * 2), static_cast<cuuint64_t>(Kp * 2 * 64),
                               static_cast<cuuint64_t>(Kp * 2 * 128)};
   const cuuint32_t boxa[4] = {KC, 64, 2, 1};
   rc = make_map(&ma, A, 4, dima, stra, boxa);
+  if (rc) return rc;
+  const cuuint64_t dims_[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(2 * nrows)};
+  const cuuint64_t strs[1] = {static_cast<cuuint64_t>(Kp * 2)};
+  const cuuint32_t boxs[2] = {KC, NC};
+  rc = make_map(&ms, S, 2, dims_, strs, boxs);
   if (rc) return rc;
   Params p{};
   p.mode = MODE_SEG;
@@ -852,13 +859,13 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   p.seg_slot = d_slot; p.segs = d_segs;
   p.tiles_per_slot = T;
   p.lo_tile_off = nslot * T;
-  p.s_base = S; p.s_slice = slice_s; p.s_ld = Kp; p.s_tiled = 0;
+  p.lo_row_off = static_cast<int>(nrows);
   p.C = a.out; p.ldc = ngb; p.c_bs = 0;
   p.scales = g_sc.as<double>();
   p.err = ctx().d_flags + 1;
   QSGW_CUDA(cudaMemsetAsync(a.out, 0, static_cast<size_t>(ngb) * a.ncol * sizeof(double2), s));
   dim3 grid(static_cast<unsigned>(T * ntiles), 1, 1);
-  return launch_split(ma, p, grid, s, "sigc_seg_tc");
+  return launch_split(ma, ms, p, grid, s, "sigc_seg_tc");
 }
 
 }  // namespace qsgw
