@@ -47,6 +47,13 @@ class SxcfArgs(ctypes.Structure):
                 ("zmel", c_vp), ("wc_imag", c_vp), ("wc_real", c_vp), ("zsec", c_vp)]
 
 
+class ZmelAtom(ctypes.Structure):
+    """Mirror of ``qsgw_zmel_atom``."""
+    _fields_ = [("ppb_d", c_vp), ("nlnm", c_int), ("nc", c_int), ("nv", c_int), ("ias", c_int),
+                ("ics", c_int), ("ims", c_int), ("mdim", c_int), ("ncore", c_int),
+                ("phase_re", c_dbl), ("phase_im", c_dbl)]
+
+
 _SIGS = {
     "qsgw_init": [c_int],
     "qsgw_finalize": [],
@@ -73,6 +80,12 @@ _SIGS = {
     "qsgw_sxcf_correlation_d": [ctypes.POINTER(SxcfArgs)],
     "qsgw_sxcf_wgtim_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_dbl, c_dbl,
                           c_dbl, c_vp, c_vp, c_vp],
+    "qsgw_sxcf_exchange_d": [c_vp, c_int, c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_dbl,
+                             c_dbl, c_dbl],
+    "qsgw_hqpe_d": [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_vp],
+    "qsgw_zmel_mt_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_int,
+                       ctypes.POINTER(ZmelAtom)],
+    "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
 }
 
 
@@ -305,3 +318,38 @@ def sxcf_wgtim_d(out, niw, ns1, ns2, ntqxx, nctot, omega, ekc, esmr, wkkr, ua, f
     _chk(load().qsgw_sxcf_wgtim_d(_p(out), niw, ns1, ns2, ntqxx, nctot, _p(o), _p(e), len(e), esmr,
                                   wkkr, ua, _p(x), _p(w), _p(ex)))
     return out
+
+
+# ---------------------------------------------------------------- Sigma_x, hqpe, zmel
+def sxcf_exchange_d(zsec, ntq, zmel, ngb, ns1, ns2, ntqxx, vcoud, ekc, nctot, ef, esmr, wkkr):
+    """sxcf_scz_exchange block (m_sxcf_gemm.f90:203-231); device zsec/zmel."""
+    v, e = _f64(vcoud), _f64(ekc)
+    _chk(load().qsgw_sxcf_exchange_d(_p(zsec), ntq, _p(zmel), ngb, ns1, ns2, ntqxx, _p(v), _p(e), len(e),
+                                     nctot, ef, esmr, wkkr))
+    return zsec
+
+
+def hqpe_d(sex2, sexcore2, sec2, vxc_band_ry, elda_ev, vxc_ev, ntq, ld, nq, eqp_ev, sigma_herm):
+    """main_hqpe.sc.f90:150-161,178-180 for nq q-points (all device arrays)."""
+    _chk(load().qsgw_hqpe_d(_p(sex2), _p(sexcore2), _p(sec2), _p(vxc_band_ry), _p(elda_ev), _p(vxc_ev), ntq, ld,
+                            nq, _p(eqp_ev), _p(sigma_herm)))
+
+
+def zmel_mt_d(zmelt, nbloch, nm1, nm2, nctot, ntp0, cphim, ldm, cphiq, ldq, atoms):
+    """Muffin-tin part of get_zmel_init_gemm; ``atoms`` is a list of dicts with
+    the qsgw_zmel_atom fields (ppb_d a device tensor)."""
+    arr = (ZmelAtom * len(atoms))()
+    keep = []
+    for i, a in enumerate(atoms):
+        keep.append(a["ppb_d"])
+        arr[i] = ZmelAtom(_p(a["ppb_d"]), a["nlnm"], a["nc"], a["nv"], a["ias"], a["ics"], a["ims"], a["mdim"],
+                          a["ncore"], float(np.real(a["phase"])), float(np.imag(a["phase"])))
+    _chk(load().qsgw_zmel_mt_d(_p(zmelt), nbloch, nm1, nm2, nctot, ntp0, _p(cphim), ldm, _p(cphiq), ldq,
+                               len(atoms), arr))
+    return zmelt
+
+
+def zmel_m2e_d(zmel, zmelt, ngb, nbb, nmtot, nqtot, m2e, is_m_basis, zmelconjg):
+    _chk(load().qsgw_zmel_m2e_d(_p(zmel), _p(zmelt), ngb, nbb, nmtot, nqtot, _p(m2e), int(is_m_basis),
+                                int(zmelconjg)))
+    return zmel

@@ -202,6 +202,57 @@ int qsgw_sxcf_wgtim_d(double *wgtim_d, int niw, int ns1, int ns2, int ntqxx,
                       const double *freqx, const double *wwx,
                       const double *expa);
 
+/* ---- Sigma_x block of sxcf_scz_exchange (m_sxcf_gemm.f90:203-231):
+ *   zsec += -wkkr * zmel^H (wtff * vcoud * zmel), K = (ngb, it)
+ * wtff(it) = 1 for cores, wfacx(-1d99, ef, ekc(it+nctot), esmr) for valence
+ * (the reference's index).  zmel: device (ngb, ns2-ns1+1, ntqxx) in the E
+ * basis; zsec: device (ntq, ntq); vcoud (effective, the kx == 1 head
+ * replacement of :218 applied by the caller) and ekc are host arrays.      */
+int qsgw_sxcf_exchange_d(double *zsec_d, int ntq, const double *zmel_d, int ngb,
+                         int ns1, int ns2, int ntqxx, const double *vcoud,
+                         const double *ekc, int nekc, int nctot, double ef,
+                         double esmr, double wkkr);
+
+/* ---- QP energies and the Hermitian self-energy of hqpe_sc
+ * (main_hqpe.sc.f90:150-161, 178-180), nq q-points at once, FP64:
+ *   eqp(i) = elda(i) + [SEx + SExcore + Re SEc](i,i) * Hartree - vxc(i)   (eV)
+ *   Sigma_h = SEx + SExcore + (SEc + SEc^H)/2 - vxc_band/2                 (Ha)
+ * Matrices (ntq, ntq) with leading dimension ld, nq of them at stride ld*ld;
+ * vxc_band in Ry (evec^H v_xc evec); elda, vxc, eqp (ntq, nq) in eV; all
+ * device arrays.                                                           */
+int qsgw_hqpe_d(const double *sex2_d, const double *sexcore2_d,
+                const double *sec2_d, const double *vxc_band_ry_d,
+                const double *elda_ev_d, const double *vxc_ev_d, int ntq, int ld,
+                int nq, double *eqp_ev_d, double *sigma_herm_d);
+
+/* ---- Product-basis matrix elements <psi|psi M>, muffin-tin part of
+ * get_zmel_init_gemm (m_zmel.f90:323-390, ncc = 0): every atom in one launch.
+ * zmelt: device (nbloch, nm1:nm2, ntp0); only the rows of the atoms' product
+ * functions are written (zero zmelt first).  cphim: device (ldm, nm1v:nm2v)
+ * valence coefficients at q-k, cphiq: device (ldq, ntp0) at q.            */
+typedef struct qsgw_zmel_atom {
+  const double *ppb_d;   /* device (nlnm, nlnm, mdim) radial integrals x rotated
+                            Gaunt coefficients: rows/cols core 1..nc then
+                            valence nc+1..nc+nv (set_ppb, m_zmel.f90:110-145) */
+  int nlnm, nc, nv;      /* channels: total, core, valence (nv <= 96)        */
+  int ias;               /* 1-based first row of the atom in cphim/cphiq     */
+  int ics;               /* core-state offset of the atom                    */
+  int ims;               /* 1-based first product-basis row (of iatomp)      */
+  int mdim;              /* product functions of the atom                    */
+  int ncore;             /* core states of the atom                          */
+  double phase_re, phase_im;   /* exp(-i 2 pi k.tau)  (m_zmel.f90:325)       */
+} qsgw_zmel_atom;
+int qsgw_zmel_mt_d(double *zmelt_d, int nbloch, int nm1, int nm2, int nctot,
+                   int ntp0, const double *cphim_d, int ldm,
+                   const double *cphiq_d, int ldq, int natom,
+                   const qsgw_zmel_atom *atoms);
+/* M->E change and conjugation (m_zmel.f90:546-563, 590-594):
+ * zmel(nbb, nmtot*nqtot) = m2e^H zmelt (or a copy when is_m_basis), then
+ * conj when zmelconjg.  m2e: device (ngb, nbb).                            */
+int qsgw_zmel_m2e_d(double *zmel_d, const double *zmelt_d, int ngb, int nbb,
+                    int nmtot, int nqtot, const double *m2e_d, int is_m_basis,
+                    int zmelconjg);
+
 #ifdef __cplusplus
 }
 #endif
