@@ -86,6 +86,7 @@ _SIGS = {
     "qsgw_zmel_mt_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_int,
                        ctypes.POINTER(ZmelAtom)],
     "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
+    "qsgw_zhegv_d": [c_vp, c_vp, c_int, c_int, c_vp],
 }
 
 
@@ -353,3 +354,11 @@ def zmel_m2e_d(zmel, zmelt, ngb, nbb, nmtot, nqtot, m2e, is_m_basis, zmelconjg):
     _chk(load().qsgw_zmel_m2e_d(_p(zmel), _p(zmelt), ngb, nbb, nmtot, nqtot, _p(m2e), int(is_m_basis),
                                 int(zmelconjg)))
     return zmel
+
+
+def zhegv_d(v, n, lda=None, o=None):
+    """Coulomb eigenproblem: v (device, Hermitian) -> eigenvectors in place;
+    returns vcoud (descending eigenvalues of v, O-orthonormal vectors)."""
+    out = np.zeros(n)
+    _chk(load().qsgw_zhegv_d(_p(v), _p(o), n, lda or n, out.ctypes.data))
+    return out

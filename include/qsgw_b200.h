@@ -253,6 +253,14 @@ int qsgw_zmel_m2e_d(double *zmel_d, const double *zmelt_d, int ngb, int nbb,
                     int nmtot, int nqtot, const double *m2e_d, int is_m_basis,
                     int zmelconjg);
 
+/* ---- Coulomb-matrix eigenproblem (main_hvccfp0.f90:322-367 with zhgv_d,
+ * m_lapack.f90:203-229): (-v) z = lambda O z, vcoud = -lambda, i.e. the
+ * eigenvalues of v in descending order with O-orthonormal eigenvectors.
+ * v_d: device (lda, n) Hermitian, overwritten by the eigenvectors z (column
+ * j belongs to vcoud[j]); o_d: device (lda, n) overlap or NULL (identity);
+ * vcoud: host (n).  FP64 parallel cyclic Jacobi.                          */
+int qsgw_zhegv_d(double *v_d, const double *o_d, int n, int lda, double *vcoud);
+
 #ifdef __cplusplus
 }
 #endif
