@@ -37,6 +37,8 @@ struct DevBuf {
 };
 
 int require_init();
+// kernels launched by this library since init (qsgw_launch_count)
+void count_launch(int n = 1);
 
 // Optional per-kernel timing with CUDA events on the launch stream
 // (qsgw_profile).  prof_begin returns -1 when profiling is off.

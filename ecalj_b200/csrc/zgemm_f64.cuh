@@ -314,6 +314,5 @@ int zgemm_f64(int opa, int opb, int m, int n, int k, double2 alpha,
               double2* C, long long ldc, long long c_bs, int nbatch, cudaStream_t s);
 int zgemm_chi0_launch(ZParams p, int nbins, int herm, int splitk, cudaStream_t s);
 int zgemm_seg_launch(ZParams p, int ncol_tiles, cudaStream_t s);
-void count_launch(int n = 1);
 
 }  // namespace qsgw

@@ -87,6 +87,20 @@ _SIGS = {
                        ctypes.POINTER(ZmelAtom)],
     "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
     "qsgw_zhegv_d": [c_vp, c_vp, c_int, c_int, c_vp],
+    "qsgw_wsurr_init": [ctypes.c_ulonglong],
+    "qsgw_wsurr_nparam": [],
+    "qsgw_wsurr_params": [c_vp, c_int],
+    "qsgw_wsurr_project_d": [c_vp, c_int, c_int, c_vp, c_vp, c_int, c_vp],
+    "qsgw_wsurr_lsq_accumulate_d": [c_vp, c_vp, c_vp, ctypes.c_longlong, c_int, c_vp],
+    "qsgw_wsurr_lsq_solve": [ctypes.c_double, c_vp],
+    "qsgw_wsurr_features_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_int, c_vp, c_vp, c_vp, c_int,
+                              c_vp, c_int, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "qsgw_wsurr_forward_d": [c_vp, c_vp, c_vp, c_int],
+    "qsgw_wsurr_grad_d": [c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp],
+    "qsgw_wsurr_train_d": [c_vp, c_vp, c_vp, c_vp, ctypes.c_longlong, c_int, c_int, ctypes.c_float,
+                           ctypes.c_ulonglong, c_vp],
+    "qsgw_wsurr_head_full_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_vp],
+    "qsgw_wsurr_scatter_d": [c_vp, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_vp],
 }
 
 
@@ -165,6 +179,18 @@ def finalize():
 
 def set_stream(stream_handle):
     _chk(load().qsgw_set_stream(stream_handle))
+
+
+def share_torch_stream():
+    """Run torch and this library on one stream: a new torch stream becomes
+    torch's current stream and the library's launch stream (the legacy
+    default stream, handle 0, does not order work against the library's own
+    non-blocking stream).  Returns the torch stream."""
+    import torch
+    s = torch.cuda.Stream()
+    torch.cuda.set_stream(s)
+    set_stream(s.cuda_stream)
+    return s
 
 
 def synchronize():
@@ -362,3 +388,104 @@ def zhegv_d(v, n, lda=None, o=None):
     out = np.zeros(n)
     _chk(load().qsgw_zhegv_d(_p(v), _p(o), n, lda or n, out.ctypes.data))
     return out
+
+
+# ---------------------------------------------------------------- W_c frequency surrogate
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def wsurr_init(seed=1234):
+    _chk(load().qsgw_wsurr_init(seed))
+
+
+def wsurr_nparam():
+    return load().qsgw_wsurr_nparam()
+
+
+def wsurr_params(values=None):
+    """Read (values None) or write the FP32 parameter vector."""
+    n = wsurr_nparam()
+    if values is None:
+        out = np.zeros(n, np.float32)
+        _chk(load().qsgw_wsurr_params(out.ctypes.data, 0))
+        return out
+    v = _f32(values)
+    if v.size != n:
+        raise ValueError(f"expected {n} parameters, got {v.size}")
+    _chk(load().qsgw_wsurr_params(v.ctypes.data, 1))
+
+
+def wsurr_project_d(wc, ld, nslot, ridx, proj, cidx=None):
+    r = _i32(ridx)
+    c = None if cidx is None else _i32(cidx)
+    if c is not None and len(c) != len(r):
+        raise ValueError("ridx and cidx differ in length")
+    _chk(load().qsgw_wsurr_project_d(_p(wc), ld, nslot, r.ctypes.data, None if c is None else c.ctypes.data, len(r),
+                                     _p(proj)))
+
+
+def wsurr_lsq_accumulate_d(x, y, wgt, n, thead):
+    h = _i32(thead)
+    _chk(load().qsgw_wsurr_lsq_accumulate_d(_p(x), _p(y), _p(wgt), n, len(h), h.ctypes.data))
+
+
+def wsurr_lsq_solve(ridge=1e-9):
+    """Solve the accumulated normal equations into the head rows; returns the rows solved."""
+    k = ctypes.c_int(0)
+    _chk(load().qsgw_wsurr_lsq_solve(ridge, ctypes.byref(k)))
+    return k.value
+
+
+def wsurr_features_d(proj, nq, nw, ne, anchors, targets, thead, xcoord, x, tix, y=None, wgt=None, scale=None,
+                     rid=None, cid=None, ftab=None):
+    a, t, h, xc = _i32(anchors), _i32(targets), _i32(thead), _f32(xcoord)
+    if len(h) != len(t) or len(xc) != nw:
+        raise ValueError("thead must match targets and xcoord must have nw entries")
+    if ftab is None:
+        r = c = f = None
+        nb = nf = 0
+    else:
+        r, c, f = _i32(rid), _i32(cid), _f32(ftab)
+        nb, nf = len(r), len(f)
+        if len(c) != nb:
+            raise ValueError("rid and cid differ in length")
+    _chk(load().qsgw_wsurr_features_d(_p(proj), nq, nw, ne, a.ctypes.data, len(a), t.ctypes.data, h.ctypes.data,
+                                      len(t), xc.ctypes.data, _p(r), _p(c), nb, _p(f), nf, _p(x), _p(tix), _p(y),
+                                      _p(wgt), _p(scale)))
+
+
+def wsurr_forward_d(x, tix, y, batch):
+    _chk(load().qsgw_wsurr_forward_d(_p(x), _p(tix), _p(y), batch))
+
+
+def wsurr_grad_d(x, tix, y, batch, wgt=None):
+    """Returns (loss, gradient) without updating the parameters."""
+    loss = np.zeros(1, np.float32)
+    grad = np.zeros(wsurr_nparam(), np.float32)
+    _chk(load().qsgw_wsurr_grad_d(_p(x), _p(tix), _p(y), _p(wgt), batch, loss.ctypes.data, grad.ctypes.data))
+    return float(loss[0]), grad
+
+
+def wsurr_train_d(x, tix, y, wgt, n, batch, nsteps, lr, seed=0):
+    """nsteps Adam steps; returns the last mini-batch's loss."""
+    loss = np.zeros(1, np.float32)
+    _chk(load().qsgw_wsurr_train_d(_p(x), _p(tix), _p(y), _p(wgt), n, batch, nsteps, lr, seed, loss.ctypes.data))
+    return float(loss[0])
+
+
+def wsurr_head_full_d(wc, n, ld, nslot, aslot, tslot, thead, txc, ftab=None):
+    a, t, h, x = _i32(aslot), _i32(tslot), _i32(thead), _f32(txc)
+    f = None if ftab is None else _f32(ftab)
+    if f is not None and len(f) != n:
+        raise ValueError("ftab must have n entries")
+    _chk(load().qsgw_wsurr_head_full_d(_p(wc), n, ld, nslot, a.ctypes.data, len(a), t.ctypes.data, h.ctypes.data,
+                                       x.ctypes.data, len(t), _p(f)))
+
+
+def wsurr_scatter_d(wc, ld, nslot, idx, tslot, pred, scale):
+    i, t = _i32(idx), _i32(tslot)
+    if pred.numel() < 2 * len(i) ** 2 * len(t) or scale.numel() < pred.numel():
+        raise ValueError("pred/scale hold fewer than 2 nb^2 nt samples")
+    _chk(load().qsgw_wsurr_scatter_d(_p(wc), ld, nslot, i.ctypes.data, len(i), t.ctypes.data, len(t), _p(pred),
+                                     _p(scale)))

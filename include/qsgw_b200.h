@@ -261,6 +261,75 @@ int qsgw_zmel_m2e_d(double *zmel_d, const double *zmelt_d, int ngb, int nbb,
  * vcoud: host (n).  FP64 parallel cyclic Jacobi.                          */
 int qsgw_zhegv_d(double *v_d, const double *o_d, int n, int lda, double *vcoud);
 
+/* ---- Learned W_c(q, i w) frequency interpolator.  No counterpart in the
+ * reference: it stands in for computing chi0 and W at every frequency of
+ * the imaginary grid.  One sample = one real channel of one element of
+ * W_c(q) at one target frequency; features (16) = the channel at the na
+ * anchor frequencies / s (s = their largest magnitude), the target's
+ * Gauss-Legendre x, 1; output (normalised by s) = C[h] . x + MLP(x), with a
+ * linear head row h per target (FP32, 128 rows; rows >= 64 take no MLP
+ * term) and an MLP 16-256-256-1 (ReLU, BF16 weights with an FP32 master
+ * copy, FP32 accumulation).  Trained with Adam on the s^2-weighted squared
+ * error, the head rows first set by least squares.
+ * Parameters live in the library (one network per process).              */
+int qsgw_wsurr_init(unsigned long long seed);
+int qsgw_wsurr_nparam(void);
+/* host FP32 parameter vector: set != 0 writes it (and the BF16 copy), else reads */
+int qsgw_wsurr_params(float *host, int set);
+/* proj_d (nslot, 2 nb nb) float <- W_c(ridx[i], cidx[j]) re/im of each slot
+ * (channel 2 (i + nb j) + c); wc_d: device slots of ld x ld complex, slot
+ * stride ld*ld; ridx, cidx: host (nb), cidx NULL = ridx.                   */
+int qsgw_wsurr_project_d(const double *wc_d, int ld, int nslot, const int *ridx,
+                         const int *cidx, int nb, float *proj_d);
+/* samples of every (q, channel, target), target fastest: proj_d (nq, nw, ne)
+ * float; anchors/targets: host slot indices into nw (na <= 10); thead: host
+ * head row of each target (< 128); xcoord: host (nw) Gauss-Legendre x.
+ * Element features (x[na+2..na+5]): ftab[row], ftab[col], re/im, diagonal,
+ * for the block rows rid and columns cid (host, nb each, ne = 2 nb nb);
+ * ftab: host (nftab) per-index feature, NULL = no element features.
+ * Outputs (device): x_d (samples, 16), tix_d (samples); optional y_d
+ * (normalised value at the target), wgt_d (s^2), scale_d (s).              */
+int qsgw_wsurr_features_d(const float *proj_d, int nq, int nw, int ne,
+                          const int *anchors, int na, const int *targets,
+                          const int *thead, int nt, const float *xcoord,
+                          const int *rid, const int *cid, int nb,
+                          const float *ftab, int nftab, float *x_d, int *tix_d,
+                          float *y_d, float *wgt_d, float *scale_d);
+/* least squares of the head rows: accumulate the s^2-weighted normal
+ * equations of n samples in the features order (nt targets, thead: host
+ * head row of each), then solve them (ridge * trace/16 added to the
+ * diagonal) into the head rows that received samples, clearing the sums.  */
+int qsgw_wsurr_lsq_accumulate_d(const float *x_d, const float *y_d,
+                                const float *wgt_d, long long n, int nt,
+                                const int *thead);
+int qsgw_wsurr_lsq_solve(double ridge, int *rows_solved);
+/* inference: y_d <- network output (normalised) for batch samples */
+int qsgw_wsurr_forward_d(const float *x_d, const int *tix_d, float *y_d, int batch);
+/* gradient only (no update): grad_host <- dL/dparams, loss_host <- L;
+ * wgt_d NULL = unweighted mean squared error                               */
+int qsgw_wsurr_grad_d(const float *x_d, const int *tix_d, const float *y_d,
+                      const float *wgt_d, int batch, float *loss_host,
+                      float *grad_host);
+/* nsteps Adam steps on random mini-batches of `batch` rows drawn from the n
+ * samples (counter-based hash of seed and step); loss_host <- last batch's L */
+int qsgw_wsurr_train_d(const float *x_d, const int *tix_d, const float *y_d,
+                       const float *wgt_d, long long n, int batch, int nsteps,
+                       float lr, unsigned long long seed, float *loss_host);
+/* full matrix, linear head only: slot tslot[t] of wc_d (nslot slots of ld x
+ * ld, n x n used) <- s * C[thead[t]] . x built from the anchor slots aslot;
+ * txc: host Gauss-Legendre x of each target; ftab: host (n) per-index
+ * feature as in qsgw_wsurr_features_d, or NULL.                            */
+int qsgw_wsurr_head_full_d(double *wc_d, int n, int ld, int nslot,
+                           const int *aslot, int na, const int *tslot,
+                           const int *thead, const float *txc, int nt,
+                           const float *ftab);
+/* block (idx x idx) of the target slots <- pred_d * scale_d; pred_d and
+ * scale_d hold 2 nb nb nt samples of one q in the features order (target
+ * fastest, then channel 2 (i + nb j) + re/im)                              */
+int qsgw_wsurr_scatter_d(double *wc_d, int ld, int nslot, const int *idx, int nb,
+                         const int *tslot, int nt, const float *pred_d,
+                         const float *scale_d);
+
 #ifdef __cplusplus
 }
 #endif

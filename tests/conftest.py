@@ -21,6 +21,7 @@ def qsgw():
         pytest.fail("GPU test collected on a machine without CUDA")
     lib.load()
     lib.init(0)
+    lib.share_torch_stream()
     yield lib
     lib.set_precision(lib.PREC_FP64)
 

@@ -1,0 +1,219 @@
+"""Learned W_c frequency interpolator: kernels against the CPU oracle, training,
+the surrogate path's validation/fallback, and what the trained network gains."""
+import numpy as np
+import pytest
+
+from oracle import mlp
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(t, a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+
+
+def _set_params(lib, rng, head_scale=0.3, out_scale=30.0):
+    lib.wsurr_init(11)
+    p = lib.wsurr_params()
+    p[mlp.OFF_C:] = rng.normal(0.0, head_scale, p.size - mlp.OFF_C).astype(np.float32)
+    p[mlp.OFF_W3:mlp.OFF_B3] *= out_scale          # make the MLP part of the output sizeable
+    p[mlp.OFF_B1:mlp.OFF_W2] = rng.normal(0.0, 0.1, mlp.NH).astype(np.float32)
+    lib.wsurr_params(p)
+    return lib.wsurr_params()
+
+
+def test_forward_and_gradient_match_oracle(qsgw):
+    import torch
+    lib = qsgw
+    rng = np.random.default_rng(3)
+    p = _set_params(lib, rng)
+    x = rng.normal(0.0, 1.0, (3000, 16)).astype(np.float32)
+    # keep rows whose pre-activations are all clear of the ReLU kink: there an
+    # FP32 / float64 difference of 1e-7 could flip a unit on or off
+    W1, b1, W2, b2 = mlp.unpack(p)[:4]
+    a1 = x @ W1 + b1
+    a2 = np.maximum(a1, 0.0) @ W2 + b2
+    x = x[(np.abs(a1).min(1) > 1e-4) & (np.abs(a2).min(1) > 1e-4)][:1000]
+    B = len(x)                                      # not a multiple of the 32-row block
+    assert B == 1000
+    tix = rng.integers(0, 80, B).astype(np.int32)   # both head banks (rows >= 64: no MLP term)
+    y = rng.normal(0.0, 1.0, B).astype(np.float32)
+    w = rng.uniform(0.1, 3.0, B).astype(np.float32)
+    xd, td, yd, wd = (_dev(torch, a) for a in (x, tix, y, w))
+    out = torch.empty(B, dtype=torch.float32, device="cuda")
+    lib.wsurr_forward_d(xd, td, out, B)
+    ref, _ = mlp.forward(p, x, tix)
+    assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-5 * np.max(np.abs(ref))
+    for wgt in (None, wd):
+        loss, g = lib.wsurr_grad_d(xd, td, yd, B, wgt=wgt)
+        L, go = mlp.loss_and_grad(p, x, tix, y, None if wgt is None else w)
+        assert abs(loss - L) <= 1e-5 * L
+        # relative error per parameter block (FP32 accumulation against float64)
+        for a, b in [(mlp.OFF_W1, mlp.OFF_B1), (mlp.OFF_B1, mlp.OFF_W2), (mlp.OFF_W2, mlp.OFF_B2),
+                     (mlp.OFF_B2, mlp.OFF_W3), (mlp.OFF_W3, mlp.OFF_B3), (mlp.OFF_B3, mlp.OFF_C),
+                     (mlp.OFF_C, mlp.NPARAM)]:
+            e = np.linalg.norm(g[a:b] - go[a:b]) / np.linalg.norm(go[a:b])
+            assert e <= 1e-4, (a, b, e)
+
+
+def test_features_match_oracle(qsgw):
+    import torch
+    lib = qsgw
+    rng = np.random.default_rng(4)
+    nq, nw, ne = 3, 11, 10
+    proj = rng.normal(0.0, 5.0, (nq, nw, ne)).astype(np.float32)
+    proj[1, :, 2] = 0.0                             # an all-zero channel
+    anchors, targets, thead = [0, 3, 6, 10], [1, 2, 5, 9], [0, 1, 2, 3]
+    xcoord = np.sort(rng.uniform(0, 1, nw)).astype(np.float32)
+    n = nq * ne * len(targets)
+    d = {k: torch.empty(n * (16 if k == "x" else 1), dtype=torch.int32 if k == "tix" else torch.float32,
+                        device="cuda") for k in ("x", "tix", "y", "w", "s")}
+    lib.wsurr_features_d(_dev(torch, proj), nq, nw, ne, anchors, targets, thead, xcoord,
+                         d["x"], d["tix"], d["y"], d["w"], d["s"])
+    x, tix, y, w, s = mlp.features(proj, anchors, targets, thead, xcoord)
+    np.testing.assert_allclose(d["x"].cpu().numpy().reshape(-1, 16), x, rtol=1e-6, atol=0)
+    np.testing.assert_array_equal(d["tix"].cpu().numpy(), tix)
+    np.testing.assert_allclose(d["y"].cpu().numpy(), y, rtol=1e-6, atol=0)
+    np.testing.assert_allclose(d["w"].cpu().numpy(), w, rtol=1e-6, atol=0)
+    np.testing.assert_allclose(d["s"].cpu().numpy(), s, rtol=0, atol=0)
+    # with element features: a 2 x 2 block (rows 3, 1; columns 1, 4) of a 6-index matrix
+    nb, ne = 2, 8
+    proj = rng.normal(0.0, 5.0, (nq, nw, ne)).astype(np.float32)
+    rid, cid, ftab = [3, 1], [1, 4], rng.normal(size=6).astype(np.float32)
+    n = nq * ne * len(targets)
+    x_d = torch.empty(n * 16, dtype=torch.float32, device="cuda")
+    t_d = torch.empty(n, dtype=torch.int32, device="cuda")
+    lib.wsurr_features_d(_dev(torch, proj), nq, nw, ne, anchors, targets, thead, xcoord, x_d, t_d,
+                         rid=rid, cid=cid, ftab=ftab)
+    x, tix, *_ = mlp.features(proj, anchors, targets, thead, xcoord, rid, cid, ftab)
+    np.testing.assert_allclose(x_d.cpu().numpy().reshape(-1, 16), x, rtol=1e-6, atol=0)
+    assert x[:, 9].any() and x[:, 9].sum() < len(x)            # the diagonal flag is set on some rows only
+
+
+def test_project_head_scatter(qsgw):
+    import torch
+    lib = qsgw
+    rng = np.random.default_rng(5)
+    ns, N = 7, 20
+    W = (rng.normal(size=(ns, N, N)) + 1j * rng.normal(size=(ns, N, N))).astype(np.complex128)
+    wd = _dev(torch, W)                 # torch [s, j, i] = column-major element (i, j) of slot s
+    idx = np.array([1, 4, 7, 12, 19], np.int32)
+    nb = len(idx)
+    pr = torch.empty(ns * 2 * nb * nb, dtype=torch.float32, device="cuda")
+    lib.wsurr_project_d(wd, N, ns, idx, pr)
+    blk = W[:, idx][:, :, idx]          # [s, j, i]
+    ref = np.stack([blk.real, blk.imag], -1).astype(np.float32).reshape(ns, -1)
+    np.testing.assert_array_equal(pr.cpu().numpy().reshape(ns, -1), ref)
+    # linear head on the full matrix
+    p = _set_params(lib, rng)
+    aslot, tslot, thead = [0, 2, 5], [1, 3, 6], [4, 0, 9]
+    xc = np.array([0.3, 0.6, 0.9], np.float32)
+    ftab = rng.normal(size=N).astype(np.float32)
+    lib.wsurr_head_full_d(wd, N, N, ns, aslot, tslot, thead, xc, ftab)
+    C = p[mlp.OFF_C:].reshape(mlp.NTMAX, mlp.NIN).astype(np.float64)
+    got = wd.cpu().numpy()
+    fr = ftab[None, :].astype(np.float64)          # torch [s, j, i]: row index i is the last axis
+    fc = ftab[:, None].astype(np.float64)
+    dg = np.eye(N)
+    for c, part in enumerate((np.real, np.imag)):
+        av = part(W[aslot]).astype(np.float32)                      # (na, N, N)
+        s = np.maximum(np.abs(av).max(0), np.float32(1e-30)).astype(np.float64)
+        for k, (t_, h) in enumerate(zip(tslot, thead)):
+            exp = s * (np.tensordot(C[h, :3], av / s, axes=(0, 0)) + C[h, 3] * xc[k] + C[h, 4]
+                       + C[h, 5] * fr + C[h, 6] * fc + C[h, 7] * c + C[h, 8] * dg)
+            np.testing.assert_allclose(part(got[t_]), exp, rtol=2e-5, atol=2e-5 * np.abs(exp).max())
+    for a in aslot:
+        np.testing.assert_array_equal(got[a], W[a])
+    # scatter of block predictions
+    nt = len(tslot)
+    pred = rng.normal(size=2 * nb * nb * nt).astype(np.float32)
+    sc = rng.uniform(0.5, 2.0, 2 * nb * nb * nt).astype(np.float32)
+    lib.wsurr_scatter_d(wd, N, ns, idx, tslot, _dev(torch, pred), _dev(torch, sc))
+    got2 = wd.cpu().numpy()
+    v = (pred * sc).astype(np.float64).reshape(nb * nb, 2, nt)     # channel = 2 (i + nb j) + c, target fastest
+    for k, t_ in enumerate(tslot):
+        val = (v[:, 0, k] + 1j * v[:, 1, k]).reshape(nb, nb)       # [j, i]
+        np.testing.assert_array_equal(got2[t_][np.ix_(idx, idx)], val)
+        mask = np.ones((N, N), bool)
+        mask[np.ix_(idx, idx)] = False
+        np.testing.assert_array_equal(got2[t_][mask], got[t_][mask])
+
+
+def test_training_reduces_loss(qsgw):
+    import torch
+    lib = qsgw
+    rng = np.random.default_rng(6)
+    n = 20000
+    x = np.zeros((n, 16), np.float32)
+    x[:, :8] = rng.uniform(-1, 1, (n, 8))
+    x[:, 8] = rng.uniform(0, 1, n)
+    x[:, 9] = 1.0
+    tix = rng.integers(0, 4, n).astype(np.int32)
+    y = (np.sin(3 * x[:, 0]) * x[:, 8] + 0.5 * x[:, 1] * x[:, 2] + 0.1 * tix).astype(np.float32)
+    lib.wsurr_init(5)
+    xd, td, yd = _dev(torch, x), _dev(torch, tix), _dev(torch, y)
+    wd = torch.ones(n, dtype=torch.float32, device="cuda")
+    l0, _ = lib.wsurr_grad_d(xd, td, yd, n, wgt=wd)
+    lib.wsurr_train_d(xd, td, yd, wd, n, 1024, 600, 1e-3, 1)
+    l1, _ = lib.wsurr_grad_d(xd, td, yd, n, wgt=wd)
+    assert l1 < 0.05 * l0, (l0, l1)
+    assert lib.wsurr_params()[mlp.OFF_C:].any()        # the head was trained too
+
+
+@pytest.fixture(scope="module")
+def trained(qsgw):
+    """The interpolator trained on exact W_c of 48 q points of the Sigma_c
+    configuration (N=600, 48 imaginary frequencies), evaluated on 3 other q."""
+    from ecalj_b200 import surrogate
+    qsgw.set_precision(qsgw.PREC_FP64)
+    return surrogate.study(N=600, nq_train=48, nq_test=3, log=print)
+
+
+def test_trained_network_gains_over_linear_interpolation(trained):
+    """What training buys, at the predicted frequencies of held-out q points:
+    the network against the linear interpolation in x its heads start from
+    (the method without learning) and against its least-squares heads alone."""
+    for r in trained["rows"]:
+        lin, lsq, tr = r["linear"], r["lsq"], r["trained"]
+        assert tr["w_rel"] < 0.1 * lin["w_rel"], r
+        assert tr["qp_mev"] < 0.1 * lin["qp_mev"], r
+        assert tr["w_rel"] <= 1.05 * lsq["w_rel"], r
+        assert tr["w_rel_block"] <= 1.05 * lsq["w_rel_block"], r
+
+
+def test_surrogate_path_meets_tolerance_and_saves_time(trained):
+    """Every q either passes validation with a true QP error <= 1 meV or was
+    recomputed exactly; the surrogate path computes 17 of 49 frequency slots
+    exactly and is faster than the plain method."""
+    for r in trained["rows"]:
+        assert r["qp_mev_final"] <= 1.0, r
+        if not r["fallback"]:
+            assert r["n_exact"] == 17
+            assert r["ms_surrogate"] < r["ms_plain"], r
+    assert sum(not r["fallback"] for r in trained["rows"]) >= 2
+
+
+def test_fallback_on_injected_error(trained, qsgw):
+    """A host-side error injected into the network (its head zeroed) makes the
+    held-out validation exceed 1 meV; the path then recomputes every predicted
+    frequency with the plain method and returns the exact W_c."""
+    import torch
+    from ecalj_b200 import surrogate
+    lib = qsgw
+    sur, work = trained["surrogate"], trained["work"]
+    p = lib.wsurr_params()
+    bad = p.copy()
+    bad[mlp.OFF_C:] = 0.0                          # both head banks
+    lib.wsurr_params(bad)
+    try:
+        iq = 48
+        probe = surrogate.SigmaProbe(work, iq)
+        wex = work.exact(iq, range(work.nw + 1))
+        sig = probe.sigma(wex, range(work.nw))
+        w, rep = surrogate.surrogate_w(sur, work, probe, iq, trained["held"], 1.0, sig)
+        assert rep["fallback"] and rep["est_mev"] > 1.0, rep
+        assert rep["n_exact"] == work.nw + 1
+        assert float(torch.linalg.vector_norm(w - wex) / torch.linalg.vector_norm(wex)) <= 1e-12
+    finally:
+        lib.wsurr_params(p)
