@@ -7,12 +7,12 @@ frequency w = 0, at a few anchor frequencies and at a few held-out
 frequencies; a network predicts W_c at the other grid points:
 
   * full matrix: a per-target linear head (bank 1) on the normalised anchor
-    values and element features of every element;
+    values of every element;
   * dominant block (the top nb eigenvectors of v, where W_c is largest):
     a second per-target head (bank 0) plus an MLP correction
     (16-256-256-1, BF16 weights).
-Element features: log10 of the Coulomb eigenvalue of the element's row and
-column (/3), re/im, diagonal.  Both heads start from linear interpolation in
+Element features of the dominant block: log10 of the Coulomb eigenvalue of
+the element's row and column (/3), re/im, diagonal.  Both heads start from linear interpolation in
 the Gauss-Legendre coordinate x, are then set by weighted least squares, and
 bank 0 and the MLP are trained with Adam.
 
@@ -23,8 +23,8 @@ backward, Adam, head, scatter) runs in this library's own kernels.
 
 Validation: the network also predicts the held-out frequencies; the
 imaginary-axis Sigma_c change that the prediction error there causes,
-scaled by sqrt(predicted / held-out frequencies), estimates the QP-energy
-error.  Above the tolerance (1 meV) the q point falls back to the plain
+scaled by n_pred / n_held, estimates the QP-energy error (largest over
+the states).  Above the tolerance (1 meV) the q point falls back to the plain
 method at every frequency.
 
 W_c slots on the device: (nslot, N, N) complex, slot 0 = w = 0, slot 1 + i =
@@ -191,9 +191,10 @@ class WcSurrogate:
         if with_y:
             d["y"] = t.empty(n, dtype=t.float32, device="cuda")
             d["w"] = t.empty(n, dtype=t.float32, device="cuda")
-        rid, cid = (self.idx, self.idx) if bank == 0 else (self.rand_r, self.rand_c)
+        # element features on the dominant block only (they do not help the linear full-matrix bank)
+        ftab = self.ftab if bank == 0 else None
         lib.wsurr_features_d(proj, nq, ns, ne, self.aslot, tsl, thead, self.work.xslot, d["x"], d["tix"],
-                             d.get("y"), d.get("w"), d["scale"], rid=rid, cid=cid, ftab=self.ftab)
+                             d.get("y"), d.get("w"), d["scale"], rid=self.idx, cid=self.idx, ftab=ftab)
         return d
 
     # ---- training
@@ -226,7 +227,7 @@ class WcSurrogate:
         tsl = [1 + i for i in targets]
         N, ns = self.work.N, w_slots.shape[0]
         thead = [self.FULL + self.targets.index(i) for i in targets]
-        lib.wsurr_head_full_d(w_slots, N, N, ns, self.aslot, tsl, thead, self.work.xslot[tsl], self.ftab)
+        lib.wsurr_head_full_d(w_slots, N, N, ns, self.aslot, tsl, thead, self.work.xslot[tsl])
         d = self.samples(self._project(w_slots, self.idx), 0, targets, with_y=False)
         out = t.empty(d["n"], dtype=t.float32, device="cuda")
         lib.wsurr_forward_d(d["x"], d["tix"], out, d["n"])
@@ -257,7 +258,7 @@ class SigmaProbe:
         self.fr = synth.freq_r_mesh(nreal)
         self.ef, self.esmr = 0.0, 0.01
         self.nwxi, self.nwx, ntmax = sched.get_nwx(self.omega, self.ekc, self.fr, self.ef, self.esmr)
-        self.ns2r = min(nm, ntmax)
+        self.ns2r = 0                       # no real-axis pole columns: only the imaginary-axis part
         self.wr = t.zeros(N * N * nreal, dtype=t.complex128, device="cuda")
         self.ntq, self.nm = ntq, nm
 
@@ -302,27 +303,39 @@ def surrogate_w(sur, work, probe, iq, held, tol_mev=1.0, sig_scale=None, inp=Non
     """W_c of q point iq on the whole grid by the surrogate path: exact at w = 0,
     the anchors and the held-out points, predicted elsewhere; validated on the
     held-out points, recomputed exactly at every predicted point when the
-    estimated QP error exceeds tol_mev.  Returns (w_slots, report)."""
+    estimated QP error exceeds tol_mev.  Returns (w_slots, report); the report
+    holds the device time of each phase (ms)."""
     t, N, nw = work.torch, work.N, work.nw
     inp = inp or work.q_inputs(iq)
     pred = [i for i in sur.targets if i not in held]
     exact_slots = [0] + sur.aslot + [1 + h for h in held]
+    ev = [t.cuda.Event(enable_timing=True) for _ in range(5)]
+    ev[0].record()
     w = t.zeros((nw + 1, N, N), dtype=t.complex128, device="cuda")
     work.exact(iq, exact_slots, out=w, inp=inp)
+    ev[1].record()
     hs = t.tensor([1 + h for h in held], device="cuda")
     wheld = w[hs].clone()
     sur.predict(w)
+    ev[2].record()
     dsig_held = probe.delta(w[hs] - wheld, held)
     w[hs] = wheld
+    ev[3].record()
     if sig_scale is None:
         sig_scale = probe.sigma(w, range(nw))
-    # errors of different frequencies are close to independent: their sum over
-    # the predicted points grows like sqrt(n_pred / n_held) times the held-out sum
-    est = qp_mev(dsig_held, sig_scale) * math.sqrt(len(pred) / len(held))
+    # the held-out points sample the predicted ones (midway between anchors,
+    # where interpolation errors peak): their Sigma_c change, scaled by
+    # n_pred / n_held, estimates the change from all predicted points
+    est = qp_mev(dsig_held, sig_scale) * len(pred) / len(held)
     fallback = est > tol_mev
     if fallback:
         work.exact(iq, [1 + i for i in pred], out=w, inp=inp)
-    return w, dict(est_mev=est, fallback=bool(fallback), n_exact=len(exact_slots) + (len(pred) if fallback else 0))
+    ev[4].record()
+    t.cuda.synchronize()
+    phases = dict(exact_ms=ev[0].elapsed_time(ev[1]), predict_ms=ev[1].elapsed_time(ev[2]),
+                  validate_ms=ev[2].elapsed_time(ev[3]), fallback_ms=ev[3].elapsed_time(ev[4]))
+    return w, dict(est_mev=est, fallback=bool(fallback), n_exact=len(exact_slots) + (len(pred) if fallback else 0),
+                   **phases)
 
 
 def prediction_errors(sur, work, probe, wex, sig, pred, params):
@@ -347,17 +360,19 @@ def prediction_errors(sur, work, probe, wex, sig, pred, params):
 
 
 def study(N=600, nq_train=48, nq_test=16, nw=48, nb=64, schedule=((1e-3, 2000), (3e-4, 1500), (1e-4, 1000)),
-          tol_mev=1.0, seed=20263, nm=400, ntq=40, log=None):
+          tol_mev=1.0, seed=20263, nm=400, ntq=40, precision="split", log=None):
     """Train on exact W_c of nq_train q points, then run the surrogate path on
     nq_test other q points and compare with the plain method (all frequencies
     exact).  Per test q: errors of the linear interpolation the heads start
     from, of the least-squares heads alone, and of the trained network; the
     surrogate path's validation estimate, fallback and time against the
-    plain method's."""
+    plain method's (in FP64 and in the path's precision)."""
     import torch as t
     log = log or (lambda m: None)
     if t.cuda.current_stream().cuda_stream == 0:
         lib.share_torch_stream()
+    prec = {"split": lib.PREC_SPLIT_F16, "fp64": lib.PREC_FP64}[precision]
+    lib.set_precision(prec)
     work = Workload(N=N, nw=nw, seed=seed)
     anchors, targets, held = split_grid(nw)
     pred = [i for i in targets if i not in held]
@@ -378,21 +393,31 @@ def study(N=600, nq_train=48, nq_test=16, nw=48, nb=64, schedule=((1e-3, 2000), 
     for iq in range(nq_train, nq_train + nq_test):
         inp = work.q_inputs(iq)
         probe = SigmaProbe(work, iq, ntq=ntq, nm=nm)
+        lib.set_precision(lib.PREC_FP64)
+        wex64, ms_plain64 = _ms(t, lambda: work.exact(iq, allslots, inp=inp))
+        lib.set_precision(prec)
         wex, ms_plain = _ms(t, lambda: work.exact(iq, allslots, inp=inp))
         sig = probe.sigma(wex, range(nw))
-        r = dict(iq=iq, ms_plain=ms_plain, sig_mean_abs_ha=float(np.mean(np.abs(sig))))
+        r = dict(iq=iq, ms_plain=ms_plain, ms_plain_fp64=ms_plain64, sig_mean_abs_ha=float(np.mean(np.abs(sig))))
         for name, prm in variants.items():
             r[name] = prediction_errors(sur, work, probe, wex, sig, pred, prm)
         lib.wsurr_params(p_trained)
         (wsur, rep), ms_sur = _ms(t, lambda: surrogate_w(sur, work, probe, iq, held, tol_mev, sig, inp))
         r.update(rep, ms_surrogate=ms_sur)
         r["qp_mev_final"] = qp_mev(probe.delta((wsur - wex)[ps], pred), sig)
+        lib.set_precision(lib.PREC_FP64)
+        sig64 = probe.sigma(wex64, range(nw))
+        lib.set_precision(prec)
+        r["qp_mev_final_vs_fp64"] = qp_mev(probe.sigma(wsur, range(nw)) - sig64, sig64)
         rows.append(r)
         log(f"q {iq}: W rel linear {r['linear']['w_rel']:.2e} lsq {r['lsq']['w_rel']:.2e} trained "
             f"{r['trained']['w_rel']:.2e} (block {r['linear']['w_rel_block']:.2e} / {r['lsq']['w_rel_block']:.2e} / "
             f"{r['trained']['w_rel_block']:.2e}); QP meV {r['linear']['qp_mev']:.3f} / {r['lsq']['qp_mev']:.3f} / "
             f"{r['trained']['qp_mev']:.3f}; est {r['est_mev']:.3f}, fallback {r['fallback']}, final "
-            f"{r['qp_mev_final']:.3f}; {ms_sur:.1f} ms vs plain {ms_plain:.1f} ms")
-        del wex, wsur, probe
-    return dict(rows=rows, train_log=tr_log, train_seconds=sur.train_seconds, train_samples=sur.train_samples,
+            f"{r['qp_mev_final']:.3f} (vs FP64 plain {r['qp_mev_final_vs_fp64']:.3f}); {ms_sur:.1f} ms "
+            f"(exact {r['exact_ms']:.1f}, predict {r['predict_ms']:.1f}, validate {r['validate_ms']:.1f}, "
+            f"fallback {r['fallback_ms']:.1f}) vs plain {ms_plain:.1f} ms, plain FP64 {ms_plain64:.1f} ms")
+        del wex, wex64, wsur, probe
+    lib.set_precision(lib.PREC_FP64)
+    return dict(rows=rows, train_log=tr_log, precision=precision, train_seconds=sur.train_seconds, train_samples=sur.train_samples,
                 anchors=anchors, held=held, predicted=pred, surrogate=sur, work=work)
