@@ -278,6 +278,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the W_c frequency-interpolator study")
     ap.add_argument("--nq", type=int, default=None, help="Sigma_c tasks (default: the configuration's 64)")
     ap.add_argument("--nk", type=int, default=None, help="k-points of the chi0 part (profiling only)")
     args = ap.parse_args()
@@ -412,6 +413,10 @@ def main():
     if not args.no_e2e:
         lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
         e2e = run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist)
+    sur = None
+    if not args.no_surrogate:
+        sur = surrogate_summary(lib, log)
+        lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline()
@@ -428,10 +433,43 @@ def main():
                            "flops_per_step": flops, "flops_chi0": fl_chi, "flops_sigc": fl_sig},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "kernel_ms": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]},
-                "fp64_peak_tflops": round(fp64_peak, 3), "compare": compare}
+                "fp64_peak_tflops": round(fp64_peak, 3), "compare": compare, "surrogate": sur}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
+
+
+def surrogate_summary(lib, log, nq_test=8):
+    """W_c(q, iw) on the 48-point imaginary grid (N=600, Sigma_c configuration
+    generator): the plain method (every frequency exact, FP64 and split) against
+    the split path with the learned frequency interpolator (17 of 49 slots
+    exact, validated, fallback above 1 meV), on q points not trained on."""
+    from ecalj_b200 import surrogate
+    res = surrogate.study(N=600, nq_train=48, nq_test=nq_test, precision="split", log=log)
+    rows = res["rows"]
+    mean = lambda k: float(np.mean([r[k] for r in rows]))
+    out = {"workload": "c3: exact W_c on 48 iw x 48 training q at N=600, 8 anchors, 8 held-out, 32 predicted; "
+                       f"{nq_test} test q",
+           "ms_w_plain_fp64": round(mean("ms_plain_fp64"), 3), "ms_w_plain_split": round(mean("ms_plain"), 3),
+           "ms_w_surrogate": round(mean("ms_surrogate"), 3),
+           "speedup_vs_plain_fp64": round(mean("ms_plain_fp64") / mean("ms_surrogate"), 3),
+           "speedup_vs_plain_split": round(mean("ms_plain") / mean("ms_surrogate"), 3),
+           "phases_ms": {k: round(mean(k), 3) for k in ("exact_ms", "predict_ms", "validate_ms", "fallback_ms")},
+           "fallbacks": int(sum(r["fallback"] for r in rows)),
+           "qp_err_mev_max_vs_fp64_plain": max(r["qp_mev_final_vs_fp64"] for r in rows),
+           "qp_err_mev_max_prediction": max(r["trained"]["qp_mev"] for r in rows),
+           "qp_err_mev_max_linear_interp": max(r["linear"]["qp_mev"] for r in rows),
+           "qp_err_mev_max_least_squares": max(r["lsq"]["qp_mev"] for r in rows),
+           "w_rel_err": {k: mean_d(rows, k) for k in ("linear", "lsq", "trained")},
+           "est_over_true": [round(r["est_mev"] / max(r["trained"]["qp_mev"], 1e-12), 2) for r in rows],
+           "train_seconds": round(res["train_seconds"], 3), "train_samples": res["train_samples"],
+           "qp_scale": "Sigma_c normalised to a mean |Re Sigma_c,nn| of 5 eV"}
+    return out
+
+
+def mean_d(rows, k):
+    return {"full": float(np.mean([r[k]["w_rel"] for r in rows])),
+            "dominant_block": float(np.mean([r[k]["w_rel_block"] for r in rows]))}
 
 
 def measure_fp64_peak():
