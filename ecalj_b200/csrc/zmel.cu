@@ -123,6 +123,81 @@ __global__ void conj_kernel(double2* a, long long n) {
 
 static DevBuf g_zm_atoms;
 
+// ---- interstitial plane-wave part (m_zmel.f90:418-535)
+// M(c, g) = ggg(sg * vg(g) - vc(c) - nadd) or 0 when that vector is not in the ggg table.
+__global__ void ipw_gmat_kernel(double2* __restrict__ M, int ncgp, int ng, const int* __restrict__ vc,
+                                const int* __restrict__ vg, int sg, int ax, int ay, int az,
+                                const int* __restrict__ box, int x0, int nx, int y0, int ny, int z0, int nz,
+                                const double2* __restrict__ ggg) {
+  const long long tot = static_cast<long long>(ncgp) * ng;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(e % ncgp), g = static_cast<int>(e / ncgp);
+    const int x = sg * vg[3 * g] - vc[3 * c] - ax - x0;
+    const int y = sg * vg[3 * g + 1] - vc[3 * c + 1] - ay - y0;
+    const int z = sg * vg[3 * g + 2] - vc[3 * c + 2] - az - z0;
+    double2 v = make_double2(0.0, 0.0);
+    if (x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz) {
+      const int k = box[x + nx * (y + ny * z)];
+      if (k >= 0) v = ggg[k];
+    }
+    M[e] = v;
+  }
+}
+
+// Tg[k + nidx b] = T[cidx[k] + ldt b]
+__global__ void gather_rows_kernel(double2* __restrict__ Tg, const double2* __restrict__ T, int ldt,
+                                   const int* __restrict__ cidx, long long nidx, int nbatch) {
+  const long long tot = nidx * nbatch;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long k = e % nidx, b = e / nidx;
+    Tg[e] = T[cidx[k] + static_cast<long long>(ldt) * b];
+  }
+}
+
+// zmelt(row0 + igc, it0 + it, itp) = phase(igc) * Z(igc, it, itp)
+__global__ void ipw_scatter_kernel(double2* __restrict__ zt, int ldz, int row0, int it0, int nmtot,
+                                   const double2* __restrict__ Z, int ngc, int nmv, int ntp0,
+                                   const double2* __restrict__ phase) {
+  const long long tot = static_cast<long long>(ngc) * nmv * ntp0;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int igc = static_cast<int>(e % ngc);
+    const long long r = e / ngc;
+    const int it = static_cast<int>(r % nmv), itp = static_cast<int>(r / nmv);
+    const double2 p = phase[igc], z = Z[e];
+    zt[row0 + igc + static_cast<long long>(ldz) * (it0 + it + static_cast<long long>(nmtot) * itp)] =
+        make_double2(p.x * z.x - p.y * z.y, p.x * z.y + p.y * z.x);
+  }
+}
+
+// Inverse table of a list of integer 3-vectors over their bounding box (-1 = absent).
+struct Box {
+  int x0 = 0, nx = 0, y0 = 0, ny = 0, z0 = 0, nz = 0;
+  std::vector<int> map;
+  void build(const int* v, int n) {
+    int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+    for (int i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], v[3 * i + d]); hi[d] = std::max(hi[d], v[3 * i + d]); }
+    x0 = lo[0]; y0 = lo[1]; z0 = lo[2];
+    nx = hi[0] - lo[0] + 1; ny = hi[1] - lo[1] + 1; nz = hi[2] - lo[2] + 1;
+    map.assign(static_cast<size_t>(nx) * ny * nz, -1);
+    for (int i = 0; i < n; ++i) map[(v[3 * i] - x0) + static_cast<size_t>(nx) * ((v[3 * i + 1] - y0) + static_cast<size_t>(ny) * (v[3 * i + 2] - z0))] = i;
+  }
+  int find(int x, int y, int z) const {
+    x -= x0; y -= y0; z -= z0;
+    if (x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz) return -1;
+    return map[x + static_cast<size_t>(nx) * (y + static_cast<size_t>(ny) * z)];
+  }
+};
+
+static DevBuf g_ipw_tab, g_ipw_m, g_ipw_t, g_ipw_tg, g_ipw_z;
+
+static int ipw_grid(long long n) {
+  return static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 16LL * ctx().sm_count)));
+}
+
 }  // namespace qsgw
 
 using namespace qsgw;
@@ -198,5 +273,94 @@ extern "C" int qsgw_zmel_m2e_d(double* zmel_d, const double* zmelt_d, int ngb, i
     count_launch();
     QSGW_LAUNCH_CHECK("conj_kernel");
   }
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_zmel_ipw_d(const qsgw_zmel_ipw_args* a) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(a, "zmel_ipw: null argument block");
+  const int ngc = a->ngc, ngp1 = a->ngp1, ngp2 = a->ngp2, ngcgp = a->ngcgp, nggg = a->nggg, ntp0 = a->ntp0;
+  const int nmv = a->nm2v - a->nm1v + 1, nmtot = a->nm2 - a->nm1 + 1;
+  if (ngc == 0 || nmv <= 0) return QSGW_OK;                        // :418 guard
+  QSGW_ARG(ngc > 0 && ngp1 >= 1 && ngp2 >= 1 && ngcgp >= 1 && nggg >= 1 && ntp0 >= 1 && nmtot >= 1,
+           "zmel_ipw: sizes ngc=%d ngp1=%d ngp2=%d ngcgp=%d nggg=%d ntp0=%d", ngc, ngp1, ngp2, ngcgp, nggg, ntp0);
+  QSGW_ARG(a->nm1v >= a->nm1 && a->nm2v <= a->nm2, "zmel_ipw: valence %d..%d outside %d..%d", a->nm1v, a->nm2v,
+           a->nm1, a->nm2);
+  QSGW_ARG(a->ngvecpB1 && a->ngvecpB2 && a->ngveccR && a->nvgcgp2 && a->nvggg && a->ggg && a->phase && a->geigq_d &&
+               a->dgeigqk_d && a->zmelt_d,
+           "zmel_ipw: null pointer");
+  QSGW_ARG(a->row0 >= 0 && a->ldz >= a->row0 + ngc && a->ldgq >= ngp1 && a->ldgk >= ngp2,
+           "zmel_ipw: leading dimensions ldz=%d (row0=%d) ldgq=%d ldgk=%d", a->ldz, a->row0, a->ldgq, a->ldgk);
+  Box bg, bc;
+  bg.build(a->nvggg, nggg);
+  bc.build(a->nvgcgp2, ngcgp);
+  // branch of the reference (:439): G1 integral first when the middle states outnumber the targets
+  const bool g1first = nmv > ntp0;
+  const int ngA = g1first ? ngp1 : ngp2;                 // plane waves contracted with the ggg matrix
+  const int ngB = g1first ? ngp2 : ngp1;                 // plane waves of the gathered contraction
+  const int* vA = g1first ? a->ngvecpB1 : a->ngvecpB2;
+  const int* vB = g1first ? a->ngvecpB2 : a->ngvecpB1;
+  const int ncolT = g1first ? ntp0 : nmv, nbat = g1first ? ntp0 : nmv;
+  // composite index of Gc + G2 (G1 first, :464-466) or Gc - G1 (G2 first, :507-509), validated here
+  std::vector<int> cidx(static_cast<size_t>(ngc) * ngB);
+  for (int g = 0; g < ngB; ++g)
+    for (int c = 0; c < ngc; ++c) {
+      const int sg = g1first ? 1 : -1;
+      const int k = bc.find(a->ngveccR[3 * c] + sg * vB[3 * g], a->ngveccR[3 * c + 1] + sg * vB[3 * g + 1],
+                            a->ngveccR[3 * c + 2] + sg * vB[3 * g + 2]);
+      QSGW_ARG(k >= 0, "zmel_ipw: composite vector of Gc %d and plane wave %d is not in nvgcgp2", c + 1, g + 1);
+      cidx[c + static_cast<size_t>(ngc) * g] = k;
+    }
+  cudaStream_t s = ctx().stream;
+  // device tables: box map, cidx, vectors (ints); ggg, phase (complex)
+  const size_t nbox = bg.map.size(), ni = nbox + cidx.size() + 3 * static_cast<size_t>(ngcgp) + 3 * static_cast<size_t>(ngA);
+  const size_t ioff_c = nbox, ioff_vc = ioff_c + cidx.size(), ioff_va = ioff_vc + 3 * static_cast<size_t>(ngcgp);
+  const size_t ibytes = ((ni * sizeof(int) + 15) / 16) * 16;
+  rc = g_ipw_tab.ensure(ibytes + (static_cast<size_t>(nggg) + ngc) * sizeof(double2));
+  if (rc) return rc;
+  int* di = g_ipw_tab.as<int>();
+  double2* dz = reinterpret_cast<double2*>(g_ipw_tab.as<char>() + ibytes);
+  QSGW_CUDA(cudaMemcpyAsync(di, bg.map.data(), nbox * sizeof(int), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(di + ioff_c, cidx.data(), cidx.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(di + ioff_vc, a->nvgcgp2, 3 * static_cast<size_t>(ngcgp) * sizeof(int), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(di + ioff_va, vA, 3 * static_cast<size_t>(ngA) * sizeof(int), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(dz, a->ggg, static_cast<size_t>(nggg) * sizeof(double2), cudaMemcpyHostToDevice, s));
+  QSGW_CUDA(cudaMemcpyAsync(dz + nggg, a->phase, static_cast<size_t>(ngc) * sizeof(double2), cudaMemcpyHostToDevice, s));
+  // scratch: M (ngcgp x ngA), T (ngcgp x ncolT), Tg (ngc x ngB x nbat), Z (ngc x nmv x ntp0)
+  if ((rc = g_ipw_m.ensure(static_cast<size_t>(ngcgp) * ngA * sizeof(double2)))) return rc;
+  if ((rc = g_ipw_t.ensure(static_cast<size_t>(ngcgp) * ncolT * sizeof(double2)))) return rc;
+  if ((rc = g_ipw_tg.ensure(static_cast<size_t>(ngc) * ngB * nbat * sizeof(double2)))) return rc;
+  if ((rc = g_ipw_z.ensure(static_cast<size_t>(ngc) * nmv * ntp0 * sizeof(double2)))) return rc;
+  double2 *M = g_ipw_m.as<double2>(), *T = g_ipw_t.as<double2>(), *Tg = g_ipw_tg.as<double2>(),
+          *Z = g_ipw_z.as<double2>();
+  const double2* geigq = reinterpret_cast<const double2*>(a->geigq_d);
+  const double2* dgk = reinterpret_cast<const double2*>(a->dgeigqk_d);
+  const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+  ipw_gmat_kernel<<<ipw_grid(static_cast<long long>(ngcgp) * ngA), 256, 0, s>>>(
+      M, ngcgp, ngA, di + ioff_vc, di + ioff_va, g1first ? 1 : -1, a->nadd[0], a->nadd[1], a->nadd[2], di, bg.x0, bg.nx,
+      bg.y0, bg.ny, bg.z0, bg.nz, dz);
+  count_launch();
+  QSGW_LAUNCH_CHECK("ipw_gmat_kernel");
+  // T = M * geigq (:458) or M * dgeigqk (:501)
+  rc = zgemm_f64(0, 0, ngcgp, ncolT, ngA, one, M, ngcgp, 0, g1first ? geigq : dgk, g1first ? a->ldgq : a->ldgk, 0,
+                 zero, T, ngcgp, 0, 1, s);
+  if (rc) return rc;
+  const long long nidx = static_cast<long long>(ngc) * ngB;
+  gather_rows_kernel<<<ipw_grid(nidx * nbat), 256, 0, s>>>(Tg, T, ngcgp, di + ioff_c, nidx, nbat);
+  count_launch();
+  QSGW_LAUNCH_CHECK("gather_rows_kernel");
+  if (g1first)   // Z(:, :, itp) = Tg(:, :, itp) * dgeigqk  (:470-479), batched over itp
+    rc = zgemm_f64(0, 0, ngc, nmv, ngp2, one, Tg, ngc, nidx, dgk, a->ldgk, 0, zero, Z, ngc,
+                   static_cast<long long>(ngc) * nmv, ntp0, s);
+  else           // Z(:, it, :) = Tg(:, :, it) * geigq  (:513-521), batched over it
+    rc = zgemm_f64(0, 0, ngc, ntp0, ngp1, one, Tg, ngc, nidx, geigq, a->ldgq, 0, zero, Z,
+                   static_cast<long long>(ngc) * nmv, ngc, nmv, s);
+  if (rc) return rc;
+  ipw_scatter_kernel<<<ipw_grid(static_cast<long long>(ngc) * nmv * ntp0), 256, 0, s>>>(
+      reinterpret_cast<double2*>(a->zmelt_d), a->ldz, a->row0, a->nm1v - a->nm1, nmtot, Z, ngc, nmv, ntp0, dz + nggg);
+  count_launch();
+  QSGW_LAUNCH_CHECK("ipw_scatter_kernel");
+  QSGW_CUDA(cudaStreamSynchronize(s));                                // host tables above die on return
   return QSGW_OK;
 }

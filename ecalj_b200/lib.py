@@ -54,6 +54,16 @@ class ZmelAtom(ctypes.Structure):
                 ("phase_re", c_dbl), ("phase_im", c_dbl)]
 
 
+class ZmelIpwArgs(ctypes.Structure):
+    """Mirror of ``qsgw_zmel_ipw_args``."""
+    _fields_ = [("ngc", c_int), ("ngp1", c_int), ("ngp2", c_int), ("ngcgp", c_int), ("nggg", c_int),
+                ("ntp0", c_int), ("nm1", c_int), ("nm2", c_int), ("nm1v", c_int), ("nm2v", c_int),
+                ("ldz", c_int), ("row0", c_int), ("nadd", c_int * 3),
+                ("ngvecpB1", c_vp), ("ngvecpB2", c_vp), ("ngveccR", c_vp), ("nvgcgp2", c_vp), ("nvggg", c_vp),
+                ("ggg", c_vp), ("phase", c_vp), ("geigq_d", c_vp), ("ldgq", c_int), ("dgeigqk_d", c_vp),
+                ("ldgk", c_int), ("zmelt_d", c_vp)]
+
+
 _SIGS = {
     "qsgw_init": [c_int],
     "qsgw_finalize": [],
@@ -86,6 +96,7 @@ _SIGS = {
     "qsgw_zmel_mt_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_int,
                        ctypes.POINTER(ZmelAtom)],
     "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
+    "qsgw_zmel_ipw_d": [c_vp],
     "qsgw_zhegv_d": [c_vp, c_vp, c_int, c_int, c_vp],
     "qsgw_wsurr_init": [ctypes.c_ulonglong],
     "qsgw_wsurr_nparam": [],
@@ -373,6 +384,26 @@ def zmel_mt_d(zmelt, nbloch, nm1, nm2, nctot, ntp0, cphim, ldm, cphiq, ldq, atom
                           a["ncore"], float(np.real(a["phase"])), float(np.imag(a["phase"])))
     _chk(load().qsgw_zmel_mt_d(_p(zmelt), nbloch, nm1, nm2, nctot, ntp0, _p(cphim), ldm, _p(cphiq), ldq,
                                len(atoms), arr))
+    return zmelt
+
+
+def zmel_ipw_d(zmelt, ldz, row0, nm1, nm2, nm1v, nm2v, ntp0, geigq, ldgq, dgeigqk, ldgk, ngvecpB1, ngvecpB2,
+               ngveccR, nvgcgp2, nvggg, ggg, nadd, phase):
+    """Interstitial plane-wave rows of zmelt (m_zmel.f90:418-535).  Integer
+    vector tables are (3, n) arrays; ggg, phase complex host arrays."""
+    iv = [np.asfortranarray(np.asarray(v, dtype=np.int32)) for v in (ngvecpB1, ngvecpB2, ngveccR, nvgcgp2, nvggg)]
+    for v in iv:
+        if v.ndim != 2 or v.shape[0] != 3:
+            raise ValueError("G-vector tables must be (3, n)")
+    g = np.ascontiguousarray(ggg, dtype=np.complex128)
+    ph = np.ascontiguousarray(phase, dtype=np.complex128)
+    a = ZmelIpwArgs(ngc=iv[2].shape[1], ngp1=iv[0].shape[1], ngp2=iv[1].shape[1], ngcgp=iv[3].shape[1],
+                    nggg=iv[4].shape[1], ntp0=ntp0, nm1=nm1, nm2=nm2, nm1v=nm1v, nm2v=nm2v, ldz=ldz, row0=row0,
+                    nadd=(c_int * 3)(*[int(x) for x in nadd]), ngvecpB1=iv[0].ctypes.data, ngvecpB2=iv[1].ctypes.data,
+                    ngveccR=iv[2].ctypes.data, nvgcgp2=iv[3].ctypes.data, nvggg=iv[4].ctypes.data,
+                    ggg=g.ctypes.data, phase=ph.ctypes.data, geigq_d=_p(geigq), ldgq=ldgq, dgeigqk_d=_p(dgeigqk),
+                    ldgk=ldgk, zmelt_d=_p(zmelt))
+    _chk(load().qsgw_zmel_ipw_d(ctypes.byref(a)))
     return zmelt
 
 

@@ -110,3 +110,31 @@ def real_axis_model(wc0, freq_r, wp=0.5):
     only on the imaginary axis): W_c(w) = W_c(0) / (1 + (w/wp)^2)."""
     g = 1.0 / (1.0 + (np.asarray(freq_r) / wp) ** 2)
     return np.asfortranarray(wc0[:, :, None] * g[None, None, :])
+
+
+def ipw_tables(seed, ngc=37, ngp1=29, ngp2=31, ntp0=5, nmv=7, span=2, gbox=6, fill=0.8):
+    """G-vector tables of the interstitial plane-wave part of zmel with the
+    structure getppx2 reads (rppovl.f90:40-66): plane waves at q (ngvecpB1)
+    and q-k (ngvecpB2), product-basis G (ngveccR), composite vectors nvgcgp2
+    holding every Gc+G2 and Gc-G1, and a ggg table on a box with a fraction
+    `fill` of its vectors present (the rest read as zero)."""
+    rng = np.random.default_rng(seed)
+    pts = np.array(np.meshgrid(*[np.arange(-span, span + 1)] * 3, indexing="ij")).reshape(3, -1)
+
+    def pick(n):
+        return pts[:, rng.choice(pts.shape[1], n, replace=False)].astype(np.int32)
+
+    b1, b2, gc = pick(ngp1), pick(ngp2), pick(ngc)
+    comp = {tuple(gc[:, c] + b2[:, g]) for c in range(ngc) for g in range(ngp2)}
+    comp |= {tuple(gc[:, c] - b1[:, g]) for c in range(ngc) for g in range(ngp1)}
+    comp = np.array(sorted(comp), np.int32).T
+    comp = comp[:, rng.permutation(comp.shape[1])]
+    box = np.array(np.meshgrid(*[np.arange(-gbox, gbox + 1)] * 3, indexing="ij")).reshape(3, -1)
+    keep = rng.random(box.shape[1]) < fill
+    nvggg = box[:, keep][:, rng.permutation(int(keep.sum()))].astype(np.int32)
+    ggg = rng.standard_normal(nvggg.shape[1]) + 1j * rng.standard_normal(nvggg.shape[1])
+    geigq = rng.standard_normal((ngp1, ntp0)) + 1j * rng.standard_normal((ngp1, ntp0))
+    dgeigqk = rng.standard_normal((ngp2, nmv)) + 1j * rng.standard_normal((ngp2, nmv))
+    phase = np.exp(-2j * np.pi * rng.random(ngc))
+    return dict(ngvecpB1=b1, ngvecpB2=b2, ngveccR=gc, nvgcgp2=comp, nvggg=nvggg, ggg=ggg, geigq=geigq,
+                dgeigqk=dgeigqk, phase=phase, nadd=np.array([1, 0, -1], np.int32))

@@ -246,6 +246,35 @@ int qsgw_zmel_mt_d(double *zmelt_d, int nbloch, int nm1, int nm2, int nctot,
                    int ntp0, const double *cphim_d, int ldm,
                    const double *cphiq_d, int ldq, int natom,
                    const qsgw_zmel_atom *atoms);
+/* Interstitial plane-wave part of get_zmel_init_gemm (m_zmel.f90:418-535):
+ *   zmelt(row0+igc, it, itp) = phase(igc) * sum_{G1,G2} ggg(G1 - (Gc+G2) - nadd)
+ *                              * geigq(G1, itp) * dgeigqk(G2, it)
+ * for it = nm1v..nm2v (middle index of zmelt nm1..nm2), itp = 1..ntp0.
+ * The G-vector tables are the reference's (getppx2, rppovl.f90:40-66):
+ * nvggg/ggg (the ggg table), nvgcgp2 (composite vectors Gc+G2 and Gc-G1),
+ * ngvecpB1/ngvecpB2 (plane waves at q and q-k), ngveccR (rotated Gc); the
+ * inverse tables are built here.  The G1-first or G2-first order follows
+ * the reference's choice (:439).  A composite vector missing from nvgcgp2
+ * is an argument error.                                                    */
+typedef struct qsgw_zmel_ipw_args {
+  int ngc, ngp1, ngp2, ngcgp, nggg;
+  int ntp0, nm1, nm2, nm1v, nm2v;
+  int ldz, row0;               /* zmelt_d (ldz, nm1:nm2, ntp0); row0 = nbloch    */
+  int nadd[3];
+  const int *ngvecpB1;         /* host (3, ngp1) */
+  const int *ngvecpB2;         /* host (3, ngp2) */
+  const int *ngveccR;          /* host (3, ngc)  */
+  const int *nvgcgp2;          /* host (3, ngcgp) */
+  const int *nvggg;            /* host (3, nggg) */
+  const double *ggg;           /* host complex (nggg) */
+  const double *phase;         /* host complex (ngc) */
+  const double *geigq_d;       /* device complex (ldgq, ntp0) */
+  int ldgq;
+  const double *dgeigqk_d;     /* device complex (ldgk, nm1v:nm2v), conjugated */
+  int ldgk;
+  double *zmelt_d;
+} qsgw_zmel_ipw_args;
+int qsgw_zmel_ipw_d(const qsgw_zmel_ipw_args *args);
 /* M->E change and conjugation (m_zmel.f90:546-563, 590-594):
  * zmel(nbb, nmtot*nqtot) = m2e^H zmelt (or a copy when is_m_basis), then
  * conj when zmelconjg.  m2e: device (ngb, nbb).                            */

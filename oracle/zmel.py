@@ -1,5 +1,6 @@
 """Product-basis matrix elements <psi|psi M>: restatement of the muffin-tin
-part and of the M->E change of get_zmel_init_gemm.  Test infrastructure only."""
+part, the interstitial plane-wave part and the M->E change of
+get_zmel_init_gemm.  Test infrastructure only."""
 import numpy as np
 
 
@@ -57,3 +58,30 @@ def zmel_m2e(zmelt, m2e, is_m_basis, zmelconjg):
         z = (m2e.conj().T @ zmelt.reshape(ngb, nm * nt, order='F')).reshape(
             m2e.shape[1], nm, nt, order='F')
     return z.conj() if zmelconjg else z
+
+
+def zmel_ipw(geigq, dgeigqk, ngvecpB1, ngvecpB2, ngveccR, nvggg, ggg, nadd, phase):
+    """SRC/subroutines/m_zmel.f90:418-535, the definition both of its branches
+    (G1 integral first, :439-480, or G2 first, :481-524) evaluate:
+
+        zmelp0(igc, it, itp) = sum_{G1, G2} ggg(G1 - (Gc + G2) - nadd)
+                                * geigq(G1, itp) * dgeigqk(G2, it)
+        rows nbloch+igc of zmelt = phase(igc) * zmelp0            (:528-532)
+
+    ggg(v) is the entry of nvggg equal to v, zero when v is absent (the
+    reference skips igggi <= 0, :453-454).
+    geigq (ngp1, ntp0), dgeigqk (ngp2, nmv) complex (dgeigqk already conj'ed);
+    ngvecpB1 (3, ngp1), ngvecpB2 (3, ngp2), ngveccR (3, ngc), nvggg (3, nggg)
+    integer; returns (ngc, nmv, ntp0) complex128."""
+    lut = {tuple(int(c) for c in nvggg[:, i]): ggg[i] for i in range(nvggg.shape[1])}
+    ngc, ngp1, ngp2 = ngveccR.shape[1], ngvecpB1.shape[1], ngvecpB2.shape[1]
+    nadd = np.asarray(nadd)
+    out = np.zeros((ngc, dgeigqk.shape[1], geigq.shape[1]), np.complex128)
+    for igc in range(ngc):
+        m = np.zeros((ngp1, ngp2), np.complex128)               # m(G1, G2) = ggg(G1 - Gc - G2 - nadd)
+        for a in range(ngp1):
+            for b in range(ngp2):
+                v = ngvecpB1[:, a] - ngveccR[:, igc] - ngvecpB2[:, b] - nadd
+                m[a, b] = lut.get(tuple(int(c) for c in v), 0.0)
+        out[igc] = phase[igc] * (dgeigqk.T @ m.T @ geigq)      # (nmv, ntp0)
+    return out

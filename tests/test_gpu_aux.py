@@ -89,3 +89,48 @@ def test_zmel_mt_and_m2e_vs_oracle(qsgw, nm1, nm2, nctot):
     qsgw.zmel_m2e_d(out, zt, nbloch, nbloch - 4, nm, ntp0, qsgw.to_device(m2e), False, True)
     qsgw.synchronize()
     assert rel_fro(qsgw.from_device(out, (nbloch - 4, nm, ntp0)), zmel.zmel_m2e(ref, m2e, False, True)) < TOL
+
+
+@pytest.mark.parametrize("ntp0,nmv", [(5, 9), (8, 3)])          # G1-first and G2-first orders
+def test_zmel_ipw_vs_oracle(qsgw, ntp0, nmv):
+    import torch
+    from ecalj_b200 import synth
+    lib = qsgw
+    t = synth.ipw_tables(11 + nmv, ngc=37, ngp1=29, ngp2=31, ntp0=ntp0, nmv=nmv)
+    nbloch, nm1, nm1v = 6, 1, 3
+    nm2 = nm1v + nmv - 1 + 2                                         # two middle states past the valence range
+    nmtot = nm2 - nm1 + 1
+    ngc = t["ngveccR"].shape[1]
+    ldz, ldgq, ldgk = nbloch + ngc + 1, 29 + 3, 31 + 2
+    gq = np.zeros((ldgq, ntp0), complex, order="F")
+    gq[:29] = t["geigq"]
+    gk = np.zeros((ldgk, nmv), complex, order="F")
+    gk[:31] = t["dgeigqk"]
+    z0 = _rc(np.random.default_rng(1), ldz, nmtot, ntp0)
+    zd = lib.to_device(z0)
+    lib.zmel_ipw_d(zd, ldz, nbloch, nm1, nm2, nm1v, nm1v + nmv - 1, ntp0, lib.to_device(gq), ldgq,
+                   lib.to_device(gk), ldgk, t["ngvecpB1"], t["ngvecpB2"], t["ngveccR"], t["nvgcgp2"], t["nvggg"],
+                   t["ggg"], t["nadd"], t["phase"])
+    got = lib.from_device(zd, (ldz, nmtot, ntp0))
+    ref = zmel.zmel_ipw(t["geigq"], t["dgeigqk"], t["ngvecpB1"], t["ngvecpB2"], t["ngveccR"], t["nvggg"],
+                        t["ggg"], t["nadd"], t["phase"])
+    it0 = nm1v - nm1
+    assert rel_fro(got[nbloch:nbloch + ngc, it0:it0 + nmv, :], ref) <= TOL
+    mask = np.ones(got.shape, bool)                                  # nothing else is touched
+    mask[nbloch:nbloch + ngc, it0:it0 + nmv, :] = False
+    np.testing.assert_array_equal(got[mask], z0[mask])
+
+
+def test_zmel_ipw_missing_composite_vector(qsgw):
+    """A Gc+G2 vector absent from nvgcgp2 is an argument error, found on the host."""
+    from ecalj_b200 import synth
+    lib = qsgw
+    t = synth.ipw_tables(4, ngc=9, ngp1=8, ngp2=7, ntp0=3, nmv=4)
+    need = t["ngveccR"][:, 0] + t["ngvecpB2"][:, 0]
+    keep = ~np.all(t["nvgcgp2"] == need[:, None], axis=0)
+    z = lib.to_device(np.zeros((20, 4, 3), complex, order="F"))
+    with pytest.raises(lib.QSGWError) as e:
+        lib.zmel_ipw_d(z, 20, 6, 1, 4, 1, 4, 3, lib.to_device(np.asfortranarray(t["geigq"])), 8,
+                       lib.to_device(np.asfortranarray(t["dgeigqk"])), 7, t["ngvecpB1"], t["ngvecpB2"], t["ngveccR"],
+                       t["nvgcgp2"][:, keep], t["nvggg"], t["ggg"], t["nadd"], t["phase"])
+    assert e.value.code == -1 and "nvgcgp2" in str(e.value)
