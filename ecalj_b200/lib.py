@@ -98,6 +98,8 @@ _SIGS = {
     "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
     "qsgw_zmel_ipw_d": [c_vp],
     "qsgw_zhegv_d": [c_vp, c_vp, c_int, c_int, c_vp],
+    "qsgw_wv_write_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int],
+    "qsgw_wv_read_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int, c_int, c_int],
     "qsgw_wsurr_init": [ctypes.c_ulonglong],
     "qsgw_wsurr_nparam": [],
     "qsgw_wsurr_params": [c_vp, c_int],
@@ -418,6 +420,19 @@ def zhegv_d(v, n, lda=None, o=None):
     returns vcoud (descending eigenvalues of v, O-orthonormal vectors)."""
     out = np.zeros(n)
     _chk(load().qsgw_zhegv_d(_p(v), _p(o), n, lda or n, out.ctypes.data))
+    return out
+
+
+# ---------------------------------------------------------------- W record files
+def wv_write_d(path, zw, nblochpmx, rec0, nrec, kind4=False):
+    """Write records rec0.. of a __WVI/__WVR file from a device W stack."""
+    _chk(load().qsgw_wv_write_d(os.fsencode(path), _p(zw), nblochpmx, rec0, nrec, int(kind4)))
+
+
+def wv_read_d(path, out, nblochpmx, rec0, nrec, kind4=False, pack=0, ngb=0):
+    """Read records into a device buffer: full (pack 0), upper triangle (1) or
+    upper triangle of (W + W^H)/2 (2) of the leading ngb x ngb block."""
+    _chk(load().qsgw_wv_read_d(os.fsencode(path), _p(out), nblochpmx, rec0, nrec, int(kind4), pack, ngb))
     return out
 
 

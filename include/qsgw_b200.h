@@ -290,6 +290,23 @@ int qsgw_zmel_m2e_d(double *zmel_d, const double *zmelt_d, int ngb, int nbb,
  * vcoud: host (n).  FP64 parallel cyclic Jacobi.                          */
 int qsgw_zhegv_d(double *v_d, const double *o_d, int n, int lda, double *vcoud);
 
+/* ---- W record files __WVI.<iq> / __WVR.<iq> in the reference's layout:
+ * fixed records without markers, record rec at byte (rec-1)*recl, one
+ * nblochpmx x nblochpmx column-major matrix per record, complex(8)
+ * (recl = 16 nblochpmx^2) or complex(4) when kind4 != 0 (m_mpiio.f90:12-73,
+ * written at m_llw.f90:177, 373; read at m_sxcf_gemm.f90:317-354).
+ * write: records rec0..rec0+nrec-1 from the device stack zw_d (nrec
+ * matrices); the file is created when missing, other records are kept.
+ * read: pack = 0 -> full matrices into out_d (nrec x nblochpmx^2);
+ * pack = 1 -> upper triangle (i <= j, column by column) of the leading
+ * ngb x ngb block, the WVI form of keepwv; pack = 2 -> the same of
+ * (W + W^H)/2, the WVR form (m_sxcf_gemm.f90:337-354); out_d then holds
+ * nrec x ngb(ngb+1)/2 values.                                              */
+int qsgw_wv_write_d(const char *path, const double *zw_d, int nblochpmx, int rec0,
+                    int nrec, int kind4);
+int qsgw_wv_read_d(const char *path, double *out_d, int nblochpmx, int rec0,
+                   int nrec, int kind4, int pack, int ngb);
+
 /* ---- Learned W_c(q, i w) frequency interpolator.  No counterpart in the
  * reference: it stands in for computing chi0 and W at every frequency of
  * the imaginary grid.  One sample = one real channel of one element of
