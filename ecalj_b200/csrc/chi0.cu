@@ -222,11 +222,32 @@ __global__ void lorentz_weight_kernel(double* __restrict__ w, const int* __restr
   }
 }
 
+// Real frequency axis: f(w) = [1/(w - de + i eta) - 1/(w + de + i eta)] / nk, whose value at
+// w = i nu is the imaginary-axis weight above.  Slot iw holds Re f, slot nw + iw holds Im f.
+__global__ void lorentz_real_weight_kernel(double* __restrict__ w, const int* __restrict__ peo,
+                                           const int* __restrict__ peu, const double* __restrict__ eo,
+                                           const double* __restrict__ eu, const double* __restrict__ fr,
+                                           long long npair, int nw, double eta, double inv_nk) {
+  const long long total = npair * nw;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long pr = i % npair;
+    const int iw = static_cast<int>(i / npair);
+    const double de = eu[peu[pr]] - eo[peo[pr]];
+    const double om = fr[iw];
+    const double a = om - de, b = om + de, e2 = eta * eta;
+    const double da = 1.0 / (a * a + e2), db = 1.0 / (b * b + e2);
+    w[i] = (a * da - b * db) * inv_nk;
+    w[static_cast<long long>(nw) * npair + i] = (-eta * da + eta * db) * inv_nk;
+  }
+}
+
 static DevBuf g_lz_map, g_lz_e, g_lz_w, g_lz_bins, g_lz_fi;
 
+// eta < 0: imaginary axis, nw slots of weights; eta >= 0: real axis, 2 nw slots (Re, Im).
 int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc, const int* nun,
                          const double* eocc, const double* eunocc, long long& npair, double*& w_d,
-                         cudaStream_t s) {
+                         cudaStream_t s, double eta = -1.0) {
   npair = 0;
   long long no_tot = 0, nu_tot = 0;
   for (int k = 0; k < nk; ++k) {
@@ -252,7 +273,7 @@ int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc,
   if (rc) return rc;
   rc = g_lz_e.ensure((no_tot + nu_tot + 1) * sizeof(double));
   if (rc) return rc;
-  rc = g_lz_w.ensure(std::max<long long>(npair, 1) * niw * sizeof(double));
+  rc = g_lz_w.ensure(std::max<long long>(npair, 1) * niw * (eta >= 0.0 ? 2 : 1) * sizeof(double));
   if (rc) return rc;
   rc = g_lz_fi.ensure(niw * sizeof(double));
   if (rc) return rc;
@@ -267,11 +288,16 @@ int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc,
   QSGW_CUDA(cudaMemcpyAsync(g_lz_fi.p, freq_i, niw * sizeof(double), cudaMemcpyHostToDevice, s));
   const long long tot = npair * niw;
   const int blocks = static_cast<int>(std::min<long long>((tot + 255) / 256, 8LL * ctx().sm_count));
-  if (tot > 0) {
+  if (tot > 0 && eta < 0.0) {
     lorentz_weight_kernel<<<std::max(blocks, 1), 256, 0, s>>>(g_lz_w.as<double>(), dpeo, dpeu, deo, deu,
                                                               g_lz_fi.as<double>(), npair, niw, 1.0 / nk);
     count_launch();
     QSGW_LAUNCH_CHECK("lorentz_weight_kernel");
+  } else if (tot > 0) {
+    lorentz_real_weight_kernel<<<std::max(blocks, 1), 256, 0, s>>>(g_lz_w.as<double>(), dpeo, dpeu, deo, deu,
+                                                                   g_lz_fi.as<double>(), npair, niw, eta, 1.0 / nk);
+    count_launch();
+    QSGW_LAUNCH_CHECK("lorentz_real_weight_kernel");
   }
   w_d = g_lz_w.as<double>();
   return QSGW_OK;
@@ -285,7 +311,22 @@ __global__ void iota_kernel(int* a, long long n) {
     a[i] = static_cast<int>(i);
 }
 
+// chi = Hre + i Him for the real axis (Hre, Him: the Re-weight and Im-weight slots)
+__global__ void combine_re_im_kernel(double2* __restrict__ chi, const double2* __restrict__ hre,
+                                     const double2* __restrict__ him, long long n) {
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const double2 a = hre[e], b = him[e];
+    chi[e] = make_double2(a.x - b.y, a.y + b.x);
+  }
+}
+
+static DevBuf g_lzr_h;
+
 }  // namespace qsgw
+
+static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int ldz, long long npair,
+                    const double* w_d, cudaStream_t s);
 
 extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const double* freq_i, int nk,
                                    const int* nocc, const int* nun, const double* eocc,
@@ -302,6 +343,14 @@ extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const doubl
   rc = chi0_lorentz_weights(niw, freq_i, nk, nocc, nun, eocc, eunocc, npair, w_d, s);
   if (rc) return rc;
   QSGW_ARG(npair < (1LL << 31), "chi0_lorentz: %lld pairs exceed the 32-bit column index", npair);
+  return chi0_run(chi0_d, npr, niw, zcols_d, ldz, npair, w_d, s);
+}
+
+// chi0 slots iw = conj(Z) diag(w[iw]) Z^T for precomputed weights w (nslot x npair), in the
+// precision mode of the context; chi0_d is overwritten.
+static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int ldz, long long npair,
+                    const double* w_d, cudaStream_t s) {
+  int rc = QSGW_OK;
   const size_t cbytes = static_cast<size_t>(npr) * npr * niw * 16;
   QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
   if (npair == 0) return QSGW_OK;
@@ -347,6 +396,36 @@ extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const doubl
   const int sk = choose_splitk(ntiles, niw, maxch);
   p.kch_per_split = (maxch + sk - 1) / sk;
   return zgemm_chi0_launch(p, niw, 1, sk, s);
+}
+
+extern "C" int qsgw_chi0_lorentz_real_d(double* chi0_d, int npr, int nw, const double* freq_r, double eta, int nk,
+                                        const int* nocc, const int* nun, const double* eocc,
+                                        const double* eunocc, const double* zcols_d, int ldz) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(chi0_d && zcols_d && freq_r && nocc && nun && eocc && eunocc, "chi0_lorentz_real: null pointer");
+  QSGW_ARG(npr >= 1 && nw >= 1 && nk >= 1 && ldz >= npr && eta >= 0.0,
+           "chi0_lorentz_real: npr=%d nw=%d nk=%d ldz=%d eta=%g", npr, nw, nk, ldz, eta);
+  QSGW_ARG((reinterpret_cast<uintptr_t>(chi0_d) & 15) == 0 && (reinterpret_cast<uintptr_t>(zcols_d) & 15) == 0,
+           "chi0_lorentz_real: complex arrays must be 16-byte aligned");
+  cudaStream_t s = ctx().stream;
+  long long npair = 0;
+  double* w_d = nullptr;
+  rc = chi0_lorentz_weights(nw, freq_r, nk, nocc, nun, eocc, eunocc, npair, w_d, s, eta);
+  if (rc) return rc;
+  QSGW_ARG(npair < (1LL << 31), "chi0_lorentz_real: %lld pairs exceed the 32-bit column index", npair);
+  const long long nn = static_cast<long long>(npr) * npr * nw;
+  rc = g_lzr_h.ensure(static_cast<size_t>(2 * nn) * sizeof(double2));
+  if (rc) return rc;
+  double2* h = g_lzr_h.as<double2>();
+  // both Hermitian parts in one run over 2 nw weight slots
+  rc = chi0_run(reinterpret_cast<double*>(h), npr, 2 * nw, zcols_d, ldz, npair, w_d, s);
+  if (rc) return rc;
+  combine_re_im_kernel<<<static_cast<int>(std::min<long long>((nn + 255) / 256, 16LL * ctx().sm_count)), 256, 0,
+                         s>>>(reinterpret_cast<double2*>(chi0_d), h, h + nn, nn);
+  count_launch();
+  QSGW_LAUNCH_CHECK("combine_re_im_kernel");
+  return QSGW_OK;
 }
 
 static qsgw::DevBuf g_lzh_z, g_lzh_c;

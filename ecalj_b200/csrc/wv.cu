@@ -197,8 +197,12 @@ static int grid_for(long long n) {
   return static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 16LL * ctx().sm_count)));
 }
 
+// general = false: imaginary axis, eps~ Hermitian positive definite (WVIllwI);
+// general = true: real axis, eps~ general, inverted with partial pivoting (WVRllwR,
+// m_llw.f90:49-264, the same per-frequency block :125-170).
 static int wvi_device(double2* zxqi, int ngb, int niw, int nspin, const double* vcousq,
-                      const double2* m2e, int is_x0_m, int is_wc_m, int iq, double2* zw, int ldzw) {
+                      const double2* m2e, int is_x0_m, int is_wc_m, int iq, double2* zw, int ldzw,
+                      bool general = false) {
   cudaStream_t s = ctx().stream;
   const long long nn = static_cast<long long>(ngb) * ngb;
   int rc = g_wv_v.ensure(ngb * sizeof(double));
@@ -233,7 +237,8 @@ static int wvi_device(double2* zxqi, int ngb, int niw, int nspin, const double* 
                                                         ngb, ix, ngb, nn, niw);
     count_launch();
     QSGW_LAUNCH_CHECK("eps_build_kernel");
-    rc = zminv_hpd_batched(g_wv_e.as<double2>(), n, n, en, niw, s);   // :350
+    rc = general ? zminv_general_batched(g_wv_e.as<double2>(), n, n, en, niw, s)    // :139
+                 : zminv_hpd_batched(g_wv_e.as<double2>(), n, n, en, niw, s);       // :350
     if (rc) return rc;
   }
   wc_build_kernel<<<grid_for(static_cast<long long>(ldzw) * ldzw * niw), 256, 0, s>>>(
@@ -290,6 +295,19 @@ extern "C" int qsgw_wvi_llw_d(double* zxqi_d, int ngb, int niw, int nspin, const
   return wvi_device(reinterpret_cast<double2*>(zxqi_d), ngb, niw, nspin, vcousq,
                     reinterpret_cast<const double2*>(m2e_d), is_x0_m_basis, is_wc_m_basis, iq,
                     reinterpret_cast<double2*>(zw_d), nblochpmx);
+}
+
+extern "C" int qsgw_wvr_llw_d(double* zxq_d, int ngb, int nw, int nspin, const double* vcousq,
+                              const double* m2e_d, int is_x0_m_basis, int is_wc_m_basis, int iq,
+                              double* zw_d, int nblochpmx) {
+  int rc = require_init();
+  if (rc) return rc;
+  rc = wvi_check(ngb, nw, nspin, iq, nblochpmx, zxq_d, zw_d, vcousq);
+  if (rc) return rc;
+  QSGW_ARG(!(is_x0_m_basis || is_wc_m_basis) || m2e_d, "wvr_llw: m2e required for basis changes");
+  return wvi_device(reinterpret_cast<double2*>(zxq_d), ngb, nw, nspin, vcousq,
+                    reinterpret_cast<const double2*>(m2e_d), is_x0_m_basis, is_wc_m_basis, iq,
+                    reinterpret_cast<double2*>(zw_d), nblochpmx, true);
 }
 
 extern "C" int qsgw_wvi_llw(double* zxqi, int ngb, int niw, int nspin, const double* vcousq,

@@ -314,5 +314,8 @@ int zgemm_f64(int opa, int opb, int m, int n, int k, double2 alpha,
               double2* C, long long ldc, long long c_bs, int nbatch, cudaStream_t s);
 int zgemm_chi0_launch(ZParams p, int nbins, int herm, int splitk, cudaStream_t s);
 int zgemm_seg_launch(ZParams p, int ncol_tiles, cudaStream_t s);
+// Batched inverses (wv.cu: Hermitian positive definite; zminv_piv.cu: general, partial pivoting).
+int zminv_hpd_batched(double2* A, int n, long long lda, long long a_bs, int nbatch, cudaStream_t s);
+int zminv_general_batched(double2* A, int n, long long lda, long long a_bs, int nbatch, cudaStream_t s);
 
 }  // namespace qsgw

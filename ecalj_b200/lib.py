@@ -98,6 +98,10 @@ _SIGS = {
     "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
     "qsgw_zmel_ipw_d": [c_vp],
     "qsgw_zhegv_d": [c_vp, c_vp, c_int, c_int, c_vp],
+    "qsgw_chi0_lorentz_real_d": [c_vp, c_int, c_int, c_vp, ctypes.c_double, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                 c_int],
+    "qsgw_wvr_llw_d": [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_int],
+    "qsgw_zminv_batched_d": [c_vp, c_int, c_int, c_int],
     "qsgw_wv_write_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int],
     "qsgw_wv_read_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int, c_int, c_int],
     "qsgw_wsurr_init": [ctypes.c_ulonglong],
@@ -421,6 +425,27 @@ def zhegv_d(v, n, lda=None, o=None):
     out = np.zeros(n)
     _chk(load().qsgw_zhegv_d(_p(v), _p(o), n, lda or n, out.ctypes.data))
     return out
+
+
+# ---------------------------------------------------------------- real frequency axis
+def chi0_lorentz_real_d(chi0, npr, nw, freq_r, eta, nk, nocc, nun, eocc, eunocc, zcols, ldz=None):
+    fr, no, nu = _f64(freq_r), _i32(nocc), _i32(nun)
+    eo, eu = _f64(eocc), _f64(eunocc)
+    _chk(load().qsgw_chi0_lorentz_real_d(_p(chi0), npr, nw, _p(fr), float(eta), nk, _p(no), _p(nu), _p(eo), _p(eu),
+                                         _p(zcols), ldz or npr))
+    return chi0
+
+
+def wvr_llw_d(zxq, ngb, nw, nspin, vcousq, m2e, is_x0_m_basis, is_wc_m_basis, iq, zw, nblochpmx=None):
+    """m_llw.f90:49-264: W - v on real frequencies (device arrays)."""
+    v = _f64(vcousq)
+    _chk(load().qsgw_wvr_llw_d(_p(zxq), ngb, nw, nspin, _p(v), _p(m2e), int(is_x0_m_basis), int(is_wc_m_basis), iq,
+                               _p(zw), nblochpmx or ngb))
+    return zw
+
+
+def zminv_batched_d(a, n, lda, nbatch):
+    _chk(load().qsgw_zminv_batched_d(_p(a), n, lda, nbatch))
 
 
 # ---------------------------------------------------------------- W record files

@@ -290,6 +290,27 @@ int qsgw_zmel_m2e_d(double *zmel_d, const double *zmelt_d, int ngb, int nbb,
  * vcoud: host (n).  FP64 parallel cyclic Jacobi.                          */
 int qsgw_zhegv_d(double *v_d, const double *o_d, int n, int lda, double *vcoud);
 
+/* ---- Real frequency axis (WVRllwR, m_llw.f90:49-264).
+ * chi0 of the Lorentzian model on real frequencies:
+ *   chi0(w) = conj(Z) diag(f) Z^T,  f = [1/(w - de + i eta) - 1/(w + de + i eta)] / nk
+ * (its value at w = i nu is the weight of qsgw_chi0_lorentz_d), computed as
+ * two Hermitian parts (Re f, Im f) on the chi0 engine; freq_r host (nw),
+ * Hartree; output (npr, npr, nw) complex, overwritten.                     */
+int qsgw_chi0_lorentz_real_d(double *chi0_d, int npr, int nw, const double *freq_r,
+                             double eta, int nk, const int *nocc, const int *nun,
+                             const double *eocc, const double *eunocc,
+                             const double *zcols_d, int ldz);
+/* W - v on real frequencies: the WVIllwI block with eps~ general, inverted
+ * by Gauss-Jordan with partial pivoting (zminv, m_lapack.f90:108-176);
+ * arguments as qsgw_wvi_llw_d.  A singular eps~ sets the status word
+ * (qsgw_synchronize returns QSGW_ERR_NUMERIC).                              */
+int qsgw_wvr_llw_d(double *zxq_d, int ngb, int nw, int nspin, const double *vcousq,
+                   const double *m2e_d, int is_x0_m_basis, int is_wc_m_basis, int iq,
+                   double *zw_d, int nblochpmx);
+/* in-place inverses of nbatch general complex n x n matrices (lda, batch
+ * stride lda*n), partial pivoting; a zero pivot sets the status word.      */
+int qsgw_zminv_batched_d(double *a, int n, int lda, int nbatch);
+
 /* ---- W record files __WVI.<iq> / __WVR.<iq> in the reference's layout:
  * fixed records without markers, record rec at byte (rec-1)*recl, one
  * nblochpmx x nblochpmx column-major matrix per record, complex(8)

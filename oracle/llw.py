@@ -64,3 +64,10 @@ def coulomb_eig(vmat, omat=None):
     b = np.eye(n, dtype=np.complex128) if omat is None else omat
     lam, z = eigh(-vmat, b, lower=False, driver='gvx')
     return -lam, z
+
+
+def wvr_llw(zxq, nspin, vcousq, m2e, is_x0_m_basis, is_wc_m_basis, iq, nblochpmx=None):
+    """SRC/subroutines/m_llw.f90:49-264 (WVRllwR): the per-frequency block
+    :125-170 is the one of WVIllwI with eps~ general; zminv_h is LAPACK's
+    pivoted zgetrf + zgetri, so the same restatement applies."""
+    return wvi_llw(zxq, nspin, vcousq, m2e, is_x0_m_basis, is_wc_m_basis, iq, nblochpmx)

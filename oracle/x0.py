@@ -100,3 +100,17 @@ def chi0_direct(zmels, tables, npr, niw):
                t['itc'], t['itpc'], t['jpmc'], t['iwini'], t['iwend'],
                t['icouini'], t['whwc'])
     return rcxq
+
+
+def chi0_real(zcols, de, nk, freq_r, eta):
+    """chi0 of the Lorentzian model on real frequencies (the stand-in for the
+    histogram + Hilbert transform of dpsion5.f90:243-292):
+        chi0(w) = conj(Z) diag(f) Z^T,  f = [1/(w - de + i eta) - 1/(w + de + i eta)] / nk,
+    whose value at w = i nu is the imaginary-axis weight -2 de/(de^2 + nu^2)/nk.
+    zcols (npr, npair) complex, de (npair,) Hartree; returns (npr, npr, nw)."""
+    z = np.asarray(zcols)
+    out = np.empty((z.shape[0], z.shape[0], len(freq_r)), np.complex128, order='F')
+    for iw, w in enumerate(freq_r):
+        f = (1.0 / (w - de + 1j * eta) - 1.0 / (w + de + 1j * eta)) / nk
+        out[:, :, iw] = (z.conj() * f) @ z.T
+    return out
