@@ -12,6 +12,8 @@
 //   4. zsec += czmelwc^H zmel (:599) with split-K, then Im zsec_ii <= 0 (:601-607).
 #include <cmath>
 #include <map>
+#include <set>
+#include <algorithm>
 #include <vector>
 #include "zgemm_f64.cuh"
 #include "split_f16.cuh"
@@ -290,47 +292,55 @@ int sxcf_device(const qsgw_sxcf_args& a) {
     }
     wr = g_sc_wr.as<double2>();
   }
-  // ---- groups: key ixs (0 = no pole); per-column wgt3
-  std::vector<double> w3(static_cast<size_t>(ncol) * 3, 0.0);
+  // ---- column tiles: columns sorted by their pole bin ixs (0 = no pole), cut into tiles of
+  // the kernel's column width; a tile's segments are the niw+1 imaginary slots and the union of
+  // its columns' real-axis bins.  scale_bin[r][col] = the column's pole weight on record r (zero
+  // when the column has no pole there), so mixing bins in a tile adds no padding columns.
   std::vector<int> key(ncol, 0);
-  for (const auto& e : poles) {
-    key[e.col] = e.ixs;
-    for (int i = 0; i < 3; ++i) w3[static_cast<size_t>(e.col) * 3 + i] = e.w3[i];
-  }
-  rc = g_sc_w3.ensure(w3.size() * sizeof(double));
+  for (const auto& e : poles) key[e.col] = e.ixs;
+  std::vector<double> scale_bin(static_cast<size_t>(std::max(nrec, 1)) * ncol, 0.0);
+  for (const auto& e : poles)
+    for (int i = 0; i < 3; ++i) {
+      auto it = bin_slot.find(e.ixs - 1 + i);
+      if (it != bin_slot.end()) scale_bin[static_cast<size_t>(it->second) * ncol + e.col] = e.w3[i];
+    }
+  rc = g_sc_w3.ensure(scale_bin.size() * sizeof(double));
   if (rc) return rc;
-  QSGW_CUDA(cudaMemcpyAsync(g_sc_w3.p, w3.data(), w3.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-  std::map<int, std::vector<int>> groups;
-  for (long long c = 0; c < ncol; ++c) groups[key[c]].push_back(static_cast<int>(c));
+  QSGW_CUDA(cudaMemcpyAsync(g_sc_w3.p, scale_bin.data(), scale_bin.size() * sizeof(double), cudaMemcpyHostToDevice,
+                            s));
+  std::vector<int> order(ncol);
+  for (long long c = 0; c < ncol; ++c) order[c] = static_cast<int>(c);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
   const bool split = ctx().prec_mode == QSGW_PREC_SPLIT_F16;
   const int tilew = split ? 128 : ZG_BN;       // column tile of the split / FP64 kernel
   std::vector<ZSeg> segs;
   std::vector<int> gseg_off, gnseg, tile_group, tile_cols, seg_slot;
   int gidx = 0;
-  for (auto& kv : groups) {
+  for (long long t0 = 0; t0 < ncol; t0 += tilew) {
+    const long long t1 = std::min<long long>(ncol, t0 + tilew);
     gseg_off.push_back(static_cast<int>(segs.size()));
     for (int sgi = 0; sgi <= niw; ++sgi) {
       ZSeg z{wi + sgi * wsz, g_sc_wg.as<double>() + sgi, niw + 1, 0};
       segs.push_back(z);
       seg_slot.push_back(sgi);
     }
-    if (kv.first > 0) {
+    std::set<int> rset;                          // records used by the tile's columns
+    for (long long j = t0; j < t1; ++j) {
+      const int k = key[order[j]];
+      if (k <= 0) continue;
       for (int i = 0; i < 3; ++i) {
-        const int b = kv.first - 1 + i;
-        auto it = bin_slot.find(b);
-        if (it == bin_slot.end()) continue;
-        ZSeg z{wr + it->second * wsz, g_sc_w3.as<double>() + i, 3, 0};
-        segs.push_back(z);
-        seg_slot.push_back(niw + 1 + it->second);
+        auto it = bin_slot.find(k - 1 + i);
+        if (it != bin_slot.end()) rset.insert(it->second);
       }
     }
-    gnseg.push_back(static_cast<int>(segs.size()) - gseg_off.back());
-    const auto& cols = kv.second;
-    for (size_t t0 = 0; t0 < cols.size(); t0 += tilew) {
-      tile_group.push_back(gidx);
-      for (int j = 0; j < tilew; ++j)
-        tile_cols.push_back(t0 + j < cols.size() ? cols[t0 + j] : -1);
+    for (int r : rset) {
+      ZSeg z{wr + r * wsz, g_sc_w3.as<double>() + static_cast<long long>(r) * ncol, 1, 0};
+      segs.push_back(z);
+      seg_slot.push_back(niw + 1 + r);
     }
+    gnseg.push_back(static_cast<int>(segs.size()) - gseg_off.back());
+    tile_group.push_back(gidx);
+    for (int j = 0; j < tilew; ++j) tile_cols.push_back(t0 + j < t1 ? order[t0 + j] : -1);
     ++gidx;
   }
   const int ntiles = static_cast<int>(tile_group.size());
@@ -345,7 +355,7 @@ int sxcf_device(const qsgw_sxcf_args& a) {
     sa.wr = wr; sa.nreal = nrec;
     sa.zmel = zmel; sa.ncol = ncol;
     sa.wgt = g_sc_wg.as<double>(); sa.nwgt = ncol * (niw + 1);
-    sa.w3 = g_sc_w3.as<double>(); sa.nw3 = poles.empty() ? 0 : ncol * 3;
+    sa.w3 = g_sc_w3.as<double>(); sa.nw3 = (poles.empty() || nrec == 0) ? 0 : static_cast<long long>(nrec) * ncol;
     sa.tile_cols = std::move(tile_cols); sa.tile_group = std::move(tile_group);
     sa.group_seg_off = std::move(gseg_off); sa.group_nseg = std::move(gnseg);
     sa.seg_slot = std::move(seg_slot); sa.segs = std::move(segs);
