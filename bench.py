@@ -279,6 +279,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the W_c frequency-interpolator study")
+    ap.add_argument("--no-graph", action="store_true", help="time eager calls instead of CUDA-graph replays")
     ap.add_argument("--nq", type=int, default=None, help="Sigma_c tasks (default: the configuration's 64)")
     ap.add_argument("--nk", type=int, default=None, help="k-points of the chi0 part (profiling only)")
     args = ap.parse_args()
@@ -323,29 +324,45 @@ def main():
             t["zsec"].zero_()
         run_sigc(lib, s)
 
-    def timed(mode, steps, warmup, sample_clocks):
+    def timed(mode, steps, warmup, sample_clocks, graph=False):
+        """Warm-up steps, then `steps` timed steps: eager calls, or replays of
+        one step recorded as a CUDA graph (launch count and per-kernel times of
+        a replay are those recorded, scaled by the number of replays)."""
         lib.set_precision(lib.PREC_SPLIT_F16 if mode == "split" else lib.PREC_FP64)
         for _ in range(warmup):
             step()
         torch.cuda.synchronize()
+        lib.profile(True)
+        per_step = None
+        if graph:
+            l0 = lib.launch_count()
+            lib.graph_begin()
+            step()
+            lib.graph_end()
+            per_step = lib.launch_count() - l0
+            lib.graph_launch()                           # one untimed replay
+            torch.cuda.synchronize()
+        run = lib.graph_launch if graph else step
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize()
         sampler = ClockSampler(local) if sample_clocks else None
         if sampler:
             sampler.start()
-        lib.profile(True)
         l0 = lib.launch_count()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         for _ in range(steps):
-            step()
+            run()
         ev1.record()
         torch.cuda.synchronize()
-        launches = lib.launch_count() - l0
+        launches = per_step * steps if graph else lib.launch_count() - l0
         ms = ev0.elapsed_time(ev1) / steps
         kt = {tag: lib.profile_get(tag) for tag in ("chi0_dmma", "sigc_seg_dmma", "gemm_dmma", "chi0_tc",
                                                    "sigc_seg_tc")}
+        if graph:                                        # the latest replay's times, for every replay
+            kt = {k: (v[0] * steps, v[1] * steps) for k, v in kt.items()}
+            lib.graph_destroy()
         lib.profile(False)
         clocks = sampler.stop() if sampler else None
         if ws > 1:
@@ -355,8 +372,11 @@ def main():
             dist.barrier()
         return ms, kt, launches, clocks
 
-    # ---- headline run
-    ms, kt, launches, clocks = timed(prec, args.steps, args.warmup, True)
+    # ---- headline run: one step recorded as a CUDA graph and replayed (eager timing beside it)
+    ms_eager = None
+    if not args.no_graph:
+        ms_eager, _, _, _ = timed(prec, max(1, min(args.steps, 2)), 1, False)
+    ms, kt, launches, clocks = timed(prec, args.steps, args.warmup, True, graph=not args.no_graph)
     value = ws * flops / (ms * 1e-3) / 1e9
     chi_main = chi.clone()
     zsec_main = [t["zsec"].clone() for t in s["tasks"]]
@@ -364,7 +384,7 @@ def main():
     # ---- the other precision, same workload, same run (the metric compares them)
     compare = None
     if prec == "split" and not args.no_compare:
-        ms64, kt64, _, _ = timed("fp64", max(1, min(args.steps, 2)), 1, False)
+        ms64, kt64, _, _ = timed("fp64", max(1, min(args.steps, 2)), 1, False, graph=not args.no_graph)
         d_chi = float(torch.linalg.vector_norm(chi_main - chi) / torch.linalg.vector_norm(chi))
         num = sum(float(torch.linalg.vector_norm(a - t["zsec"]) ** 2) for a, t in zip(zsec_main, s["tasks"]))
         den = sum(float(torch.linalg.vector_norm(t["zsec"]) ** 2) for t in s["tasks"])
@@ -429,6 +449,8 @@ def main():
                                        f"{c1['npair']} pairs) + c2 Sigma_c ({len(s['tasks'])} tasks, N=600, "
                                        "40x400 states, 24+1 iw, 50-point real mesh)",
                            "precision": prec, "parallelism": f"replicas x{ws}",
+                           "execution": "CUDA graph replay" if not args.no_graph else "eager calls",
+                           "eager_ms_per_step": round(ms_eager, 3) if ms_eager else None,
                            "l2": "inputs exceed L2 (zmel columns 3.73 GB)",
                            "flops_per_step": flops, "flops_chi0": fl_chi, "flops_sigc": fl_sig},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,

@@ -281,11 +281,11 @@ int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc,
   int* dpeu = dpeo + npair;
   double* deo = g_lz_e.as<double>();
   double* deu = deo + no_tot;
-  QSGW_CUDA(cudaMemcpyAsync(dpeo, peo.data(), npair * sizeof(int), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(dpeu, peu.data(), npair * sizeof(int), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(deo, eocc, no_tot * sizeof(double), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(deu, eunocc, nu_tot * sizeof(double), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(g_lz_fi.p, freq_i, niw * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((rc = h2d(dpeo, peo.data(), npair * sizeof(int), s))) return rc;
+  if ((rc = h2d(dpeu, peu.data(), npair * sizeof(int), s))) return rc;
+  if ((rc = h2d(deo, eocc, no_tot * sizeof(double), s))) return rc;
+  if ((rc = h2d(deu, eunocc, nu_tot * sizeof(double), s))) return rc;
+  if ((rc = h2d(g_lz_fi.p, freq_i, niw * sizeof(double), s))) return rc;
   const long long tot = npair * niw;
   const int blocks = static_cast<int>(std::min<long long>((tot + 255) / 256, 8LL * ctx().sm_count));
   if (tot > 0 && eta < 0.0) {
@@ -376,9 +376,8 @@ static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int
   rc = g_lz_bins.ensure(2 * niw * (sizeof(long long) + sizeof(int)));
   if (rc) return rc;
   unsigned char* base = g_lz_bins.as<unsigned char>();
-  QSGW_CUDA(cudaMemcpyAsync(base, off.data(), 2 * niw * sizeof(long long), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(base + 2 * niw * sizeof(long long), cs.data(), 2 * niw * sizeof(int),
-                            cudaMemcpyHostToDevice, s));
+  if ((rc = h2d(base, off.data(), 2 * niw * sizeof(long long), s))) return rc;
+  if ((rc = h2d(base + 2 * niw * sizeof(long long), cs.data(), 2 * niw * sizeof(int), s))) return rc;
   ZParams p{};
   p.M = npr; p.N = npr;
   p.A = reinterpret_cast<const double2*>(zcols_d); p.a_rs = 1; p.a_ks = ldz; p.a_conj = 1;

@@ -21,6 +21,11 @@ struct Context {
   int nslices = 2;
   int sm_count = 148;
   int* d_flags = nullptr;             // device-side error/status words
+  // CUDA graph of one recorded call sequence (qsgw_graph_*)
+  bool capturing = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<void*> graph_host;      // pinned copies of host tables the graph reads
 };
 
 Context& ctx();
@@ -37,6 +42,11 @@ struct DevBuf {
 };
 
 int require_init();
+// Host -> device copy of a small host table on stream s.  Outside capture it
+// copies from the caller's memory; while a graph is being recorded the data
+// is first copied into pinned memory owned by the graph, which the recorded
+// copy node reads at every replay.
+int h2d(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // kernels launched by this library since init (qsgw_launch_count)
 void count_launch(int n = 1);
 

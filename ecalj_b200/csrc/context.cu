@@ -30,6 +30,12 @@ int check_cuda(cudaError_t e, const char* what) {
 
 int DevBuf::ensure(size_t n) {
   if (n <= bytes && p) return QSGW_OK;
+  if (g_ctx.capturing) {
+    // nodes recorded earlier may point into the old buffer
+    set_error("scratch of %zu bytes needed while recording a graph: run the same calls once before "
+              "qsgw_graph_begin", n);
+    return QSGW_ERR_UNSUPPORTED;
+  }
   if (p) cudaFree(p);
   p = nullptr;
   bytes = 0;
@@ -41,6 +47,17 @@ int DevBuf::ensure(size_t n) {
   }
   bytes = want;
   return QSGW_OK;
+}
+
+int h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return QSGW_OK;
+  if (!g_ctx.capturing) return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "H2D table");
+  void* pin = nullptr;
+  int rc = check_cuda(cudaHostAlloc(&pin, bytes, cudaHostAllocDefault), "cudaHostAlloc(graph table)");
+  if (rc) return rc;
+  std::memcpy(pin, src, bytes);
+  g_ctx.graph_host.push_back(pin);
+  return check_cuda(cudaMemcpyAsync(dst, pin, bytes, cudaMemcpyHostToDevice, s), "H2D table (graph)");
 }
 
 void DevBuf::release() {
@@ -76,17 +93,25 @@ static void prof_reset() {
   g_prof_recs.clear();
 }
 
+// While a graph is recorded the events become external event-record nodes:
+// each replay records them again, so the times read afterwards are those of
+// the latest replay.
+static void prof_record(cudaEvent_t e, cudaStream_t s) {
+  if (g_ctx.capturing) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+  else cudaEventRecord(e, s);
+}
+
 int prof_begin(const char* tag, cudaStream_t s) {
   if (!g_prof) return -1;
   ProfRec r{tag, pool_event(), pool_event()};
-  cudaEventRecord(r.a, s);
+  prof_record(r.a, s);
   g_prof_recs.push_back(r);
   return static_cast<int>(g_prof_recs.size()) - 1;
 }
 
 void prof_end(int idx, cudaStream_t s) {
   if (idx < 0 || idx >= static_cast<int>(g_prof_recs.size())) return;
-  cudaEventRecord(g_prof_recs[idx].b, s);
+  prof_record(g_prof_recs[idx].b, s);
 }
 
 int require_init() {
@@ -131,11 +156,20 @@ extern "C" int qsgw_init(int device) {
   return QSGW_OK;
 }
 
+static void graph_free();
+
 extern "C" int qsgw_finalize(void) {
   Context& c = ctx();
   if (!c.initialized) return QSGW_OK;
   cudaSetDevice(c.device);
+  if (c.capturing) {                       // abandon an unfinished recording
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(c.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    c.capturing = false;
+  }
   cudaDeviceSynchronize();
+  graph_free();
   if (c.d_flags) cudaFree(c.d_flags);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
   c = Context();
@@ -145,6 +179,7 @@ extern "C" int qsgw_finalize(void) {
 extern "C" int qsgw_set_stream(void* stream) {
   int rc = require_init();
   if (rc) return rc;
+  QSGW_ARG(!ctx().capturing, "set_stream: a graph is being recorded");
   Context& c = ctx();
   if (stream == nullptr) {
     if (!c.own_stream) {
@@ -206,6 +241,7 @@ extern "C" long long qsgw_launch_count(void) { return g_launches.load(); }
 extern "C" int qsgw_profile(int enable) {
   int rc = require_init();
   if (rc) return rc;
+  QSGW_ARG(!ctx().capturing, "qsgw_profile: a graph is being recorded");
   QSGW_CUDA(cudaStreamSynchronize(ctx().stream));
   prof_reset();
   g_prof = enable != 0;
@@ -228,5 +264,68 @@ extern "C" int qsgw_profile_get(const char* tag, double* ms, long long* launches
   }
   *ms = tot;
   *launches = n;
+  return QSGW_OK;
+}
+
+
+// ---- CUDA graph of a recorded call sequence
+static void graph_free() {
+  Context& c = ctx();
+  if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
+  if (c.graph) cudaGraphDestroy(c.graph);
+  c.graph_exec = nullptr;
+  c.graph = nullptr;
+  for (void* p : c.graph_host) cudaFreeHost(p);
+  c.graph_host.clear();
+}
+
+extern "C" int qsgw_graph_begin(void) {
+  int rc = require_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  QSGW_ARG(!c.capturing, "graph_begin: already recording");
+  QSGW_ARG(c.stream != nullptr, "graph_begin: the launch stream cannot be the legacy default stream");
+  QSGW_CUDA(cudaStreamSynchronize(c.stream));
+  graph_free();
+  // relaxed: pinned host tables are allocated while recording
+  QSGW_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+  c.capturing = true;
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_graph_end(void) {
+  int rc = require_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  QSGW_ARG(c.capturing, "graph_end: not recording");
+  c.capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c.stream, &g);
+  if (e != cudaSuccess || g == nullptr) {
+    if (g) cudaGraphDestroy(g);
+    graph_free();
+    return check_cuda(e != cudaSuccess ? e : cudaErrorStreamCaptureInvalidated, "graph_end: cudaStreamEndCapture");
+  }
+  c.graph = g;
+  rc = check_cuda(cudaGraphInstantiate(&c.graph_exec, g, 0), "graph_end: cudaGraphInstantiate");
+  if (rc) graph_free();
+  return rc;
+}
+
+extern "C" int qsgw_graph_launch(void) {
+  int rc = require_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  QSGW_ARG(c.graph_exec && !c.capturing, "graph_launch: no recorded graph");
+  QSGW_CUDA(cudaGraphLaunch(c.graph_exec, c.stream));
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_graph_destroy(void) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(!ctx().capturing, "graph_destroy: still recording");
+  QSGW_CUDA(cudaStreamSynchronize(ctx().stream));
+  graph_free();
   return QSGW_OK;
 }

@@ -231,11 +231,11 @@ int sxcf_device(const qsgw_sxcf_args& a) {
   if (rc) return rc;
   double* dt = g_sc_tabs.as<double>();
   double *d_x = dt, *d_wt = dt + niw, *d_ex = dt + 2 * niw, *d_om = dt + 3 * niw, *d_ekc = d_om + a.ntq;
-  QSGW_CUDA(cudaMemcpyAsync(d_x, a.freqx, niw * sizeof(double), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(d_wt, a.wwx, niw * sizeof(double), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(d_ex, a.expa, niw * sizeof(double), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(d_om, a.omega, a.ntq * sizeof(double), cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(d_ekc, a.ekc, a.nekc * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((rc = h2d(d_x, a.freqx, niw * sizeof(double), s))) return rc;
+  if ((rc = h2d(d_wt, a.wwx, niw * sizeof(double), s))) return rc;
+  if ((rc = h2d(d_ex, a.expa, niw * sizeof(double), s))) return rc;
+  if ((rc = h2d(d_om, a.omega, a.ntq * sizeof(double), s))) return rc;
+  if ((rc = h2d(d_ekc, a.ekc, a.nekc * sizeof(double), s))) return rc;
   rc = g_sc_wg.ensure(ncol * (niw + 1) * sizeof(double));
   if (rc) return rc;
   wgtim_kernel<<<static_cast<int>((ncol + 127) / 128), 128, 0, s>>>(
@@ -284,7 +284,7 @@ int sxcf_device(const qsgw_sxcf_args& a) {
         QSGW_LAUNCH_CHECK("unpack_upper_kernel");
       }
     } else {
-      QSGW_CUDA(cudaMemcpyAsync(g_sc_recs.p, recs.data(), nrec * sizeof(int), cudaMemcpyHostToDevice, s));
+      if ((rc = h2d(g_sc_recs.p, recs.data(), nrec * sizeof(int), s))) return rc;
       hermitize_kernel<<<grid_for(static_cast<long long>(ngb) * ngb * nrec), 256, 0, s>>>(
           g_sc_wr.as<double2>(), wr_src, g_sc_recs.as<int>(), ngb, ldw, nrec);
       count_launch();
@@ -306,8 +306,7 @@ int sxcf_device(const qsgw_sxcf_args& a) {
     }
   rc = g_sc_w3.ensure(scale_bin.size() * sizeof(double));
   if (rc) return rc;
-  QSGW_CUDA(cudaMemcpyAsync(g_sc_w3.p, scale_bin.data(), scale_bin.size() * sizeof(double), cudaMemcpyHostToDevice,
-                            s));
+  if ((rc = h2d(g_sc_w3.p, scale_bin.data(), scale_bin.size() * sizeof(double), s))) return rc;
   std::vector<int> order(ncol);
   for (long long c = 0; c < ncol; ++c) order[c] = static_cast<int>(c);
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
@@ -372,7 +371,7 @@ int sxcf_device(const qsgw_sxcf_args& a) {
     int cprc = 0;
     auto put = [&](const void* src, size_t n) -> const void* {
       void* dst = tbase + off;
-      if (!cprc) cprc = check_cuda(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s), "H2D sxcf tables");
+      if (!cprc) cprc = h2d(dst, src, n, s);
       off += (n + 15) & ~size_t(15);
       return dst;
     };

@@ -821,7 +821,7 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   int cprc = 0;
   auto put = [&](const void* src, size_t n) -> const void* {
     void* dst = tb + off;
-    if (!cprc && n) cprc = check_cuda(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s), "H2D split tables");
+    if (!cprc && n) cprc = h2d(dst, src, n, s);
     off += (n + 15) & ~size_t(15);
     return dst;
   };

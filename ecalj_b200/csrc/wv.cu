@@ -207,7 +207,7 @@ static int wvi_device(double2* zxqi, int ngb, int niw, int nspin, const double* 
   const long long nn = static_cast<long long>(ngb) * ngb;
   int rc = g_wv_v.ensure(ngb * sizeof(double));
   if (rc) return rc;
-  QSGW_CUDA(cudaMemcpyAsync(g_wv_v.p, vcousq, ngb * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((rc = h2d(g_wv_v.p, vcousq, ngb * sizeof(double), s))) return rc;
   if (nspin == 1) {   // zxqi = 2 zxqi in place (m_llw.f90:299-303)
     zscale_real_kernel<<<grid_for(nn * niw), 256, 0, s>>>(zxqi, nn * niw, 2.0);
     count_launch();

@@ -98,6 +98,10 @@ _SIGS = {
     "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
     "qsgw_zmel_ipw_d": [c_vp],
     "qsgw_zhegv_d": [c_vp, c_vp, c_int, c_int, c_vp],
+    "qsgw_graph_begin": [],
+    "qsgw_graph_end": [],
+    "qsgw_graph_launch": [],
+    "qsgw_graph_destroy": [],
     "qsgw_chi0_lorentz_real_d": [c_vp, c_int, c_int, c_vp, ctypes.c_double, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
                                  c_int],
     "qsgw_wvr_llw_d": [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_int],
@@ -425,6 +429,23 @@ def zhegv_d(v, n, lda=None, o=None):
     out = np.zeros(n)
     _chk(load().qsgw_zhegv_d(_p(v), _p(o), n, lda or n, out.ctypes.data))
     return out
+
+
+# ---------------------------------------------------------------- CUDA graph of a call sequence
+def graph_begin():
+    _chk(load().qsgw_graph_begin())
+
+
+def graph_end():
+    _chk(load().qsgw_graph_end())
+
+
+def graph_launch():
+    _chk(load().qsgw_graph_launch())
+
+
+def graph_destroy():
+    _chk(load().qsgw_graph_destroy())
 
 
 # ---------------------------------------------------------------- real frequency axis

@@ -290,6 +290,23 @@ int qsgw_zmel_m2e_d(double *zmel_d, const double *zmelt_d, int ngb, int nbb,
  * vcoud: host (n).  FP64 parallel cyclic Jacobi.                          */
 int qsgw_zhegv_d(double *v_d, const double *o_d, int n, int lda, double *vcoud);
 
+/* ---- CUDA graph of a recorded call sequence (no reference counterpart: the
+ * reference launches every kernel from the host each time).  Between
+ * qsgw_graph_begin and qsgw_graph_end the device entry points
+ * (qsgw_chi0_lorentz_d, qsgw_wvi_llw_d, qsgw_sxcf_correlation_d, ... and any
+ * other work the caller puts on the library stream) are recorded instead of
+ * run; qsgw_graph_launch replays them.  Host tables passed during recording
+ * (frequencies, energies, band counts, pole tables) are copied into pinned
+ * memory owned by the graph and replayed as recorded; device arrays are read
+ * at replay time.  Record only after the same calls ran once (scratch must
+ * not grow while recording: such a call fails with QSGW_ERR_UNSUPPORTED).
+ * One graph per context; begin replaces the previous one.  The library
+ * stream must not be the legacy default stream.                          */
+int qsgw_graph_begin(void);
+int qsgw_graph_end(void);
+int qsgw_graph_launch(void);
+int qsgw_graph_destroy(void);
+
 /* ---- Real frequency axis (WVRllwR, m_llw.f90:49-264).
  * chi0 of the Lorentzian model on real frequencies:
  *   chi0(w) = conj(Z) diag(f) Z^T,  f = [1/(w - de + i eta) - 1/(w + de + i eta)] / nk
