@@ -280,6 +280,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the W_c frequency-interpolator study")
     ap.add_argument("--no-graph", action="store_true", help="time eager calls instead of CUDA-graph replays")
+    ap.add_argument("--no-autotune", action="store_true", help="heuristic launch parameters only")
     ap.add_argument("--nq", type=int, default=None, help="Sigma_c tasks (default: the configuration's 64)")
     ap.add_argument("--nk", type=int, default=None, help="k-points of the chi0 part (profiling only)")
     args = ap.parse_args()
@@ -298,6 +299,8 @@ def main():
     lib.load()
     lib.init(local)
     lib.share_torch_stream()
+    if not args.no_autotune:
+        lib.set_autotune(1, None)          # the first (untimed) call of each shape picks its split-K
     prec = args.precision
     peaks, peak_src = load_peaks()
 
@@ -455,7 +458,8 @@ def main():
                            "flops_per_step": flops, "flops_chi0": fl_chi, "flops_sigc": fl_sig},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "kernel_ms": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]},
-                "fp64_peak_tflops": round(fp64_peak, 3), "compare": compare, "surrogate": sur}
+                "fp64_peak_tflops": round(fp64_peak, 3), "compare": compare, "surrogate": sur,
+                "autotune": lib.autotune_report()}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()

@@ -8,6 +8,7 @@
 // and the weight are folded into the operand loads of the DMMA engine.
 #include <vector>
 #include "zgemm_f64.cuh"
+#include "autotune.cuh"
 #include "split_f16.cuh"
 
 namespace qsgw {
@@ -392,9 +393,23 @@ static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int
   p.wts = w_d;
   const int maxch = static_cast<int>((npair + ZG_BK - 1) / ZG_BK);
   const int ntiles = p.ntm * (p.ntm + 1) / 2;
-  const int sk = choose_splitk(ntiles, niw, maxch);
-  p.kch_per_split = (maxch + sk - 1) / sk;
-  return zgemm_chi0_launch(p, niw, 1, sk, s);
+  const int heur = choose_splitk(ntiles, niw, maxch);
+  // split K: the autotuner times the heuristic and its neighbours (x1/2, x2, x4) on this shape
+  auto run = [&](int sk) -> int {
+    ZParams q = p;
+    q.kch_per_split = (maxch + sk - 1) / sk;
+    QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
+    return zgemm_chi0_launch(q, niw, 1, sk, s);
+  };
+  std::vector<int> cands;
+  for (int c : {heur / 2, heur, heur * 2, heur * 4})
+    if (c >= 1 && c <= maxch && (cands.empty() || cands.back() != c)) cands.push_back(c);
+  char key[160];
+  std::snprintf(key, sizeof(key), "chi0_dmma npr=%d npair=%lld niw=%d", npr, npair, niw);
+  int sk = heur;
+  rc = tuned_choice(key, cands, heur, run, s, &sk);
+  if (rc) return rc;
+  return run(sk);
 }
 
 extern "C" int qsgw_chi0_lorentz_real_d(double* chi0_d, int npr, int nw, const double* freq_r, double eta, int nk,

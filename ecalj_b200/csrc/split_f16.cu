@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 #include <vector>
 #include "split_f16.cuh"
+#include "autotune.cuh"
 
 namespace qsgw {
 namespace tc {
@@ -755,12 +756,26 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
       if (mt * BMC + BMC - 1 >= nt * NC) ++units;
   units *= niw;
   const long long slots = 2LL * ctx().sm_count;
-  int splitk = static_cast<int>(std::max<long long>(1, (slots + units - 1) / units));
-  splitk = std::min(splitk, std::max(1, p.kch_total / 8));
-  p.kch_per_split = (p.kch_total + splitk - 1) / splitk;
-  splitk = (p.kch_total + p.kch_per_split - 1) / p.kch_per_split;
-  dim3 grid(static_cast<unsigned>(T * Tn), niw, splitk);
-  return launch_split(ma, ms, p, grid, s, "chi0_tc");
+  const int maxsplit = std::max(1, p.kch_total / 8);
+  int heur = static_cast<int>(std::max<long long>(1, (slots + units - 1) / units));
+  heur = std::min(heur, maxsplit);
+  // split K: the autotuner times 1..4 (and the heuristic) on this shape; each trial clears chi0
+  auto run = [&](int splitk) -> int {
+    Params q = p;
+    q.kch_per_split = (q.kch_total + splitk - 1) / splitk;
+    const int sk = (q.kch_total + q.kch_per_split - 1) / q.kch_per_split;
+    QSGW_CUDA(cudaMemsetAsync(chi0, 0, static_cast<size_t>(npr) * npr * niw * sizeof(double2), s));
+    return launch_split(ma, ms, q, dim3(static_cast<unsigned>(T * Tn), niw, sk), s, "chi0_tc");
+  };
+  std::vector<int> cands;
+  for (int c = 1; c <= std::min(4, maxsplit); ++c) cands.push_back(c);
+  if (heur > 4) cands.push_back(heur);
+  char key[160];
+  std::snprintf(key, sizeof(key), "chi0_split_f16 npr=%d npair=%lld niw=%d", npr, npair, niw);
+  int splitk = heur;
+  rc = tuned_choice(key, cands, heur, run, s, &splitk);
+  if (rc) return rc;
+  return run(splitk);
 }
 
 int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {

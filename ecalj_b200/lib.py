@@ -98,6 +98,8 @@ _SIGS = {
     "qsgw_zmel_m2e_d": [c_vp, c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_int],
     "qsgw_zmel_ipw_d": [c_vp],
     "qsgw_zhegv_d": [c_vp, c_vp, c_int, c_int, c_vp],
+    "qsgw_set_autotune": [c_int, ctypes.c_char_p],
+    "qsgw_autotune_report": [ctypes.c_char_p, c_int],
     "qsgw_graph_begin": [],
     "qsgw_graph_end": [],
     "qsgw_graph_launch": [],
@@ -429,6 +431,19 @@ def zhegv_d(v, n, lda=None, o=None):
     out = np.zeros(n)
     _chk(load().qsgw_zhegv_d(_p(v), _p(o), n, lda or n, out.ctypes.data))
     return out
+
+
+# ---------------------------------------------------------------- autotuner
+def set_autotune(mode=1, cache_path=None):
+    _chk(load().qsgw_set_autotune(mode, None if cache_path is None else os.fsencode(cache_path)))
+
+
+def autotune_report():
+    """The tuned choices, {shape key: value}."""
+    import json
+    buf = ctypes.create_string_buffer(1 << 16)
+    _chk(load().qsgw_autotune_report(buf, len(buf)))
+    return json.loads(buf.value.decode())
 
 
 # ---------------------------------------------------------------- CUDA graph of a call sequence

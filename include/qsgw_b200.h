@@ -290,6 +290,17 @@ int qsgw_zmel_m2e_d(double *zmel_d, const double *zmelt_d, int ngb, int nbb,
  * vcoud: host (n).  FP64 parallel cyclic Jacobi.                          */
 int qsgw_zhegv_d(double *v_d, const double *o_d, int n, int lda, double *vcoud);
 
+/* ---- Autotuner.  mode 0: launch parameters from heuristics (default);
+ * mode 1: the first call with a new problem shape times the candidates of a
+ * tunable parameter (today the split-K count of the chi0 contractions, FP64
+ * and split precision) on the caller's data and keeps the fastest; later
+ * calls with that shape reuse it.  cache_path (may be NULL) names a JSON file
+ * {"shape key": choice} read now and rewritten when a choice is added.
+ * No tuning while a graph is being recorded (cached choices still apply).
+ * report: the current choices as JSON text (QSGW_ERR_ARG if len is short).  */
+int qsgw_set_autotune(int mode, const char *cache_path);
+int qsgw_autotune_report(char *buf, int len);
+
 /* ---- CUDA graph of a recorded call sequence (no reference counterpart: the
  * reference launches every kernel from the host each time).  Between
  * qsgw_graph_begin and qsgw_graph_end the device entry points
