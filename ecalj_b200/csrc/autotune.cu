@@ -13,6 +13,10 @@
 namespace qsgw {
 
 static int g_mode = 0;                     // 0 = heuristics, 1 = tune unseen shapes
+static int g_suspend = 0;
+
+TuneSuspend::TuneSuspend() { ++g_suspend; }
+TuneSuspend::~TuneSuspend() { --g_suspend; }
 static std::string g_path;
 static std::map<std::string, int> g_cache;
 
@@ -53,19 +57,21 @@ static void save_cache() {
 }
 
 int tuned_choice(const std::string& key, const std::vector<int>& cands, int heuristic,
-                 const std::function<int(int)>& run, cudaStream_t s, int* chosen) {
+                 const std::function<int(int)>& run, cudaStream_t s, int* chosen, bool* tried) {
   *chosen = heuristic;
+  *tried = false;
   auto it = g_cache.find(key);
   if (it != g_cache.end()) {
     *chosen = it->second;
     return QSGW_OK;
   }
-  if (g_mode == 0 || ctx().capturing || cands.size() < 2) return QSGW_OK;
+  if (g_mode == 0 || g_suspend > 0 || ctx().capturing || cands.size() < 2) return QSGW_OK;
   cudaEvent_t e0, e1;
   QSGW_CUDA(cudaEventCreate(&e0));
   QSGW_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int rc = QSGW_OK;
+  *tried = true;
   for (int c : cands) {
     cudaEventRecord(e0, s);
     rc = run(c);

@@ -6,6 +6,7 @@
 // The host builds the (jpm, iw) bin lists in the reference's icoun order
 // (x0gemm.f90:37-64); the GPU never materialises zw / wzw: the pair gather
 // and the weight are folded into the operand loads of the DMMA engine.
+#include <memory>
 #include <vector>
 #include "zgemm_f64.cuh"
 #include "autotune.cuh"
@@ -248,7 +249,8 @@ static DevBuf g_lz_map, g_lz_e, g_lz_w, g_lz_bins, g_lz_fi;
 // eta < 0: imaginary axis, nw slots of weights; eta >= 0: real axis, 2 nw slots (Re, Im).
 int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc, const int* nun,
                          const double* eocc, const double* eunocc, long long& npair, double*& w_d,
-                         cudaStream_t s, double eta = -1.0) {
+                         cudaStream_t s, double eta = -1.0, int nk_norm = 0) {
+  const double inv_nk = 1.0 / (nk_norm > 0 ? nk_norm : nk);   // 1/nk of the whole k mesh
   npair = 0;
   long long no_tot = 0, nu_tot = 0;
   for (int k = 0; k < nk; ++k) {
@@ -291,12 +293,12 @@ int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc,
   const int blocks = static_cast<int>(std::min<long long>((tot + 255) / 256, 8LL * ctx().sm_count));
   if (tot > 0 && eta < 0.0) {
     lorentz_weight_kernel<<<std::max(blocks, 1), 256, 0, s>>>(g_lz_w.as<double>(), dpeo, dpeu, deo, deu,
-                                                              g_lz_fi.as<double>(), npair, niw, 1.0 / nk);
+                                                              g_lz_fi.as<double>(), npair, niw, inv_nk);
     count_launch();
     QSGW_LAUNCH_CHECK("lorentz_weight_kernel");
   } else if (tot > 0) {
     lorentz_real_weight_kernel<<<std::max(blocks, 1), 256, 0, s>>>(g_lz_w.as<double>(), dpeo, dpeu, deo, deu,
-                                                                   g_lz_fi.as<double>(), npair, niw, eta, 1.0 / nk);
+                                                                   g_lz_fi.as<double>(), npair, niw, eta, inv_nk);
     count_launch();
     QSGW_LAUNCH_CHECK("lorentz_real_weight_kernel");
   }
@@ -327,7 +329,7 @@ static DevBuf g_lzr_h;
 }  // namespace qsgw
 
 static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int ldz, long long npair,
-                    const double* w_d, cudaStream_t s);
+                    const double* w_d, cudaStream_t s, bool accumulate = false);
 
 extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const double* freq_i, int nk,
                                    const int* nocc, const int* nun, const double* eocc,
@@ -350,11 +352,12 @@ extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const doubl
 // chi0 slots iw = conj(Z) diag(w[iw]) Z^T for precomputed weights w (nslot x npair), in the
 // precision mode of the context; chi0_d is overwritten.
 static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int ldz, long long npair,
-                    const double* w_d, cudaStream_t s) {
+                    const double* w_d, cudaStream_t s, bool accumulate) {
   int rc = QSGW_OK;
   const size_t cbytes = static_cast<size_t>(npr) * npr * niw * 16;
-  QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
+  if (!accumulate) QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
   if (npair == 0) return QSGW_OK;
+  std::unique_ptr<TuneSuspend> hold(accumulate ? new TuneSuspend() : nullptr);   // trials would clear chi0
   if (ctx().prec_mode == QSGW_PREC_SPLIT_F16) {
     return chi0_split_f16(reinterpret_cast<double2*>(chi0_d), npr, niw,
                           reinterpret_cast<const double2*>(zcols_d), ldz, npair, w_d, s);
@@ -395,10 +398,10 @@ static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int
   const int ntiles = p.ntm * (p.ntm + 1) / 2;
   const int heur = choose_splitk(ntiles, niw, maxch);
   // split K: the autotuner times the heuristic and its neighbours (x1/2, x2, x4) on this shape
-  auto run = [&](int sk) -> int {
+  auto run = [&](int sk, bool clear) -> int {      // trials clear chi0 (it was cleared above)
     ZParams q = p;
     q.kch_per_split = (maxch + sk - 1) / sk;
-    QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
+    if (clear) QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
     return zgemm_chi0_launch(q, niw, 1, sk, s);
   };
   std::vector<int> cands;
@@ -407,9 +410,29 @@ static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int
   char key[160];
   std::snprintf(key, sizeof(key), "chi0_dmma npr=%d npair=%lld niw=%d", npr, npair, niw);
   int sk = heur;
-  rc = tuned_choice(key, cands, heur, run, s, &sk);
+  bool tried = false;
+  rc = tuned_choice(key, cands, heur, [&](int c) { return run(c, true); }, s, &sk, &tried);
   if (rc) return rc;
-  return run(sk);
+  return run(sk, tried);
+}
+
+extern "C" int qsgw_chi0_lorentz_acc_d(double* chi0_d, int npr, int niw, const double* freq_i, int nk_total,
+                                       int nkb, const int* nocc, const int* nun, const double* eocc,
+                                       const double* eunocc, const double* zcols_d, int ldz) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(chi0_d && zcols_d && freq_i && nocc && nun && eocc && eunocc, "chi0_lorentz_acc: null pointer");
+  QSGW_ARG(npr >= 1 && niw >= 1 && nkb >= 1 && nk_total >= nkb && ldz >= npr,
+           "chi0_lorentz_acc: npr=%d niw=%d nkb=%d nk_total=%d ldz=%d", npr, niw, nkb, nk_total, ldz);
+  QSGW_ARG((reinterpret_cast<uintptr_t>(chi0_d) & 15) == 0 && (reinterpret_cast<uintptr_t>(zcols_d) & 15) == 0,
+           "chi0_lorentz_acc: complex arrays must be 16-byte aligned");
+  cudaStream_t s = ctx().stream;
+  long long npair = 0;
+  double* w_d = nullptr;
+  rc = chi0_lorentz_weights(niw, freq_i, nkb, nocc, nun, eocc, eunocc, npair, w_d, s, -1.0, nk_total);
+  if (rc) return rc;
+  QSGW_ARG(npair < (1LL << 31), "chi0_lorentz_acc: %lld pairs exceed the 32-bit column index", npair);
+  return chi0_run(chi0_d, npr, niw, zcols_d, ldz, npair, w_d, s, true);
 }
 
 extern "C" int qsgw_chi0_lorentz_real_d(double* chi0_d, int npr, int nw, const double* freq_r, double eta, int nk,

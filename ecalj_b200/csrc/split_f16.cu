@@ -760,11 +760,11 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   int heur = static_cast<int>(std::max<long long>(1, (slots + units - 1) / units));
   heur = std::min(heur, maxsplit);
   // split K: the autotuner times 1..4 (and the heuristic) on this shape; each trial clears chi0
-  auto run = [&](int splitk) -> int {
+  auto run = [&](int splitk, bool clear) -> int {   // trials clear chi0; the caller cleared it or accumulates
     Params q = p;
     q.kch_per_split = (q.kch_total + splitk - 1) / splitk;
     const int sk = (q.kch_total + q.kch_per_split - 1) / q.kch_per_split;
-    QSGW_CUDA(cudaMemsetAsync(chi0, 0, static_cast<size_t>(npr) * npr * niw * sizeof(double2), s));
+    if (clear) QSGW_CUDA(cudaMemsetAsync(chi0, 0, static_cast<size_t>(npr) * npr * niw * sizeof(double2), s));
     return launch_split(ma, ms, q, dim3(static_cast<unsigned>(T * Tn), niw, sk), s, "chi0_tc");
   };
   std::vector<int> cands;
@@ -773,9 +773,10 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   char key[160];
   std::snprintf(key, sizeof(key), "chi0_split_f16 npr=%d npair=%lld niw=%d", npr, npair, niw);
   int splitk = heur;
-  rc = tuned_choice(key, cands, heur, run, s, &splitk);
+  bool tried = false;
+  rc = tuned_choice(key, cands, heur, [&](int c) { return run(c, true); }, s, &splitk, &tried);
   if (rc) return rc;
-  return run(splitk);
+  return run(splitk, tried);
 }
 
 int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {

@@ -104,6 +104,7 @@ _SIGS = {
     "qsgw_graph_end": [],
     "qsgw_graph_launch": [],
     "qsgw_graph_destroy": [],
+    "qsgw_chi0_lorentz_acc_d": [c_vp, c_int, c_int, c_vp, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_int],
     "qsgw_chi0_lorentz_real_d": [c_vp, c_int, c_int, c_vp, ctypes.c_double, c_int, c_vp, c_vp, c_vp, c_vp, c_vp,
                                  c_int],
     "qsgw_wvr_llw_d": [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_int],
@@ -192,12 +193,24 @@ def _f64(a):
 
 
 # ---------------------------------------------------------------- context
+_initialized = False
+
+
 def init(device=0):
+    global _initialized
     _chk(load().qsgw_init(device))
+    _initialized = True
 
 
 def finalize():
+    global _initialized
     _chk(load().qsgw_finalize())
+    _initialized = False
+
+
+def initialized():
+    """True between init() and finalize() in this process."""
+    return _initialized
 
 
 def set_stream(stream_handle):
@@ -461,6 +474,15 @@ def graph_launch():
 
 def graph_destroy():
     _chk(load().qsgw_graph_destroy())
+
+
+def chi0_lorentz_acc_d(chi0, npr, niw, freq_i, nk_total, nocc, nun, eocc, eunocc, zcols, ldz=None):
+    """chi0 += the contribution of one batch of k-points (len(nocc) of them)."""
+    fi, no, nu = _f64(freq_i), _i32(nocc), _i32(nun)
+    eo, eu = _f64(eocc), _f64(eunocc)
+    _chk(load().qsgw_chi0_lorentz_acc_d(_p(chi0), npr, niw, _p(fi), nk_total, len(no), _p(no), _p(nu), _p(eo),
+                                        _p(eu), _p(zcols), ldz or npr))
+    return chi0
 
 
 # ---------------------------------------------------------------- real frequency axis

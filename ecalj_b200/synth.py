@@ -19,6 +19,8 @@ CONFIGS = {
     # Sigma_c band sum
     "c2": dict(N=600, nq=64, niw=24, ntq=40, nm=400, nreal=50, seed=20262,
                chi_nk=64, chi_nocc=4, chi_nun=(40, 60)),
+    # all-in: zmel of all k is 369 GB, so it is streamed through the GPU k by k
+    "c4": dict(N=1500, nk=512, nocc=40, nun=(300, 1200), niw=32, seed=20264),
 }
 
 

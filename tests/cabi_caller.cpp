@@ -1,0 +1,69 @@
+// A C++ caller of libqsgw_b200 written the way a Fortran or C host would use it:
+// plain pointers to column-major complex(8) arrays, status codes, no torch.
+//   cabi_caller          checks that calls before qsgw_init fail cleanly (no GPU needed)
+//   cabi_caller gpu      also multiplies Fortran-layout matrices with qsgw_zmm (host
+//                        pointers, op(A) = A^H) and compares with a plain triple loop
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include "qsgw_b200.h"
+
+typedef std::complex<double> cd;
+
+static int fail(const char* what) {
+  char msg[512];
+  qsgw_last_error(msg, sizeof(msg));
+  std::printf("FAIL %s: %s\n", what, msg);
+  return 1;
+}
+
+int main(int argc, char** argv) {
+  // before init: every entry point returns QSGW_ERR_NOTINIT and sets a message
+  double dummy[2] = {0, 0};
+  if (qsgw_zmm(dummy, dummy, dummy, 1, 1, 1, 0, 0, dummy, dummy, 1, 1, 1) != QSGW_ERR_NOTINIT)
+    return fail("qsgw_zmm before init");
+  char msg[256];
+  qsgw_last_error(msg, sizeof(msg));
+  if (std::strstr(msg, "qsgw_init") == nullptr) return fail("error text");
+  if (argc < 2 || std::strcmp(argv[1], "gpu") != 0) {
+    std::printf("OK cpu\n");
+    return 0;
+  }
+  if (qsgw_init(0) != QSGW_OK) return fail("qsgw_init");
+  const int m = 37, n = 29, k = 41, lda = k + 3, ldb = k + 1, ldc = m + 2;
+  std::vector<cd> a(static_cast<size_t>(lda) * m), b(static_cast<size_t>(ldb) * n), c(static_cast<size_t>(ldc) * n);
+  unsigned s = 12345u;
+  auto rnd = [&]() { s = s * 1664525u + 1013904223u; return (s >> 8) / 16777216.0 - 0.5; };
+  for (auto& x : a) x = cd(rnd(), rnd());
+  for (auto& x : b) x = cd(rnd(), rnd());
+  for (auto& x : c) x = cd(rnd(), rnd());
+  std::vector<cd> ref = c;
+  const cd alpha(0.5, -1.25), beta(2.0, 0.5);
+  // C = alpha A^H B + beta C, A stored (k x m), column-major
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) {
+      cd acc = 0;
+      for (int l = 0; l < k; ++l) acc += std::conj(a[l + static_cast<size_t>(lda) * i]) * b[l + static_cast<size_t>(ldb) * j];
+      ref[i + static_cast<size_t>(ldc) * j] = alpha * acc + beta * c[i + static_cast<size_t>(ldc) * j];
+    }
+  const double al[2] = {alpha.real(), alpha.imag()}, be[2] = {beta.real(), beta.imag()};
+  if (qsgw_zmm(reinterpret_cast<double*>(a.data()), reinterpret_cast<double*>(b.data()),
+               reinterpret_cast<double*>(c.data()), m, n, k, 2, 0, al, be, lda, ldb, ldc) != QSGW_OK)
+    return fail("qsgw_zmm");
+  double num = 0, den = 0;
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) {
+      num += std::norm(c[i + static_cast<size_t>(ldc) * j] - ref[i + static_cast<size_t>(ldc) * j]);
+      den += std::norm(ref[i + static_cast<size_t>(ldc) * j]);
+    }
+  const double rel = std::sqrt(num / den);
+  qsgw_finalize();
+  if (!(rel <= 1e-13)) {
+    std::printf("FAIL relative error %.3e\n", rel);
+    return 1;
+  }
+  std::printf("OK gpu %.3e\n", rel);
+  return 0;
+}
