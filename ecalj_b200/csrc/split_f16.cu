@@ -40,7 +40,7 @@ constexpr int NSTAGE = 2;
 constexpr int NTHREADS = 576;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..17 drain
 constexpr int NCONV = 256;               // converter threads (warps 2..9), two per B' row
 constexpr int CONV_W0 = 2, DRAIN_W0 = 10;
-constexpr int NDRAIN_WARPS = 8;          // drain warps 10..17: two per TMEM lane quadrant, 64 columns each
+constexpr int NDRAIN_WARPS = 8;          // chi0 drain warps 10..17 (64 columns each); Sigma_c: warps 2..17 (32 each)
 constexpr int NBUF = 3;                  // B' buffers
 constexpr int DRAIN_PERIOD = 2;          // K chunks per FP32 accumulation run (24 MMAs)
 constexpr int SLICE_A = BM2 * KC * 2;    // 16 KB
@@ -268,12 +268,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   }
   const int nchunk = (p.mode == MODE_SEG) ? nseg * p.cps : max(0, c1 - c0);
   const int cbeg = (p.mode == MODE_SEG) ? 0 : c0;
-  const int nper = (nchunk + DRAIN_PERIOD - 1) / DRAIN_PERIOD;
+  // accumulation periods of DRAIN_PERIOD chunks; Sigma_c periods never straddle a segment,
+  // because the drain applies the segment's per-column weight to the period's sum
+  // Sigma_c: one period per segment (its K is short: 2 ngb), so the drain has a whole
+  // segment of MMA time to fold the previous one in
+  const int sdp = (p.mode == MODE_SEG) ? p.cps : DRAIN_PERIOD;   // chunks per period
+  const int pps = (p.cps + sdp - 1) / sdp;                       // periods per segment
+  const int nper = (p.mode == MODE_SEG) ? nseg * pps : (nchunk + DRAIN_PERIOD - 1) / DRAIN_PERIOD;
 
   if (tid == 0) {
     for (int i = 0; i < NSTAGE; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
     for (int i = 0; i < NBUF; ++i) { mbar_init(&bfull[i], NCONV); mbar_init(&bempty[i], 1); }
-    for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], NDRAIN_WARPS); }
+    // Sigma_c has no converters: their warps drain too (twice the drain warps)
+    const int ndrain = (p.mode == MODE_SEG) ? 2 * NDRAIN_WARPS : NDRAIN_WARPS;
+    for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], ndrain); }
     mbar_init(done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -319,18 +327,31 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       for (int c = max(0, issued - NSTAGE); c < issued; ++c) mbar_drain(&full[c % NSTAGE], (c / NSTAGE) & 1);
     } else if (warp == 1 && lane == 0) {
       // ---------------- MMA issuer
+      const bool seg_mode = p.mode == MODE_SEG;
       for (int c = 0; c < nchunk && !*abort_flag; ++c) {
         const int st = c % NSTAGE;
-        const int per = c / DRAIN_PERIOD;
+        int per, cin;
+        if (seg_mode) {
+          const int sg = c / p.cps;
+          cin = c - sg * p.cps;
+          per = sg * pps + cin / sdp;
+        } else {
+          cin = c;
+          per = c / DRAIN_PERIOD;
+        }
         const int ab = per & 1;                      // accumulator of this period
-        const bool first_of_period = (c % DRAIN_PERIOD) == 0;
+        const bool first_of_period = (cin % sdp) == 0;
+        const bool last_of_period = (cin % sdp) == sdp - 1 || c == nchunk - 1 || (seg_mode && cin == p.cps - 1);
         if (first_of_period && per >= 2 && !mbar_wait(&accempty[ab], ((per >> 1) - 1) & 1, abort_flag)) break;
         if (!mbar_wait(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
-        const int b = c % NBUF;                      // B' buffer
-        if (!mbar_wait(&bfull[b], (c / NBUF) & 1, abort_flag)) break;
+        // chi0: B' = weight x S rebuilt by the converters; Sigma_c: B = S itself (its per-column
+        // weight is applied to the FP32 period sums by the drain warps)
+        const int b = c % NBUF;
+        if (!seg_mode && !mbar_wait(&bfull[b], (c / NBUF) & 1, abort_flag)) break;
         tc_fence_after();
         const uint32_t a_hi = smem_u32(sA + st * 2 * SLICE_A), a_lo = a_hi + SLICE_A;
-        const uint32_t b_hi = smem_u32(sB + b * 2 * SLICE_B), b_lo = b_hi + SLICE_B;
+        const uint32_t b_hi = seg_mode ? smem_u32(sS + st * 2 * SLICE_S) : smem_u32(sB + b * 2 * SLICE_B);
+        const uint32_t b_lo = b_hi + (seg_mode ? SLICE_S : SLICE_B);
         const uint32_t d = tmem + static_cast<uint32_t>(ab * NC);
 #pragma unroll
         for (int kk = 0; kk < KC / 16; ++kk) {
@@ -340,15 +361,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_lo + ko), 1u);
           umma_f16(d, sw128_desc(a_lo + ko), sw128_desc(b_hi + ko), 1u);
         }
-        umma_commit(&bempty[b]);
+        if (!seg_mode) umma_commit(&bempty[b]);
         umma_commit(&empty[st]);
-        if ((c % DRAIN_PERIOD) == DRAIN_PERIOD - 1 || c == nchunk - 1) umma_commit(&accfull[ab]);
+        if (last_of_period) umma_commit(&accfull[ab]);
       }
       // everything issued has retired before TMEM may be freed
       umma_commit(done);
       mbar_drain(done, 0);
-    } else if (warp >= CONV_W0 && warp < DRAIN_W0) {
-      // ---------------- converters: B' = weight * (S_hi + S_lo), re-split to FP16 hi/lo
+    } else if (warp >= CONV_W0 && warp < DRAIN_W0 && p.mode == MODE_CHI0) {
+      // ---------------- converters (chi0): B' = weight * (S_hi + S_lo), re-split to FP16 hi/lo
       const int ctid = tid - 32 * CONV_W0;     // 0..255
       const int ct = ctid >> 1;                // row n of the tile
       const int h = ctid & 1;                  // which four of the eight 16-byte chunks
@@ -359,28 +380,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
         for (int i = 0; i < 4; ++i) wv[i] = __ldg(src + i);
       };
-      if (p.mode == MODE_CHI0) load_w(0, wn);
-      int seg_cached = -1;
-      float rs = 0.f;
+      load_w(0, wn);
       for (int c = 0; c < nchunk; ++c) {
         const int st = c % NSTAGE;
         float4 wc[4];
-        if (p.mode == MODE_CHI0) {
 #pragma unroll
-          for (int i = 0; i < 4; ++i) wc[i] = wn[i];
-          if (c + 1 < nchunk) load_w(c + 1, wn);      // prefetch while this chunk converts
-        } else {
-#pragma unroll
-          for (int i = 0; i < 4; ++i) wc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-          const int sg = c / p.cps;
-          if (sg != seg_cached) {
-            const int col = p.tile_cols[nt * NC + ct];
-            const ZSeg zs = p.segs[seg0 + sg];
-            const double sc = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
-            rs = static_cast<float>(sc * p.scales[2]);
-            seg_cached = sg;
-          }
-        }
+        for (int i = 0; i < 4; ++i) wc[i] = wn[i];
+        if (c + 1 < nchunk) load_w(c + 1, wn);      // prefetch while this chunk converts
         if (!mbar_wait_warp(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
         const int b = c % NBUF;
         if (c >= NBUF && !mbar_wait_warp(&bempty[b], ((c / NBUF) - 1) & 1, abort_flag)) break;
@@ -403,7 +409,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             // the pair (re, im) of complex k = 4*ch + q
-            const float f = (p.mode == MODE_CHI0) ? wq[q] : rs;
+            const float f = wq[q];
             const float2 fh = __half22float2(h2[q]);
             const float2 fl = __half22float2(l2[q]);
             const float v0 = (fh.x + fl.x) * f, v1 = (fh.y + fl.y) * f;
@@ -418,20 +424,37 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         fence_async_smem();
         mbar_arrive(&bfull[b]);
       }
-    } else if (warp >= DRAIN_W0) {
-      // ---------------- drain: FP32 accumulator -> FP64 sums in TMEM, then the output
-      const int quad = warp & 3;                          // TMEM lanes 32*quad .. +31
-      const int colh = (warp - DRAIN_W0) >> 2;            // columns 64*colh .. +63
+    } else if (warp >= DRAIN_W0 || (p.mode == MODE_SEG && warp >= CONV_W0)) {
+      // ---------------- drain: FP32 accumulator -> FP64 sums in TMEM, then the output.
+      // chi0: warps 10..17, 64 columns each; Sigma_c: warps 2..17, 32 columns each.
+      const bool seg_mode = p.mode == MODE_SEG;
+      const int d = warp - (seg_mode ? CONV_W0 : DRAIN_W0);
+      const int quad = warp & 3;                          // TMEM lanes 32*quad .. +31 (warp id mod 4)
+      const int ncolw = seg_mode ? NC / 4 : NC / 2;       // columns of this warp
+      const int c_lo = (d >> 2) * ncolw;                  // first column
       const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
       bool ok = true;
+      // Sigma_c: the segment's weights of this warp's columns, in the (then unused) B' area
+      double* wsm = reinterpret_cast<double*>(sB + d * 64 * sizeof(double));
+      int wseg = -1;
       for (int per = 0; per < nper; ++per) {
         const int ab = per & 1;
+        if (seg_mode && per / pps != wseg) {              // a new segment: its per-column weights
+          wseg = per / pps;
+          const ZSeg zs = p.segs[seg0 + wseg];
+          __syncwarp();                                   // the previous segment's reads are done
+          for (int j = lane; j < ncolw; j += 32) {
+            const int col = p.tile_cols[nt * NC + c_lo + j];
+            wsm[j] = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
+          }
+          __syncwarp();
+        }
         if (!mbar_wait_warp(&accfull[ab], (per >> 1) & 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
 #pragma unroll 1
-        for (int cp = 0; cp < 2; ++cp) {                  // two pairs of 16-column blocks
+        for (int cp = 0; cp < ncolw / 32; ++cp) {         // pairs of 16-column blocks
           uint32_t f32a[16], f32b[16], f64w[32];
-          const int c0b = colh * 64 + cp * 32;
+          const int c0b = c_lo + cp * 32;
           tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + c0b), f32a);
           tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NC + c0b + 16), f32b);
 #pragma unroll
@@ -442,7 +465,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
               double a0 = (per > 0) ? __hiloint2double(static_cast<int>(f64w[2 * i + 1]), static_cast<int>(f64w[2 * i])) : 0.0;
-              a0 += static_cast<double>(__uint_as_float(half ? f32b[i] : f32a[i]));
+              const double v = static_cast<double>(__uint_as_float(half ? f32b[i] : f32a[i]));
+              if (seg_mode) {                             // column cp*32 + half*16 + i of this warp's
+                a0 = fma(v, wsm[cp * 32 + half * 16 + i], a0);
+              } else {
+                a0 += v;
+              }
               f64w[2 * i] = static_cast<uint32_t>(__double2loint(a0));
               f64w[2 * i + 1] = static_cast<uint32_t>(__double2hiint(a0));
             }
@@ -464,13 +492,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (p.mode == MODE_CHI0) {
           inv /= p.scales[2 + jw];
           Cj = p.C + static_cast<long long>(jw) * p.c_bs;
-        } else {
-          inv /= p.scales[2];
-        }
+        }                                           // Sigma_c: weights applied in FP64 above, no sigma_B
 #pragma unroll 1
-        for (int cb = 0; cb < 4; ++cb) {
+        for (int cb = 0; cb < ncolw / 16; ++cb) {
           uint32_t f64[32];
-          const int cbase = colh * 64 + cb * 16;
+          const int cbase = c_lo + cb * 16;
           tmem_ld32w(tmem + lane_base + FP64_COL + static_cast<uint32_t>(2 * cbase), f64);
           tmem_wait_ld();
           if (m >= p.M) continue;
