@@ -36,8 +36,8 @@ METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err 
 # ----------------------------------------------------------------------------- helpers
 # DRAM bytes (read + write) of one split-precision Sigma_c task launch
 # (N=600, 40 x 400 states, 25 imaginary slots + real-axis pole columns),
-# measured with ncu on that launch: 2.118 GB read + 0.196 GB written.
-SIGC_TC_TRAFFIC = 2.314e9
+# measured with ncu on that launch: 1.975 GB read + 0.240 GB written.
+SIGC_TC_TRAFFIC = 2.215e9
 
 
 def load_peaks():
