@@ -109,6 +109,8 @@ _SIGS = {
                                  c_int],
     "qsgw_wvr_llw_d": [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_int],
     "qsgw_zminv_batched_d": [c_vp, c_int, c_int, c_int],
+    "qsgw_tetwt_hist_d": [c_vp, c_int, c_int, c_int, c_int, c_vp, c_int, c_vp, c_vp, c_vp, c_int, ctypes.c_double,
+                          c_vp, c_vp],
     "qsgw_wv_write_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int],
     "qsgw_wv_read_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int, c_int, c_int],
     "qsgw_wsurr_init": [ctypes.c_ulonglong],
@@ -504,6 +506,23 @@ def wvr_llw_d(zxq, ngb, nw, nspin, vcousq, m2e, is_x0_m_basis, is_wc_m_basis, iq
 
 def zminv_batched_d(a, n, lda, nbatch):
     _chk(load().qsgw_zminv_batched_d(_p(a), n, lda, nbatch))
+
+
+# ---------------------------------------------------------------- tetrahedron weights
+def tetwt_hist_d(w, idtet, qbzw, ek, ekq, efermi, frhis, nocc, nunocc):
+    """w (device, nwhis x nunocc x nocc x nk, accumulated) += tetrahedron
+    histogram weights; idtet (ntet, 4) 0-based, qbzw (nk, 3), ek/ekq (nk, nband).
+    Returns the total tetrahedron volume."""
+    it = np.ascontiguousarray(np.asarray(idtet, dtype=np.int32))
+    q = np.ascontiguousarray(np.asarray(qbzw, dtype=np.float64))
+    a = np.ascontiguousarray(np.asarray(ek, dtype=np.float64))       # (nk, nband) C order = (nband, nk) F order
+    b = np.ascontiguousarray(np.asarray(ekq, dtype=np.float64))
+    fr = _f64(frhis)
+    vt = ctypes.c_double(0.0)
+    _chk(load().qsgw_tetwt_hist_d(_p(w), a.shape[0], nocc, nunocc, len(fr) - 1, it.ctypes.data, it.shape[0],
+                                  q.ctypes.data, a.ctypes.data, b.ctypes.data, a.shape[1], float(efermi),
+                                  fr.ctypes.data, ctypes.byref(vt)))
+    return vt.value
 
 
 # ---------------------------------------------------------------- W record files

@@ -140,3 +140,36 @@ def ipw_tables(seed, ngc=37, ngp1=29, ngp2=31, ntp0=5, nmv=7, span=2, gbox=6, fi
     phase = np.exp(-2j * np.pi * rng.random(ngc))
     return dict(ngvecpB1=b1, ngvecpB2=b2, ngveccR=gc, nvgcgp2=comp, nvggg=nvggg, ggg=ggg, geigq=geigq,
                 dgeigqk=dgeigqk, phase=phase, nadd=np.array([1, 0, -1], np.int32))
+
+
+def tetra_mesh(n, nband=6, q=(0.13, 0.05, -0.08), seed=0):
+    """A k mesh of the unit cube (n^3 cells, (n+1)^3 corner points) cut into
+    6 tetrahedra per cell, and smooth bands e_b(k) (Ry) crossing e = 0 at k
+    and at k+q: idtet (6 n^3, 4), qbzw ((n+1)^3, 3), ek, ekq ((n+1)^3, nband)."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(n + 1) / n
+    kx, ky, kz = np.meshgrid(g, g, g, indexing="ij")
+    qbzw = np.stack([kx.ravel(), ky.ravel(), kz.ravel()], axis=1)
+    idx = lambda i, j, k: (i * (n + 1) + j) * (n + 1) + k
+    # Freudenthal split of a cube along its main diagonal: 6 tetrahedra
+    paths = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
+    tets = []
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                for p in paths:
+                    c = [i, j, k]
+                    corners = [idx(*c)]
+                    for d in p:
+                        c = list(c)
+                        c[d] += 1
+                        corners.append(idx(*c))
+                    tets.append(corners)
+    phase = rng.uniform(0, 2 * np.pi, (nband, 3))
+    amp = rng.uniform(0.15, 0.3, nband)
+    base = np.linspace(-0.7, 0.8, nband)
+
+    def bands(kp):
+        return base[None, :] + amp[None, :] * np.cos(2 * np.pi * kp[:, None, :] + phase[None, :, :]).sum(-1)
+
+    return np.array(tets, np.int32), qbzw, bands(qbzw), bands(qbzw + np.asarray(q)[None, :])

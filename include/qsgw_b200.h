@@ -347,6 +347,26 @@ int qsgw_wvr_llw_d(double *zxq_d, int ngb, int nw, int nspin, const double *vcou
  * stride lda*n), partial pivoting; a zero pivot sets the status word.      */
 int qsgw_zminv_batched_d(double *a, int n, int lda, int nbatch);
 
+/* ---- Tetrahedron histogram weights of chi0 (tetwt5x_dtet4 with lindtet6,
+ * SRC/subroutines/tetwt5.f90:9-787, tetrahedron_matrix_linear = F, npm = 1,
+ * one micro tetrahedron): for every tetrahedron and every pair (occupied
+ * band ib < nocc at k, band jb < nunocc at k+q) the Rath-Freeman integral
+ *   wtthis(ihis) = int_bin d omega int_tet d^3k f(e_k)(1 - f(e_k+q)) delta(omega - (e_k+q - e_k)/2)
+ * is added to each corner k: w_d(ihis, jb, ib, k) += wtthis * pi / (4 voltot)
+ * (w_d device, nwhis x nunocc x nocc x nk, accumulated: zero it first).
+ * idtet: host (4, ntet) 0-based corner k indices; qbzw: host (3, nk) k
+ * vectors; ek/ekq: host (nband, nk) energies at k and k+q (Ry, as the
+ * reference; omega in Hartree); frhis: host (nwhis + 1) increasing bin
+ * edges (Hartree).  voltot (host, may be NULL) <- total volume.  A pair
+ * whose excitation energies leave the histogram sets the status word
+ * (qsgw_synchronize returns QSGW_ERR_NUMERIC); the reference stops there.
+ * Dense output instead of the reference's (ibjb, ihw, nhw, jhw, whw)
+ * storage; its symmetrisation over degenerate bands is not applied.       */
+int qsgw_tetwt_hist_d(double *w_d, int nk, int nocc, int nunocc, int nwhis,
+                      const int *idtet, int ntet, const double *qbzw,
+                      const double *ek, const double *ekq, int nband,
+                      double efermi, const double *frhis, double *voltot);
+
 /* ---- W record files __WVI.<iq> / __WVR.<iq> in the reference's layout:
  * fixed records without markers, record rec at byte (rec-1)*recl, one
  * nblochpmx x nblochpmx column-major matrix per record, complex(8)
