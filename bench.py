@@ -438,6 +438,7 @@ def main():
         e2e = run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist)
     sur = None
     if not args.no_surrogate:
+        lib.set_autotune(0, None)          # no tuning trials inside the study's timed calls
         sur = surrogate_summary(lib, log)
         lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
     cpu = None

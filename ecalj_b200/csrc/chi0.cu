@@ -7,6 +7,7 @@
 // (x0gemm.f90:37-64); the GPU never materialises zw / wzw: the pair gather
 // and the weight are folded into the operand loads of the DMMA engine.
 #include <memory>
+#include <cmath>
 #include <vector>
 #include "zgemm_f64.cuh"
 #include "autotune.cuh"
@@ -408,7 +409,9 @@ static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int
   for (int c : {heur / 2, heur, heur * 2, heur * 4})
     if (c >= 1 && c <= maxch && (cands.empty() || cands.back() != c)) cands.push_back(c);
   char key[160];
-  std::snprintf(key, sizeof(key), "chi0_dmma npr=%d npair=%lld niw=%d", npr, npair, niw);
+  // pair counts within ~9% share a choice (they differ from q to q)
+  std::snprintf(key, sizeof(key), "chi0_dmma npr=%d npair~2^%.3f niw=%d", npr,
+                std::round(8.0 * std::log2(static_cast<double>(npair))) / 8.0, niw);
   int sk = heur;
   bool tried = false;
   rc = tuned_choice(key, cands, heur, [&](int c) { return run(c, true); }, s, &sk, &tried);

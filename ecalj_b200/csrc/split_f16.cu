@@ -25,6 +25,7 @@
 #include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+#include <cmath>
 #include <vector>
 #include "split_f16.cuh"
 #include "autotune.cuh"
@@ -797,7 +798,9 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   for (int c = 1; c <= std::min(4, maxsplit); ++c) cands.push_back(c);
   if (heur > 4) cands.push_back(heur);
   char key[160];
-  std::snprintf(key, sizeof(key), "chi0_split_f16 npr=%d npair=%lld niw=%d", npr, npair, niw);
+  // pair counts within ~9% share a choice (they differ from q to q)
+  std::snprintf(key, sizeof(key), "chi0_split_f16 npr=%d npair~2^%.3f niw=%d", npr,
+                std::round(8.0 * std::log2(static_cast<double>(npair))) / 8.0, niw);
   int splitk = heur;
   bool tried = false;
   rc = tuned_choice(key, cands, heur, [&](int c) { return run(c, true); }, s, &splitk, &tried);
