@@ -410,14 +410,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             // the pair (re, im) of complex k = 4*ch + q
-            const float f = wq[q];
-            const float2 fh = __half22float2(h2[q]);
-            const float2 fl = __half22float2(l2[q]);
-            const float v0 = (fh.x + fl.x) * f, v1 = (fh.y + fl.y) * f;
-            const __half2 hi = __floats2half2_rn(v0, v1);
+            // (S_hi + S_lo) w, then its FP16 hi and the FP16 of the remainder; the packed
+            // FP32x2 operations round exactly as their scalar pairs
+            const float2 f2 = make_float2(wq[q], wq[q]);
+            const float2 v = __fmul2_rn(__fadd2_rn(__half22float2(h2[q]), __half22float2(l2[q])), f2);
+            const __half2 hi = __float22half2_rn(v);
             const float2 fb = __half22float2(hi);
             oh2[q] = hi;
-            ol2[q] = __floats2half2_rn(v0 - fb.x, v1 - fb.y);
+            ol2[q] = __float22half2_rn(__fadd2_rn(v, make_float2(-fb.x, -fb.y)));
           }
           *reinterpret_cast<uint4*>(d_hi + off) = oh;
           *reinterpret_cast<uint4*>(d_lo + off) = ol;
