@@ -72,5 +72,61 @@ module m_qsgw_b200
       import :: c_int, qsgw_sxcf_args
       type(qsgw_sxcf_args), intent(in) :: args
     end function
+    integer(c_int) function qsgw_wvr_llw_d(zxq, ngb, nw, nspin, vcousq, m2e, is_x0_m_basis, &
+         is_wc_m_basis, iq, zw, nblochpmx) bind(C, name='qsgw_wvr_llw_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: zxq, m2e, zw
+      integer(c_int), value :: ngb, nw, nspin, is_x0_m_basis, is_wc_m_basis, iq, nblochpmx
+      real(c_double), intent(in) :: vcousq(*)
+    end function
+    integer(c_int) function qsgw_zminv_batched_d(a, n, lda, nbatch) bind(C, name='qsgw_zminv_batched_d')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: a
+      integer(c_int), value :: n, lda, nbatch
+    end function
+    integer(c_int) function qsgw_sxcf_exchange_d(zsec, ntq, zmel, ngb, ns1, ns2, ntqxx, vcoud, ekc, nekc, &
+         nctot, ef, esmr, wkkr) bind(C, name='qsgw_sxcf_exchange_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: zsec, zmel
+      integer(c_int), value :: ntq, ngb, ns1, ns2, ntqxx, nekc, nctot
+      real(c_double), intent(in) :: vcoud(*), ekc(*)
+      real(c_double), value :: ef, esmr, wkkr
+    end function
+    integer(c_int) function qsgw_zhegv_d(v, o, n, lda, vcoud) bind(C, name='qsgw_zhegv_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: v, o
+      integer(c_int), value :: n, lda
+      real(c_double), intent(out) :: vcoud(*)
+    end function
+    integer(c_int) function qsgw_tetwt_hist_d(w, nk, nocc, nunocc, nwhis, idtet, ntet, qbzw, ek, ekq, &
+         nband, efermi, frhis, voltot) bind(C, name='qsgw_tetwt_hist_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: w
+      integer(c_int), value :: nk, nocc, nunocc, nwhis, ntet, nband
+      integer(c_int), intent(in) :: idtet(*)
+      real(c_double), intent(in) :: qbzw(*), ek(*), ekq(*), frhis(*)
+      real(c_double), value :: efermi
+      real(c_double), intent(out) :: voltot
+    end function
+    integer(c_int) function qsgw_wv_write_d(path, zw, nblochpmx, rec0, nrec, kind4) bind(C, name='qsgw_wv_write_d')
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), intent(in) :: path(*)
+      type(c_ptr), value :: zw
+      integer(c_int), value :: nblochpmx, rec0, nrec, kind4
+    end function
+    integer(c_int) function qsgw_graph_begin() bind(C, name='qsgw_graph_begin')
+      import :: c_int
+    end function
+    integer(c_int) function qsgw_graph_end() bind(C, name='qsgw_graph_end')
+      import :: c_int
+    end function
+    integer(c_int) function qsgw_graph_launch() bind(C, name='qsgw_graph_launch')
+      import :: c_int
+    end function
+    integer(c_int) function qsgw_set_autotune(mode, cache_path) bind(C, name='qsgw_set_autotune')
+      import :: c_int, c_char
+      integer(c_int), value :: mode
+      character(kind=c_char), intent(in) :: cache_path(*)
+    end function
   end interface
 end module m_qsgw_b200
