@@ -99,6 +99,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+from ecalj_b200.replicas import max_over_ranks  # noqa: E402
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -369,9 +372,7 @@ def main():
         lib.profile(False)
         clocks = sampler.stop() if sampler else None
         if ws > 1:
-            tt = torch.tensor([ms], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
+            ms = max_over_ranks(ms, dist, "cuda")
             dist.barrier()
         return ms, kt, launches, clocks
 
@@ -565,9 +566,7 @@ def run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / nst
     if ws > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+        ms = max_over_ranks(ms, dist, "cuda")
     del host
     return {"value": round(ws * flops / (ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(ms, 3),
