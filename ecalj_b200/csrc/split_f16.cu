@@ -38,6 +38,7 @@ constexpr int BMC = 64;                  // complex rows per tile
 constexpr int NC = 128;                  // complex columns per tile (UMMA N)
 constexpr int KC = 64;                   // FP16 elements per chunk along K' (32 complex k)
 constexpr int NSTAGE = 2;
+static_assert((NSTAGE & (NSTAGE - 1)) == 0, "stage index uses a mask");
 constexpr int NTHREADS = 576;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..17 drain
 constexpr int NCONV = 256;               // converter threads (warps 2..9), two per B' row
 constexpr int CONV_W0 = 2, DRAIN_W0 = 10;
@@ -302,8 +303,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // ---------------- TMA producer
       const uint32_t bytes = 2 * SLICE_A + 2 * SLICE_S;
       int issued = 0;
+      // Sigma_c: segment and chunk-in-segment advanced by counting (this thread is on the
+      // critical path of every chunk: no divisions, one table load per segment)
+      int sg = 0, cin = 0;
+      int t = (p.mode == MODE_SEG && nseg > 0) ? p.seg_slot[seg0] * p.tiles_per_slot + mt : 0;
       for (int c = 0; c < nchunk; ++c) {
-        const int st = c % NSTAGE;
+        const int st = c & (NSTAGE - 1);
         if (c >= NSTAGE && !mbar_wait(&empty[st], ((c / NSTAGE) - 1) & 1, abort_flag)) break;
         issued = c + 1;
         mbar_expect_tx(&full[st], bytes);
@@ -316,39 +321,33 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           tma_load_4d(s, &mapS, &full[st], x, 0, 0, 2 * nt);
           tma_load_4d(s + SLICE_S, &mapS, &full[st], x, 0, 0, p.lo_row_off + 2 * nt);
         } else {
-          const int sg = c / p.cps;
-          const int x = (c - sg * p.cps) * KC;
-          const int t = p.seg_slot[seg0 + sg] * p.tiles_per_slot + mt;
+          const int x = cin * KC;
           tma_load_4d(a, &mapA, &full[st], x, 0, 0, t);
           tma_load_4d(a + SLICE_A, &mapA, &full[st], x, 0, 0, p.lo_tile_off + t);
           tma_load_2d(s, &mapS, &full[st], x, nt * NC);
           tma_load_2d(s + SLICE_S, &mapS, &full[st], x, p.lo_row_off + nt * NC);
+          if (++cin == p.cps) {
+            cin = 0;
+            if (++sg < nseg) t = p.seg_slot[seg0 + sg] * p.tiles_per_slot + mt;
+          }
         }
       }
       for (int c = max(0, issued - NSTAGE); c < issued; ++c) mbar_drain(&full[c % NSTAGE], (c / NSTAGE) & 1);
     } else if (warp == 1 && lane == 0) {
       // ---------------- MMA issuer
       const bool seg_mode = p.mode == MODE_SEG;
+      // counters instead of divisions: this thread's issue latency paces the tensor pipe
+      int per = 0, cin = 0, cin_p = 0, b = 0, bph = 0;
       for (int c = 0; c < nchunk && !*abort_flag; ++c) {
-        const int st = c % NSTAGE;
-        int per, cin;
-        if (seg_mode) {
-          const int sg = c / p.cps;
-          cin = c - sg * p.cps;
-          per = sg * pps + cin / sdp;
-        } else {
-          cin = c;
-          per = c / DRAIN_PERIOD;
-        }
+        const int st = c & (NSTAGE - 1);
         const int ab = per & 1;                      // accumulator of this period
-        const bool first_of_period = (cin % sdp) == 0;
-        const bool last_of_period = (cin % sdp) == sdp - 1 || c == nchunk - 1 || (seg_mode && cin == p.cps - 1);
+        const bool first_of_period = cin_p == 0;
+        const bool last_of_period = cin_p == sdp - 1 || c == nchunk - 1 || (seg_mode && cin == p.cps - 1);
         if (first_of_period && per >= 2 && !mbar_wait(&accempty[ab], ((per >> 1) - 1) & 1, abort_flag)) break;
         if (!mbar_wait(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
         // chi0: B' = weight x S rebuilt by the converters; Sigma_c: B = S itself (its per-column
         // weight is applied to the FP32 period sums by the drain warps)
-        const int b = c % NBUF;
-        if (!seg_mode && !mbar_wait(&bfull[b], (c / NBUF) & 1, abort_flag)) break;
+        if (!seg_mode && !mbar_wait(&bfull[b], bph, abort_flag)) break;
         tc_fence_after();
         const uint32_t a_hi = smem_u32(sA + st * 2 * SLICE_A), a_lo = a_hi + SLICE_A;
         const uint32_t b_hi = seg_mode ? smem_u32(sS + st * 2 * SLICE_S) : smem_u32(sB + b * 2 * SLICE_B);
@@ -365,6 +364,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (!seg_mode) umma_commit(&bempty[b]);
         umma_commit(&empty[st]);
         if (last_of_period) umma_commit(&accfull[ab]);
+        // advance: B' buffer, chunk in period / segment, period
+        if (++b == NBUF) { b = 0; bph ^= 1; }
+        ++cin_p;
+        if (seg_mode && ++cin == p.cps) { cin = 0; cin_p = 0; ++per; }
+        else if (cin_p == sdp) { cin_p = 0; ++per; }
       }
       // everything issued has retired before TMEM may be freed
       umma_commit(done);
