@@ -12,13 +12,15 @@
 //
 // The weight that differs per frequency (chi0, x0gemm.f90:84) or per
 // segment and column (Sigma_c, m_sxcf_gemm.f90:485) multiplies B.  A' and
-// the B source are pre-split once into HBM and streamed by TMA; four
-// converter warps apply the weight to the B source in shared memory and
-// re-split it into B' for every frequency / segment, while one thread issues
-// the MMAs.  Warp roles (448 threads, one CTA per SM):
+// the B source are pre-split once into HBM and streamed by TMA.  chi0: eight
+// converter warps apply the frequency weight to the B source in shared
+// memory and re-split it into B' for every frequency, while one thread issues
+// the MMAs.  Sigma_c: S itself is the B operand and the drain applies the
+// per-(segment, column) weight to each segment's FP32 sum in FP64.  Warp
+// roles (576 threads, one CTA per SM):
 //     warp 0        TMA producer
 //     warp 1        TMEM owner and MMA issuer
-//     warps 2..9    B' converters (two threads per B' row)
+//     warps 2..9    chi0: B' converters (two threads per B' row); Sigma_c: drain
 //     warps 10..17  drain: FP32 accumulators -> FP64 sums in TMEM -> output
 // Every mbarrier wait is bounded; on time-out the CTA records an error,
 // drains its own TMA and MMA work, frees TMEM and exits.
@@ -37,8 +39,6 @@ constexpr int BM2 = 128;                 // real accumulator rows (64 complex x 
 constexpr int BMC = 64;                  // complex rows per tile
 constexpr int NC = 128;                  // complex columns per tile (UMMA N)
 constexpr int KC = 64;                   // FP16 elements per chunk along K' (32 complex k)
-constexpr int NSTAGE = 2;
-static_assert((NSTAGE & (NSTAGE - 1)) == 0, "stage index uses a mask");
 constexpr int NTHREADS = 576;            // warp 0 TMA, 1 MMA, 2..9 converters, 10..17 drain
 constexpr int NCONV = 256;               // converter threads (warps 2..9), two per B' row
 constexpr int CONV_W0 = 2, DRAIN_W0 = 10;
@@ -48,18 +48,28 @@ constexpr int DRAIN_PERIOD = 2;          // K chunks per FP32 accumulation run (
 constexpr int SLICE_A = BM2 * KC * 2;    // 16 KB
 constexpr int SLICE_S = NC * KC * 2;     // 16 KB
 constexpr int SLICE_B = NC * KC * 2;     // 16 KB
-constexpr int OFF_A = 0;
-constexpr int OFF_S = OFF_A + NSTAGE * 2 * SLICE_A;
-constexpr int OFF_B = OFF_S + NSTAGE * 2 * SLICE_S;
-constexpr int OFF_BAR = OFF_B + NBUF * 2 * SLICE_B;
-constexpr int NBAR = 2 * NSTAGE + 2 * NBUF + 2 + 2 + 1;
-constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
-constexpr int SMEM_BYTES = OFF_MISC + 64 + 1024;        // + slack for 1024-B alignment
 constexpr uint32_t TMEM_COLS = 512;                      // acc0 [0,128) acc1 [128,256) FP64 sums [256,512)
 constexpr uint32_t FP64_COL = 256;
 constexpr long long WAIT_LIMIT = 1LL << 24;              // bounded spin (several seconds)
 
 enum { MODE_CHI0 = 0, MODE_SEG = 1 };
+
+// Shared-memory layout per mode.  chi0: two TMA stages (A' and S, hi and lo
+// slices) and three B' buffers.  Sigma_c multiplies by S directly, so the B'
+// area only holds the drain warps' per-column weights and a third stage fits.
+template <int MODE>
+struct Cfg {
+  static constexpr int NST = MODE == MODE_SEG ? 3 : 2;            // TMA stages
+  static constexpr int BAREA = MODE == MODE_SEG ? 2 * 8 * 64 * 8 : NBUF * 2 * SLICE_B;
+  static constexpr int OFF_A = 0;
+  static constexpr int OFF_S = OFF_A + NST * 2 * SLICE_A;
+  static constexpr int OFF_B = OFF_S + NST * 2 * SLICE_S;
+  static constexpr int OFF_BAR = OFF_B + BAREA;
+  static constexpr int NBAR = 2 * NST + 2 * NBUF + 2 + 2 + 1;
+  static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
+  static constexpr int SMEM_BYTES = OFF_MISC + 64 + 1024;         // + slack for 1024-B alignment
+  static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
+};
 
 struct Params {
   int mode;
@@ -232,26 +242,31 @@ __device__ __forceinline__ int sw128_off(int r, int c) { return r * 128 + ((c ^ 
 // (chi0) or of the Sigma_c column tile, over its K range.  FP32 accumulation
 // in the tensor core truncates, so its error grows with the run length; the
 // MMA thread therefore alternates two TMEM accumulators every DRAIN_PERIOD
-// chunks while four drain warps fold the finished one into FP64 sums kept in
+// chunks (Sigma_c: every segment) while the drain warps fold the finished one
+// into FP64 sums kept in
 // TMEM (columns 256..511, two 32-bit words per value).
+template <int MODE>
 __global__ void __launch_bounds__(NTHREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapS,
                       const Params p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  unsigned char* sA = sm + OFF_A;
-  unsigned char* sS = sm + OFF_S;
-  unsigned char* sB = sm + OFF_B;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
-  uint64_t* full = bar;                  // [NSTAGE] TMA -> MMA, converters
-  uint64_t* empty = bar + NSTAGE;        // [NSTAGE] MMA -> TMA
-  uint64_t* bfull = bar + 2 * NSTAGE;    // [NBUF] converters -> MMA
+  using L = Cfg<MODE>;
+  constexpr int NST = L::NST;
+  constexpr bool SEG = MODE == MODE_SEG;
+  unsigned char* sA = sm + L::OFF_A;
+  unsigned char* sS = sm + L::OFF_S;
+  unsigned char* sB = sm + L::OFF_B;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::OFF_BAR);
+  uint64_t* full = bar;                  // [NST] TMA -> MMA, converters
+  uint64_t* empty = bar + NST;        // [NST] MMA -> TMA
+  uint64_t* bfull = bar + 2 * NST;    // [NBUF] converters -> MMA
   uint64_t* bempty = bfull + NBUF;       // [NBUF] MMA -> converters
   uint64_t* accfull = bempty + NBUF;     // [2] MMA -> drain
   uint64_t* accempty = accfull + 2;      // [2] drain -> MMA
   uint64_t* done = accempty + 2;         // [1] every MMA of the CTA retired
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + OFF_MISC);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + OFF_MISC + 8);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::OFF_MISC);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::OFF_MISC + 8);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // ---- work unit
@@ -259,30 +274,30 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   const int mt = tileid % p.ntm, nt = tileid / p.ntm;
   const int jw = blockIdx.y;                       // chi0: frequency index
   const int split = blockIdx.z;
-  if (p.mode == MODE_CHI0 && p.herm && mt * BMC + BMC - 1 < nt * NC) return;   // strictly upper tile
+  if (!SEG && p.herm && mt * BMC + BMC - 1 < nt * NC) return;   // strictly upper tile
   const int c0 = split * p.kch_per_split;
   const int c1 = min(p.kch_total, c0 + p.kch_per_split);
   int seg0 = 0, nseg = 0;
-  if (p.mode == MODE_SEG) {
+  if (SEG) {
     const int group = p.tile_group[nt];
     nseg = p.group_nseg[group];
     seg0 = p.group_seg_off[group];
   }
-  const int nchunk = (p.mode == MODE_SEG) ? nseg * p.cps : max(0, c1 - c0);
-  const int cbeg = (p.mode == MODE_SEG) ? 0 : c0;
+  const int nchunk = SEG ? nseg * p.cps : max(0, c1 - c0);
+  const int cbeg = SEG ? 0 : c0;
   // accumulation periods of DRAIN_PERIOD chunks; Sigma_c periods never straddle a segment,
   // because the drain applies the segment's per-column weight to the period's sum
   // Sigma_c: one period per segment (its K is short: 2 ngb), so the drain has a whole
   // segment of MMA time to fold the previous one in
-  const int sdp = (p.mode == MODE_SEG) ? p.cps : DRAIN_PERIOD;   // chunks per period
+  const int sdp = SEG ? p.cps : DRAIN_PERIOD;                    // chunks per period
   const int pps = (p.cps + sdp - 1) / sdp;                       // periods per segment
-  const int nper = (p.mode == MODE_SEG) ? nseg * pps : (nchunk + DRAIN_PERIOD - 1) / DRAIN_PERIOD;
+  const int nper = SEG ? nseg * pps : (nchunk + DRAIN_PERIOD - 1) / DRAIN_PERIOD;
 
   if (tid == 0) {
-    for (int i = 0; i < NSTAGE; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
     for (int i = 0; i < NBUF; ++i) { mbar_init(&bfull[i], NCONV); mbar_init(&bempty[i], 1); }
     // Sigma_c has no converters: their warps drain too (twice the drain warps)
-    const int ndrain = (p.mode == MODE_SEG) ? 2 * NDRAIN_WARPS : NDRAIN_WARPS;
+    const int ndrain = SEG ? 2 * NDRAIN_WARPS : NDRAIN_WARPS;
     for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], ndrain); }
     mbar_init(done, 1);
     *abort_flag = 0;
@@ -306,15 +321,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // Sigma_c: segment and chunk-in-segment advanced by counting (this thread is on the
       // critical path of every chunk: no divisions, one table load per segment)
       int sg = 0, cin = 0;
-      int t = (p.mode == MODE_SEG && nseg > 0) ? p.seg_slot[seg0] * p.tiles_per_slot + mt : 0;
+      int t = (SEG && nseg > 0) ? p.seg_slot[seg0] * p.tiles_per_slot + mt : 0;
       for (int c = 0; c < nchunk; ++c) {
-        const int st = c & (NSTAGE - 1);
-        if (c >= NSTAGE && !mbar_wait(&empty[st], ((c / NSTAGE) - 1) & 1, abort_flag)) break;
+        const int st = c % NST;
+        if (c >= NST && !mbar_wait(&empty[st], ((c / NST) - 1) & 1, abort_flag)) break;
         issued = c + 1;
         mbar_expect_tx(&full[st], bytes);
         unsigned char* a = sA + st * 2 * SLICE_A;
         unsigned char* s = sS + st * 2 * SLICE_S;
-        if (p.mode == MODE_CHI0) {
+        if (!SEG) {
           const int x = (cbeg + c) * KC;
           tma_load_4d(a, &mapA, &full[st], x, 0, 0, mt);
           tma_load_4d(a + SLICE_A, &mapA, &full[st], x, 0, 0, p.lo_tile_off + mt);
@@ -332,19 +347,19 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
         }
       }
-      for (int c = max(0, issued - NSTAGE); c < issued; ++c) mbar_drain(&full[c % NSTAGE], (c / NSTAGE) & 1);
+      for (int c = max(0, issued - NST); c < issued; ++c) mbar_drain(&full[c % NST], (c / NST) & 1);
     } else if (warp == 1 && lane == 0) {
       // ---------------- MMA issuer
-      const bool seg_mode = p.mode == MODE_SEG;
+      constexpr bool seg_mode = SEG;
       // counters instead of divisions: this thread's issue latency paces the tensor pipe
       int per = 0, cin = 0, cin_p = 0, b = 0, bph = 0;
       for (int c = 0; c < nchunk && !*abort_flag; ++c) {
-        const int st = c & (NSTAGE - 1);
+        const int st = c % NST;
         const int ab = per & 1;                      // accumulator of this period
         const bool first_of_period = cin_p == 0;
         const bool last_of_period = cin_p == sdp - 1 || c == nchunk - 1 || (seg_mode && cin == p.cps - 1);
         if (first_of_period && per >= 2 && !mbar_wait(&accempty[ab], ((per >> 1) - 1) & 1, abort_flag)) break;
-        if (!mbar_wait(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
+        if (!mbar_wait(&full[st], (c / NST) & 1, abort_flag)) break;
         // chi0: B' = weight x S rebuilt by the converters; Sigma_c: B = S itself (its per-column
         // weight is applied to the FP32 period sums by the drain warps)
         if (!seg_mode && !mbar_wait(&bfull[b], bph, abort_flag)) break;
@@ -373,7 +388,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // everything issued has retired before TMEM may be freed
       umma_commit(done);
       mbar_drain(done, 0);
-    } else if (warp >= CONV_W0 && warp < DRAIN_W0 && p.mode == MODE_CHI0) {
+    } else if (warp >= CONV_W0 && warp < DRAIN_W0 && !SEG) {
       // ---------------- converters (chi0): B' = weight * (S_hi + S_lo), re-split to FP16 hi/lo
       const int ctid = tid - 32 * CONV_W0;     // 0..255
       const int ct = ctid >> 1;                // row n of the tile
@@ -387,12 +402,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       };
       load_w(0, wn);
       for (int c = 0; c < nchunk; ++c) {
-        const int st = c % NSTAGE;
+        const int st = c % NST;
         float4 wc[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) wc[i] = wn[i];
         if (c + 1 < nchunk) load_w(c + 1, wn);      // prefetch while this chunk converts
-        if (!mbar_wait_warp(&full[st], (c / NSTAGE) & 1, abort_flag)) break;
+        if (!mbar_wait_warp(&full[st], (c / NST) & 1, abort_flag)) break;
         const int b = c % NBUF;
         if (c >= NBUF && !mbar_wait_warp(&bempty[b], ((c / NBUF) - 1) & 1, abort_flag)) break;
         const unsigned char* s_hi = sS + st * 2 * SLICE_S;
@@ -429,10 +444,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         fence_async_smem();
         mbar_arrive(&bfull[b]);
       }
-    } else if (warp >= DRAIN_W0 || (p.mode == MODE_SEG && warp >= CONV_W0)) {
+    } else if (warp >= DRAIN_W0 || (SEG && warp >= CONV_W0)) {
       // ---------------- drain: FP32 accumulator -> FP64 sums in TMEM, then the output.
       // chi0: warps 10..17, 64 columns each; Sigma_c: warps 2..17, 32 columns each.
-      const bool seg_mode = p.mode == MODE_SEG;
+      constexpr bool seg_mode = SEG;
       const int d = warp - (seg_mode ? CONV_W0 : DRAIN_W0);
       const int quad = warp & 3;                          // TMEM lanes 32*quad .. +31 (warp id mod 4)
       const int ncolw = seg_mode ? NC / 4 : NC / 2;       // columns of this warp
@@ -494,7 +509,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const bool im_part = row >= 64;
         double inv = 1.0 / (p.scales[0] * p.scales[1]);
         double2* Cj = p.C;
-        if (p.mode == MODE_CHI0) {
+        if (!SEG) {
           inv /= p.scales[2 + jw];
           Cj = p.C + static_cast<long long>(jw) * p.c_bs;
         }                                           // Sigma_c: weights applied in FP64 above, no sigma_B
@@ -509,7 +524,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           for (int i = 0; i < 16; ++i) {
             const double v = __hiloint2double(static_cast<int>(f64[2 * i + 1]), static_cast<int>(f64[2 * i])) * inv;
             const int nloc = cbase + i;
-            if (p.mode == MODE_CHI0) {
+            if (!SEG) {
               const int n = nt * NC + nloc;
               if (n >= p.N) continue;
               if (p.herm && m < n) continue;                // upper part comes from the mirror
@@ -690,16 +705,24 @@ static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* di
 }
 
 static DevBuf g_a, g_s, g_mx, g_sc, g_tabs, g_w32;
-static bool g_attr = false;
+
+template <int MODE>
+static int launch_mode(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    QSGW_CUDA(cudaFuncSetAttribute(split_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Cfg<MODE>::SMEM_BYTES));
+    attr = true;
+  }
+  split_gemm_kernel<MODE><<<grid, NTHREADS, Cfg<MODE>::SMEM_BYTES, s>>>(ma, ms, p);
+  return QSGW_OK;
+}
 
 static int launch_split(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s,
                         const char* tag) {
-  if (!g_attr) {
-    QSGW_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    g_attr = true;
-  }
   const int pi = prof_begin(tag, s);
-  split_gemm_kernel<<<grid, NTHREADS, SMEM_BYTES, s>>>(ma, ms, p);
+  const int rc = (p.mode == MODE_SEG) ? launch_mode<MODE_SEG>(ma, ms, p, grid, s) : launch_mode<MODE_CHI0>(ma, ms, p, grid, s);
+  if (rc) return rc;
   prof_end(pi, s);
   count_launch();
   QSGW_LAUNCH_CHECK("split_gemm_kernel");
