@@ -70,6 +70,7 @@ _SIGS = {
     "qsgw_set_stream": [c_vp],
     "qsgw_synchronize": [],
     "qsgw_set_precision": [c_int, c_int],
+    "qsgw_set_sigc_kernel": [c_int],
     "qsgw_get_precision": [c_ip, c_ip],
     "qsgw_last_error": [ctypes.c_char_p, c_int],
     "qsgw_profile": [c_int],
@@ -237,6 +238,11 @@ def synchronize():
 
 def set_precision(mode, nslices=2):
     _chk(load().qsgw_set_precision(mode, nslices))
+
+
+def set_sigc_kernel(pair):
+    """Split-precision Sigma_c kernel: False = one CTA per tile (default), True = CTA pairs."""
+    _chk(load().qsgw_set_sigc_kernel(1 if pair else 0))
 
 
 def get_precision():

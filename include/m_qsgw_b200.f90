@@ -26,6 +26,10 @@ module m_qsgw_b200
       import :: c_int
       integer(c_int), value :: mode, nslices
     end function
+    integer(c_int) function qsgw_set_sigc_kernel(pair) bind(C, name='qsgw_set_sigc_kernel')
+      import :: c_int
+      integer(c_int), value :: pair
+    end function
     integer(c_int) function qsgw_last_error(buf, len) bind(C, name='qsgw_last_error')
       import :: c_int, c_char
       character(kind=c_char) :: buf(*)

@@ -56,6 +56,11 @@ int qsgw_synchronize(void);
  * (m_kind.f90:3-11).  nslices: FP16 slices per operand for SPLIT_F16 (2). */
 int qsgw_set_precision(int mode, int nslices);
 int qsgw_get_precision(int *mode, int *nslices);
+/* Kernel of the split-precision Sigma_c contraction: 0 = one CTA per
+ * output tile (the default), 1 = CTA pairs (tcgen05 cta_group::2, M = 256
+ * over two SMs, each loading half of the B tile).  Both compute the same
+ * sums; the environment variable QSGW_SIGC_PAIR=1 sets 1 at load time. */
+int qsgw_set_sigc_kernel(int pair);
 /* Copies the last error message (NUL-terminated, truncated to len). */
 int qsgw_last_error(char *buf, int len);
 /* Number of kernels this library has launched since qsgw_init. */

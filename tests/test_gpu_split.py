@@ -72,3 +72,50 @@ def test_sigc_split_vs_oracle(split, keepwv):
     print(f"sigc split keepwv={keepwv}: rel err {err:.2e}, max QP shift {dqp:.3e} meV")
     assert err < TOL
     assert dqp < 1.0          # QP energies within 1 meV of the FP64 oracle
+
+
+def _sigc_problem(ngb, ntq, nm, niw, nreal, seed):
+    """A Sigma_c task with several 64-row tiles of the product basis (the
+    golden case has one), random W on the imaginary and real axes."""
+    rng = np.random.default_rng(seed)
+    t = synth.sigc_task(ngb, ntq, nm, niw, nreal, seed=seed, nctot=2, esmr=0.02, ef=0.05)
+    wi = np.asfortranarray(rng.standard_normal((ngb, ngb, niw + 1))
+                           + 1j * rng.standard_normal((ngb, ngb, niw + 1))) * 0.1
+    wr = np.asfortranarray(rng.standard_normal((ngb, ngb, nreal)) + 1j * rng.standard_normal((ngb, ngb, nreal))) * 0.1
+    zz = np.asfortranarray(rng.standard_normal((ngb, nm + 2, ntq)) + 1j * rng.standard_normal((ngb, nm + 2, ntq)))
+    return dict(t=t, wi=wi, wr=wr, z=zz, ngb=ngb, ntq=ntq, nm=nm + 2)
+
+
+@pytest.mark.parametrize("ngb", [150, 256])
+def test_sigc_split_kernels_multi_tile(split, ngb):
+    """Both split Sigma_c kernels (CTA pairs over two row tiles, one CTA per
+    tile) against the oracle; 150 rows = 3 row tiles, so one pair has a
+    padding tile."""
+    s = _sigc_problem(ngb, 8, 60, 6, 12, seed=ngb)
+    t = s['t']
+    nwxi, nwx, ntmax = sigc_window(t, s['ntq'])
+    ns2r = min(s['nm'], ntmax)
+    ref = np.zeros((s['ntq'], s['ntq']), complex, order='F')
+    sxcf.correlation_block(ref, s['z'], 1, s['nm'], ns2r, nwxi, nwx, s['ntq'], s['wi'], s['wr'], t['omega'],
+                           t['ekc'], t['nctot'], t['ef'], t['esmr'], 1.0 / 64, t['ua'], t['x'], t['wx'], t['expa'],
+                           t['freq_r'])
+    outs = {}
+    try:
+        for pair in (True, False):
+            split.set_sigc_kernel(pair)
+            got = np.zeros((s['ntq'], s['ntq']), complex, order='F')
+            split.sxcf_correlation(got, s['z'], 1, s['nm'], ns2r, nwxi, nwx, s['ntq'], s['wi'], s['wr'],
+                                   t['omega'], t['ekc'], t['nctot'], t['ef'], t['esmr'], 1.0 / 64, t['ua'], t['x'],
+                                   t['wx'], t['expa'], t['freq_r'])
+            outs[pair] = got
+    finally:
+        split.set_sigc_kernel(False)
+    for pair, got in outs.items():
+        err = rel_fro(got, ref)
+        dqp = np.max(np.abs(np.real(np.diag(got) - np.diag(ref)))) * HARTREE_MEV
+        print(f"sigc split ngb={ngb} pair={pair}: rel err {err:.2e}, max QP shift {dqp:.3e} meV")
+        assert err < TOL
+        assert dqp < 1.0
+    d = rel_fro(outs[True], outs[False])
+    print(f"pair vs single CTA: rel difference {d:.2e}")
+    assert d < 1e-6
