@@ -12,6 +12,7 @@
 #include "zgemm_f64.cuh"
 #include "autotune.cuh"
 #include "split_f16.cuh"
+#include "hoststage.cuh"
 
 namespace qsgw {
 
@@ -468,7 +469,8 @@ extern "C" int qsgw_chi0_lorentz_real_d(double* chi0_d, int npr, int nw, const d
   return QSGW_OK;
 }
 
-static qsgw::DevBuf g_lzh_z, g_lzh_c;
+static qsgw::DevBuf g_lzh_c;
+static qsgw::HostRing g_lzh_ring(2);    // zcols of the host-pointer calls
 
 extern "C" int qsgw_chi0_lorentz(double* chi0, int npr, int niw, const double* freq_i, int nk,
                                  const int* nocc, const int* nun, const double* eocc,
@@ -483,13 +485,18 @@ extern "C" int qsgw_chi0_lorentz(double* chi0, int npr, int niw, const double* f
   cudaStream_t s = ctx().stream;
   const size_t zb = static_cast<size_t>(ldz) * ncol * 16;
   const size_t cb = static_cast<size_t>(npr) * npr * niw * 16;
-  rc = g_lzh_z.ensure(zb); if (rc) return rc;
-  rc = g_lzh_c.ensure(cb); if (rc) return rc;
-  QSGW_CUDA(cudaMemcpyAsync(g_lzh_z.p, zcols, zb, cudaMemcpyHostToDevice, s));
+  HostSlot* sl = nullptr;
+  cudaStream_t cs = nullptr;
+  rc = g_lzh_ring.begin(&sl, &cs); if (rc) return rc;
+  DevBuf& dz = sl->buf[0];
+  rc = dz.ensure(zb); if (rc) return rc;
+  rc = g_lzh_c.ensure(cb); if (rc) return rc;   // one output image, reused in stream order
+  QSGW_CUDA(cudaMemcpyAsync(dz.p, zcols, zb, cudaMemcpyHostToDevice, cs));
+  rc = g_lzh_ring.ready(*sl, cs);
+  if (rc) return rc;
   rc = qsgw_chi0_lorentz_d(g_lzh_c.as<double>(), npr, niw, freq_i, nk, nocc, nun, eocc, eunocc,
-                           g_lzh_z.as<double>(), ldz);
+                           dz.as<double>(), ldz);
   if (rc) return rc;
   QSGW_CUDA(cudaMemcpyAsync(chi0, g_lzh_c.p, cb, cudaMemcpyDeviceToHost, s));
-  QSGW_CUDA(cudaStreamSynchronize(s));
-  return QSGW_OK;
+  return g_lzh_ring.finish(*sl);
 }

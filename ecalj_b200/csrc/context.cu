@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <atomic>
 #include "common.cuh"
+#include "hoststage.cuh"
 
 namespace qsgw {
 
@@ -51,7 +52,10 @@ int DevBuf::ensure(size_t n) {
 
 int h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (bytes == 0) return QSGW_OK;
-  if (!g_ctx.capturing) return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "H2D table");
+  if (!g_ctx.capturing) {
+    if (host_async()) return async_table_h2d(dst, src, bytes, s);
+    return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "H2D table");
+  }
   void* pin = nullptr;
   int rc = check_cuda(cudaHostAlloc(&pin, bytes, cudaHostAllocDefault), "cudaHostAlloc(graph table)");
   if (rc) return rc;
@@ -170,6 +174,7 @@ extern "C" int qsgw_finalize(void) {
   }
   cudaDeviceSynchronize();
   graph_free();
+  host_stage_release();
   if (c.d_flags) cudaFree(c.d_flags);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
   c = Context();
@@ -202,6 +207,8 @@ extern "C" int qsgw_synchronize(void) {
   if (rc) return rc;
   Context& c = ctx();
   QSGW_CUDA(cudaStreamSynchronize(c.stream));
+  rc = host_stage_sync();
+  if (rc) return rc;
   int flag = 0;
   QSGW_CUDA(cudaMemcpy(&flag, c.d_flags, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {

@@ -17,6 +17,7 @@
 #include <vector>
 #include "zgemm_f64.cuh"
 #include "split_f16.cuh"
+#include "hoststage.cuh"
 
 namespace qsgw {
 
@@ -200,7 +201,10 @@ static int pole_table_h(const qsgw_sxcf_args& a, std::vector<PoleEntry>& out) {
 }
 
 static DevBuf g_sc_wg, g_sc_w3, g_sc_cz, g_sc_wi, g_sc_wr, g_sc_tabs, g_sc_recs, g_sc_tmp;
-static DevBuf g_sc_host_z, g_sc_host_wi, g_sc_host_wr, g_sc_host_zs;
+static DevBuf g_sc_host_zs;
+// zmel, W(i omega), W(omega) records of the host-pointer calls: twelve slots (about 0.6 GB each
+// at ngb = 600), so the inputs of the next tasks keep the copy engine busy through a long kernel
+static HostRing g_sc_ring(12);
 
 static int grid_for(long long n) {
   return static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 16LL * ctx().sm_count)));
@@ -431,12 +435,16 @@ extern "C" int qsgw_sxcf_correlation(const qsgw_sxcf_args* args) {
                                : static_cast<size_t>(a.nblochpmx) * a.nblochpmx * 16;
   const size_t wib = wrec * (a.niw + 1), wrb = wrec * (a.nw + 1);
   const size_t sb = static_cast<size_t>(a.ntq) * a.ntq * 16;
-  rc = g_sc_host_z.ensure(zb); if (rc) return rc;
-  rc = g_sc_host_wi.ensure(wib); if (rc) return rc;
-  rc = g_sc_host_wr.ensure(wrb); if (rc) return rc;
-  rc = g_sc_host_zs.ensure(sb); if (rc) return rc;
-  if (zb) QSGW_CUDA(cudaMemcpyAsync(g_sc_host_z.p, a.zmel, zb, cudaMemcpyHostToDevice, s));
-  QSGW_CUDA(cudaMemcpyAsync(g_sc_host_wi.p, a.wc_imag, wib, cudaMemcpyHostToDevice, s));
+  HostSlot* sl = nullptr;
+  cudaStream_t cs = nullptr;
+  rc = g_sc_ring.begin(&sl, &cs); if (rc) return rc;
+  DevBuf &dz = sl->buf[0], &dwi = sl->buf[1], &dwr = sl->buf[2];
+  rc = dz.ensure(zb); if (rc) return rc;
+  rc = dwi.ensure(wib); if (rc) return rc;
+  rc = dwr.ensure(wrb); if (rc) return rc;
+  // inputs on the copy stream (the asynchronous mode overlaps them with the previous call)
+  if (zb) QSGW_CUDA(cudaMemcpyAsync(dz.p, a.zmel, zb, cudaMemcpyHostToDevice, cs));
+  QSGW_CUDA(cudaMemcpyAsync(dwi.p, a.wc_imag, wib, cudaMemcpyHostToDevice, cs));
   // only the real-axis records the pole part reads travel (as the reference
   // reads __WVR records by index, m_sxcf_gemm.f90:570)
   {
@@ -453,20 +461,31 @@ extern "C" int qsgw_sxcf_correlation(const qsgw_sxcf_args* args) {
       }
     for (int b = 0; b <= a.nw; ++b)
       if (need[b])
-        QSGW_CUDA(cudaMemcpyAsync(g_sc_host_wr.as<char>() + b * wrec, reinterpret_cast<const char*>(a.wc_real) + b * wrec,
-                                  wrec, cudaMemcpyHostToDevice, s));
+        QSGW_CUDA(cudaMemcpyAsync(dwr.as<char>() + b * wrec, reinterpret_cast<const char*>(a.wc_real) + b * wrec,
+                                  wrec, cudaMemcpyHostToDevice, cs));
   }
-  QSGW_CUDA(cudaMemcpyAsync(g_sc_host_zs.p, a.zsec, sb, cudaMemcpyHostToDevice, s));
+  rc = g_sc_ring.ready(*sl, cs);
+  if (rc) return rc;
+  // zsec accumulates: synchronous calls copy it in and out; asynchronous calls accumulate into
+  // one device image per host array until qsgw_synchronize
+  void* zs_dev = nullptr;
+  if (host_async()) {
+    rc = host_acc_target(a.zsec, sb, s, &zs_dev);
+    if (rc) return rc;
+  } else {
+    rc = g_sc_host_zs.ensure(sb); if (rc) return rc;
+    zs_dev = g_sc_host_zs.p;
+    QSGW_CUDA(cudaMemcpyAsync(zs_dev, a.zsec, sb, cudaMemcpyHostToDevice, s));
+  }
   qsgw_sxcf_args d = a;
-  d.zmel = g_sc_host_z.as<double>();
-  d.wc_imag = g_sc_host_wi.as<double>();
-  d.wc_real = g_sc_host_wr.as<double>();
-  d.zsec = g_sc_host_zs.as<double>();
+  d.zmel = dz.as<double>();
+  d.wc_imag = dwi.as<double>();
+  d.wc_real = dwr.as<double>();
+  d.zsec = static_cast<double*>(zs_dev);
   rc = sxcf_device(d);
   if (rc) return rc;
-  QSGW_CUDA(cudaMemcpyAsync(a.zsec, g_sc_host_zs.p, sb, cudaMemcpyDeviceToHost, s));
-  QSGW_CUDA(cudaStreamSynchronize(s));
-  return QSGW_OK;
+  QSGW_CUDA(cudaMemcpyAsync(a.zsec, zs_dev, sb, cudaMemcpyDeviceToHost, s));
+  return g_sc_ring.finish(*sl);
 }
 
 extern "C" int qsgw_sxcf_wgtim_d(double* wgtim_d, int niw, int ns1, int ns2, int ntqxx, int nctot,

@@ -71,6 +71,7 @@ _SIGS = {
     "qsgw_synchronize": [],
     "qsgw_set_precision": [c_int, c_int],
     "qsgw_set_sigc_kernel": [c_int],
+    "qsgw_set_host_async": [c_int],
     "qsgw_get_precision": [c_ip, c_ip],
     "qsgw_last_error": [ctypes.c_char_p, c_int],
     "qsgw_profile": [c_int],
@@ -238,6 +239,12 @@ def synchronize():
 
 def set_precision(mode, nslices=2):
     _chk(load().qsgw_set_precision(mode, nslices))
+
+
+def set_host_async(on):
+    """Host-pointer calls return once enqueued (True) or with their outputs written (False, default);
+    in the asynchronous mode outputs are valid after synchronize()."""
+    _chk(load().qsgw_set_host_async(1 if on else 0))
 
 
 def set_sigc_kernel(pair):

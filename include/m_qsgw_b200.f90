@@ -26,6 +26,10 @@ module m_qsgw_b200
       import :: c_int
       integer(c_int), value :: mode, nslices
     end function
+    integer(c_int) function qsgw_set_host_async(on) bind(C, name='qsgw_set_host_async')
+      import :: c_int
+      integer(c_int), value :: on
+    end function
     integer(c_int) function qsgw_set_sigc_kernel(pair) bind(C, name='qsgw_set_sigc_kernel')
       import :: c_int
       integer(c_int), value :: pair

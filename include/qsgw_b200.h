@@ -52,6 +52,15 @@ int qsgw_finalize(void);
 /* Launch stream for every later call (a cudaStream_t; 0 = library stream). */
 int qsgw_set_stream(void *stream);
 int qsgw_synchronize(void);
+/* Host-pointer calls (qsgw_chi0_lorentz, qsgw_sxcf_correlation) copy their
+ * inputs on a copy stream into one of two device slots.  on = 0 (default):
+ * each call returns with its outputs written, like the reference's Fortran
+ * calls.  on = 1: each call returns once its copies and kernels are enqueued,
+ * so the copy of one call overlaps the computation of the previous one; the
+ * host outputs are valid, and the host inputs may be changed, only after
+ * qsgw_synchronize().  zsec arrays accumulated by several calls are kept on
+ * the device between synchronisations (one image per host array). */
+int qsgw_set_host_async(int on);
 /* Runtime precision switch; the reference's is the compile-time -D__MP
  * (m_kind.f90:3-11).  nslices: FP16 slices per operand for SPLIT_F16 (2). */
 int qsgw_set_precision(int mode, int nslices);
