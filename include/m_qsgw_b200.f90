@@ -69,6 +69,15 @@ module m_qsgw_b200
       real(c_double), intent(in) :: freq_i(*), eocc(*), eunocc(*)
       integer(c_int), intent(in) :: nocc(*), nun(*)
     end function
+    ! the same with host chi0 and zcols (c_loc of the Fortran arrays)
+    integer(c_int) function qsgw_chi0_lorentz(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, &
+         zcols, ldz) bind(C, name='qsgw_chi0_lorentz')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: chi0, zcols
+      integer(c_int), value :: npr, niw, nk, ldz
+      real(c_double), intent(in) :: freq_i(*), eocc(*), eunocc(*)
+      integer(c_int), intent(in) :: nocc(*), nun(*)
+    end function
     integer(c_int) function qsgw_wvi_llw_d(zxqi, ngb, niw, nspin, vcousq, m2e, is_x0_m_basis, &
          is_wc_m_basis, iq, zw, nblochpmx) bind(C, name='qsgw_wvi_llw_d')
       import :: c_int, c_double, c_ptr
@@ -77,6 +86,11 @@ module m_qsgw_b200
       real(c_double), intent(in) :: vcousq(*)
     end function
     integer(c_int) function qsgw_sxcf_correlation_d(args) bind(C, name='qsgw_sxcf_correlation_d')
+      import :: c_int, qsgw_sxcf_args
+      type(qsgw_sxcf_args), intent(in) :: args
+    end function
+    ! the same with host arrays in args (zmel, wc_imag, wc_real, zsec): copies in and out
+    integer(c_int) function qsgw_sxcf_correlation(args) bind(C, name='qsgw_sxcf_correlation')
       import :: c_int, qsgw_sxcf_args
       type(qsgw_sxcf_args), intent(in) :: args
     end function
