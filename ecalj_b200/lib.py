@@ -72,6 +72,7 @@ _SIGS = {
     "qsgw_set_precision": [c_int, c_int],
     "qsgw_set_sigc_kernel": [c_int],
     "qsgw_set_host_async": [c_int],
+    "qsgw_dpsion_chiq_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_vp, c_vp],
     "qsgw_get_precision": [c_ip, c_ip],
     "qsgw_last_error": [ctypes.c_char_p, c_int],
     "qsgw_profile": [c_int],
@@ -341,6 +342,25 @@ def chi0_lorentz_d(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, zcols, l
     f = load().qsgw_chi0_lorentz if host else load().qsgw_chi0_lorentz_d
     _chk(f(_p(chi0), npr, niw, _p(fi), nk, _p(no), _p(nu), _p(eo), _p(eu), _p(zcols), ldz or npr))
     return chi0
+
+
+def dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, freq_i, freq_r=None, ecut=1e10, zxqi=None, zxq=None):
+    """Hilbert transform of the chi0 histogram (dpsion5.f90:77-137, 215-292), npm = 1.
+    rcxq, zxqi, zxq: device complex128 tensors (zxqi, zxq allocated when None).
+    Returns (zxqi, zxq); zxq is None without freq_r."""
+    import torch
+    fh, fi = _f64(frhis), _f64(freq_i)
+    niw = len(fi)
+    nw = -1 if freq_r is None else len(freq_r) - 1
+    fr = _f64(freq_r) if freq_r is not None else np.zeros(1)
+    M = npr * npr_col
+    if zxqi is None and niw > 0:
+        zxqi = torch.empty(M * niw, dtype=torch.complex128, device=rcxq.device)
+    if zxq is None and nw >= 0:
+        zxq = torch.empty(M * (nw + 1), dtype=torch.complex128, device=rcxq.device)
+    _chk(load().qsgw_dpsion_chiq_d(_p(rcxq), npr, npr_col, nwhis, _p(fh), niw, _p(fi), nw, _p(fr), ecut,
+                                   _p(zxqi) if zxqi is not None else None, _p(zxq) if zxq is not None else None))
+    return zxqi, zxq
 
 
 # ---------------------------------------------------------------- W

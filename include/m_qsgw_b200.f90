@@ -69,6 +69,15 @@ module m_qsgw_b200
       real(c_double), intent(in) :: freq_i(*), eocc(*), eunocc(*)
       integer(c_int), intent(in) :: nocc(*), nun(*)
     end function
+    ! Hilbert transform of the chi0 histogram (dpsion_init + dpsion_chiq, npm = 1)
+    integer(c_int) function qsgw_dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, niw, freq_i, nw, freq_r, &
+         ecut, zxqi, zxq) bind(C, name='qsgw_dpsion_chiq_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: rcxq, zxqi, zxq
+      integer(c_int), value :: npr, npr_col, nwhis, niw, nw
+      real(c_double), intent(in) :: frhis(*), freq_i(*), freq_r(*)
+      real(c_double), value :: ecut
+    end function
     ! the same with host chi0 and zcols (c_loc of the Fortran arrays)
     integer(c_int) function qsgw_chi0_lorentz(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, &
          zcols, ldz) bind(C, name='qsgw_chi0_lorentz')

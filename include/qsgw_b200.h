@@ -117,6 +117,20 @@ int qsgw_zminv_hpd_batched_d(double *a, int n, int lda, int nbatch);
 int qsgw_zminv_hpd_batched_noalloc_d(double *a, int n, int lda, int nbatch,
                                      void *stream);
 
+/* ---- Hilbert transform of the chi0 histogram: drop-in for dpsion_init +
+ * dpsion_chiq (dpsion5.f90:77-137, 215-292; hilbertmat.f90:14-79), time
+ * reversal (npm = 1), no chi+- and no SmearX0 filter.
+ * rcxq (device, npr*npr_col x (nwhis+1) complex, slots 0..nwhis as x0gemm
+ * leaves them), frhis (host, nwhis+1 increasing bin edges, Hartree), freq_i
+ * (host, niw), freq_r (host, nw+1, freq_r[0] = 0; nw = -1 skips the real
+ * axis), ecut (>= 1e9: no Gaussian cut).  zxqi (device, npr*npr_col x niw)
+ * = chi0(i freq_i), zxq (device, npr*npr_col x (nw+1)) = chi0(freq_r): the
+ * reference leaves the latter in rcxq(:, :, 0:nw); rcxq is not modified here. */
+int qsgw_dpsion_chiq_d(const double *rcxq, int npr, int npr_col, int nwhis,
+                       const double *frhis, int niw, const double *freq_i,
+                       int nw, const double *freq_r, double ecut,
+                       double *zxqi, double *zxq);
+
 /* ---- chi0 rank-k accumulation: drop-in for x0gemm (x0gemm.f90:2-97) ----
  * rcxq(npr, npr_col, (1-npm)*nwhis : nwhis) += sum over pairs of
  *   conj(zmel(:,it,itp)) * whw * zmel(ipr_col-1+:, it, itp)^T
