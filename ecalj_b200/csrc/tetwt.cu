@@ -251,3 +251,52 @@ extern "C" int qsgw_tetwt_hist_d(double* w_d, int nk, int nocc, int nunocc, int 
   QSGW_LAUNCH_CHECK("tetwt_hist_kernel");
   return QSGW_OK;
 }
+
+// Pair/bin lists of x0gemm from the dense weights (host logic): the index
+// accumulation of X0kf_v4hz_init (x0kf_v4h.f90:48-142) for npm = 1, no core
+// states, no cRPA.  For every k (k-major, then occupied ib, then jb) the pair
+// gets one entry when any of its bins has a nonzero weight: the contiguous bin
+// range from its first to its last nonzero bin, with the weights of that range
+// appended to whwc.  job 0 counts, job 1 fills (arrays of the counted sizes).
+extern "C" int qsgw_x0_lists(const double* w, int nk, int nocc, int nunocc, int nwhis, int job, int* ncoun,
+                             int* ncount, int* itc, int* itpc, int* jpmc, int* iwini, int* iwend, int* icouini,
+                             double* whwc, int* icounkmin, int* icounkmax) {
+  QSGW_ARG(w && ncoun && ncount && nk >= 1 && nocc >= 0 && nunocc >= 0 && nwhis >= 1 && (job == 0 || job == 1),
+           "x0_lists: nk=%d nocc=%d nunocc=%d nwhis=%d job=%d", nk, nocc, nunocc, nwhis, job);
+  const int cap_coun = *ncoun, cap_count = *ncount;
+  QSGW_ARG(job == 0 || (itc && itpc && jpmc && iwini && iwend && icouini && whwc && icounkmin && icounkmax),
+           "x0_lists: job 1 needs every output array");
+  long long icoun = 0, icount = 0;
+  for (int k = 0; k < nk; ++k) {
+    if (job == 1) icounkmin[k] = static_cast<int>(icoun + 1);
+    for (int ib = 0; ib < nocc; ++ib)
+      for (int jb = 0; jb < nunocc; ++jb) {
+        const double* wp = w + static_cast<size_t>(nwhis) * (jb + static_cast<size_t>(nunocc) * (ib + static_cast<size_t>(nocc) * k));
+        int first = -1, last = -1;
+        for (int h = 0; h < nwhis; ++h)
+          if (wp[h] != 0.0) {
+            if (first < 0) first = h;
+            last = h;
+          }
+        if (first < 0) continue;
+        if (job == 1) {
+          QSGW_ARG(icoun < cap_coun && icount + (last - first + 1) <= cap_count,
+                   "x0_lists: the job 1 arrays are smaller than job 0 counted");
+          itc[icoun] = ib + 1;
+          itpc[icoun] = jb + 1;
+          jpmc[icoun] = 1;
+          iwini[icoun] = first + 1;
+          iwend[icoun] = last + 1;
+          icouini[icoun] = static_cast<int>(icount + 1);
+          for (int h = first; h <= last; ++h) whwc[icount + (h - first)] = wp[h];
+        }
+        ++icoun;
+        icount += last - first + 1;
+      }
+    if (job == 1) icounkmax[k] = static_cast<int>(icoun);
+  }
+  QSGW_ARG(icount <= 2147483647LL, "x0_lists: %lld weights exceed the int range", icount);
+  *ncoun = static_cast<int>(icoun);
+  *ncount = static_cast<int>(icount);
+  return QSGW_OK;
+}

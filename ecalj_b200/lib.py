@@ -72,6 +72,8 @@ _SIGS = {
     "qsgw_set_precision": [c_int, c_int],
     "qsgw_set_sigc_kernel": [c_int],
     "qsgw_set_host_async": [c_int],
+    "qsgw_x0_lists": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                      c_vp, c_vp, c_vp],
     "qsgw_dpsion_chiq_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_vp, c_vp],
     "qsgw_get_precision": [c_ip, c_ip],
     "qsgw_last_error": [ctypes.c_char_p, c_int],
@@ -542,6 +544,26 @@ def zminv_batched_d(a, n, lda, nbatch):
 
 
 # ---------------------------------------------------------------- tetrahedron weights
+def x0_lists(w):
+    """x0gemm pair/bin lists from dense histogram weights w (nk, nocc, nunocc, nwhis), numpy, the
+    layout of tetwt_hist_d's output (x0kf_v4h.f90:48-142, npm = 1).  Returns a dict of the 1-based
+    tables itc, itpc, jpmc, iwini, iwend, icouini, whwc, icounkmin, icounkmax (host, no GPU needed)."""
+    w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+    nk, nocc, nunocc, nwhis = w.shape
+    nc, nt = ctypes.c_int(0), ctypes.c_int(0)
+    f = load().qsgw_x0_lists
+    _chk(f(_p(w), nk, nocc, nunocc, nwhis, 0, ctypes.byref(nc), ctypes.byref(nt), *([None] * 9)))
+    t = {k: np.zeros(max(nc.value, 1), np.int32) for k in ("itc", "itpc", "jpmc", "iwini", "iwend", "icouini")}
+    t["whwc"] = np.zeros(max(nt.value, 1))
+    t["icounkmin"] = np.zeros(nk, np.int32)
+    t["icounkmax"] = np.zeros(nk, np.int32)
+    _chk(f(_p(w), nk, nocc, nunocc, nwhis, 1, ctypes.byref(nc), ctypes.byref(nt), _p(t["itc"]), _p(t["itpc"]),
+           _p(t["jpmc"]), _p(t["iwini"]), _p(t["iwend"]), _p(t["icouini"]), _p(t["whwc"]), _p(t["icounkmin"]),
+           _p(t["icounkmax"])))
+    t["ncoun"], t["ncount"] = nc.value, nt.value
+    return t
+
+
 def tetwt_hist_d(w, idtet, qbzw, ek, ekq, efermi, frhis, nocc, nunocc):
     """w (device, nwhis x nunocc x nocc x nk, accumulated) += tetrahedron
     histogram weights; idtet (ntet, 4) 0-based, qbzw (nk, 3), ek/ekq (nk, nband).

@@ -69,6 +69,17 @@ module m_qsgw_b200
       real(c_double), intent(in) :: freq_i(*), eocc(*), eunocc(*)
       integer(c_int), intent(in) :: nocc(*), nun(*)
     end function
+    ! x0gemm pair/bin lists from dense tetrahedron weights (host arrays, no GPU needed)
+    integer(c_int) function qsgw_x0_lists(w, nk, nocc, nunocc, nwhis, job, ncoun, ncount, itc, itpc, jpmc, &
+         iwini, iwend, icouini, whwc, icounkmin, icounkmax) bind(C, name='qsgw_x0_lists')
+      import :: c_int, c_double
+      real(c_double), intent(in) :: w(*)
+      integer(c_int), value :: nk, nocc, nunocc, nwhis, job
+      integer(c_int), intent(inout) :: ncoun, ncount
+      integer(c_int), intent(out) :: itc(*), itpc(*), jpmc(*), iwini(*), iwend(*), icouini(*)
+      integer(c_int), intent(out) :: icounkmin(*), icounkmax(*)
+      real(c_double), intent(out) :: whwc(*)
+    end function
     ! Hilbert transform of the chi0 histogram (dpsion_init + dpsion_chiq, npm = 1)
     integer(c_int) function qsgw_dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, niw, freq_i, nw, freq_r, &
          ecut, zxqi, zxq) bind(C, name='qsgw_dpsion_chiq_d')

@@ -394,6 +394,19 @@ int qsgw_tetwt_hist_d(double *w_d, int nk, int nocc, int nunocc, int nwhis,
                       const int *idtet, int ntet, const double *qbzw,
                       const double *ek, const double *ekq, int nband,
                       double efermi, const double *frhis, double *voltot);
+/* Pair/bin lists of qsgw_x0gemm from those weights copied to the host
+ * (w: nwhis x nunocc x nocc x nk): the index accumulation of X0kf_v4hz_init
+ * (x0kf_v4h.f90:48-142), npm = 1, no core states, no cRPA.  A pair with any
+ * nonzero bin gets one entry (k-major, then ib, then jb): itc = ib+1, itpc =
+ * jb+1, jpmc = 1, the bin range [iwini, iwend] from its first to its last
+ * nonzero bin, icouini = 1-based start of its weights in whwc; icounkmin/max
+ * (nk each) = the entries of each k, 1-based.  job 0 sets *ncoun, *ncount;
+ * job 1 fills arrays of those sizes (*ncoun, *ncount = their capacities).
+ * Host-only: needs no GPU and no qsgw_init.                                */
+int qsgw_x0_lists(const double *w, int nk, int nocc, int nunocc, int nwhis,
+                  int job, int *ncoun, int *ncount, int *itc, int *itpc,
+                  int *jpmc, int *iwini, int *iwend, int *icouini,
+                  double *whwc, int *icounkmin, int *icounkmax);
 
 /* ---- W record files __WVI.<iq> / __WVR.<iq> in the reference's layout:
  * fixed records without markers, record rec at byte (rec-1)*recl, one
