@@ -1,6 +1,7 @@
 // A C++ caller of libqsgw_b200 written the way a Fortran or C host would use it:
 // plain pointers to column-major complex(8) arrays, status codes, no torch.
-//   cabi_caller          checks that calls before qsgw_init fail cleanly (no GPU needed)
+//   cabi_caller          checks that calls before qsgw_init fail cleanly and builds x0gemm
+//                        pair/bin lists with the host-only qsgw_x0_lists (no GPU needed)
 //   cabi_caller gpu      also multiplies Fortran-layout matrices with qsgw_zmm (host
 //                        pointers, op(A) = A^H) and compares with a plain triple loop
 #include <cmath>
@@ -27,6 +28,29 @@ int main(int argc, char** argv) {
   char msg[256];
   qsgw_last_error(msg, sizeof(msg));
   if (std::strstr(msg, "qsgw_init") == nullptr) return fail("error text");
+  {
+    // host-only: x0gemm pair/bin lists from dense tetrahedron weights w(ihis, jb, ib, k)
+    const int nk = 2, nocc = 2, nunocc = 2, nwhis = 4;
+    std::vector<double> w(static_cast<size_t>(nwhis) * nunocc * nocc * nk, 0.0);
+    auto W = [&](int h, int jb, int ib, int k) -> double& { return w[h + nwhis * (jb + nunocc * (ib + nocc * k))]; };
+    W(1, 0, 1, 0) = 0.5;                      // k = 1: pair (it = 2, itp = 1), bins 2..4 with a hole at 3
+    W(3, 0, 1, 0) = 0.25;
+    W(0, 1, 0, 1) = 1.0;                      // k = 2: pair (it = 1, itp = 2), bin 1
+    int ncoun = 0, ncount = 0;
+    if (qsgw_x0_lists(w.data(), nk, nocc, nunocc, nwhis, 0, &ncoun, &ncount, nullptr, nullptr, nullptr, nullptr,
+                      nullptr, nullptr, nullptr, nullptr, nullptr) != QSGW_OK || ncoun != 2 || ncount != 4)
+      return fail("qsgw_x0_lists job 0");
+    std::vector<int> itc(ncoun), itpc(ncoun), jpmc(ncoun), iwini(ncoun), iwend(ncoun), icouini(ncoun), kmin(nk), kmax(nk);
+    std::vector<double> whwc(ncount);
+    if (qsgw_x0_lists(w.data(), nk, nocc, nunocc, nwhis, 1, &ncoun, &ncount, itc.data(), itpc.data(), jpmc.data(),
+                      iwini.data(), iwend.data(), icouini.data(), whwc.data(), kmin.data(), kmax.data()) != QSGW_OK)
+      return fail("qsgw_x0_lists job 1");
+    const bool ok = itc[0] == 2 && itpc[0] == 1 && iwini[0] == 2 && iwend[0] == 4 && icouini[0] == 1 &&
+                    itc[1] == 1 && itpc[1] == 2 && iwini[1] == 1 && iwend[1] == 1 && icouini[1] == 4 &&
+                    jpmc[0] == 1 && jpmc[1] == 1 && whwc[0] == 0.5 && whwc[1] == 0.0 && whwc[2] == 0.25 &&
+                    whwc[3] == 1.0 && kmin[0] == 1 && kmax[0] == 1 && kmin[1] == 2 && kmax[1] == 2;
+    if (!ok) return fail("qsgw_x0_lists tables");
+  }
   if (argc < 2 || std::strcmp(argv[1], "gpu") != 0) {
     std::printf("OK cpu\n");
     return 0;
