@@ -315,7 +315,7 @@ int sxcf_device(const qsgw_sxcf_args& a) {
   for (long long c = 0; c < ncol; ++c) order[c] = static_cast<int>(c);
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
   const bool split = ctx().prec_mode == QSGW_PREC_SPLIT_F16;
-  const int tilew = split ? 128 : ZG_BN;       // column tile of the split / FP64 kernel
+  const int tilew = split ? sigc_split_tile_width() : ZG_BN;   // column tile of the split / FP64 kernel
   std::vector<ZSeg> segs;
   std::vector<int> gseg_off, gnseg, tile_group, tile_cols, seg_slot;
   int gidx = 0;

@@ -99,6 +99,7 @@ struct Params {
   long long ldc, c_bs;
   const double* scales;     // [0] sigma_A, [1] sigma_S, [2 + j] sigma_B(j)
   int* err;
+  double* scratch;          // Sigma_c on 256-column tiles: FP64 sums, 256 x 128 per CTA
 };
 
 // ------------------------------------------------------------------ PTX helpers
@@ -553,6 +554,212 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   }
 }
 
+// ------------------------------------------------------------------ Sigma_c on 256-column tiles
+// The Sigma_c contraction with N = 256 MMAs (64 complex rows x 256 columns per
+// CTA): twice the work per instruction, four 48 KB stages of 32-element K
+// chunks (64-byte swizzled rows).  Measured on B200 (8 tasks of 600 x 600 at
+// 1965 MHz): 35.4 ms against 31.0 ms for the 64 x 128 kernel (37.3 ms with two
+// 96 KB stages of 64-element chunks), although a bare stream of N = 256 MMAs
+// does twice the work of the N = 128 stream in 1.36 times the time; so it is
+// the opt-in variant.  The two FP32
+// accumulators (one per segment, alternating) fill TMEM's 512 columns, so the
+// FP64 sums over segments live in a per-CTA scratch tile in global memory
+// (L2-resident while the CTA runs, [column][TMEM lane], coalesced per warp):
+// the drain warps add weight x period sum into it in FP64 (the same fma order
+// as the TMEM sums of the 128-column kernel) and the epilogue adds the tile
+// into the output.
+constexpr int NW = 256;                          // complex columns per tile (UMMA N)
+constexpr int KCW = 32;                          // FP16 elements per K chunk (64-byte swizzled rows)
+constexpr int WIDE_NST = 4;                      // four 48 KB stages
+constexpr int SLICE_AW = BM2 * KCW * 2;          // 8 KB: one A' slice of a stage
+constexpr int SLICE_SW = NW * KCW * 2;           // 16 KB: one S slice of a stage
+struct WideCfg {
+  static constexpr int OFF_A = 0;
+  static constexpr int OFF_S = OFF_A + WIDE_NST * 2 * SLICE_AW;
+  static constexpr int OFF_W = OFF_S + WIDE_NST * 2 * SLICE_SW;      // drain weights, 16 warps x 64 doubles
+  static constexpr int OFF_BAR = OFF_W + 2 * NDRAIN_WARPS * 64 * 8;
+  static constexpr int NBAR = 2 * WIDE_NST + 2 + 2 + 1;
+  static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
+  static constexpr int SMEM_BYTES = OFF_MISC + 64 + 1024;
+  static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
+};
+// kind::f16, A = B = F16, D = F32, both K-major, M = 128, N = 256
+constexpr uint32_t IDESC_W = (1u << 4) | (static_cast<uint32_t>(NW >> 3) << 17) | (static_cast<uint32_t>(BM2 >> 4) << 24);
+
+// K-major, 64-byte swizzle: rows of 64 B in 8-row atoms (SBO = 512 B), layout type SWIZZLE_64B
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
+  d |= static_cast<uint64_t>(1) << 16;
+  d |= static_cast<uint64_t>(512 >> 4) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(4) << 61;
+  return d;
+}
+__device__ __forceinline__ void umma_f16_w(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC_W), "r"(accumulate));
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+    sigc_wide_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapS,
+                     const Params p) {
+  using L = WideCfg;
+  constexpr int NST = WIDE_NST;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* sA = sm + L::OFF_A;
+  unsigned char* sS = sm + L::OFF_S;
+  unsigned char* sW = sm + L::OFF_W;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::OFF_BAR);
+  uint64_t* full = bar;                  // [NST] TMA -> MMA
+  uint64_t* empty = bar + NST;           // [NST] MMA -> TMA
+  uint64_t* accfull = bar + 2 * NST;     // [2] MMA -> drain
+  uint64_t* accempty = accfull + 2;      // [2] drain -> MMA
+  uint64_t* done = accempty + 2;         // [1] every MMA of the CTA retired
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::OFF_MISC);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::OFF_MISC + 8);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int mt = blockIdx.x % p.ntm, nt = blockIdx.x / p.ntm;
+  const int group = p.tile_group[nt];
+  const int nseg = p.group_nseg[group];
+  const int seg0 = p.group_seg_off[group];
+  const int nchunk = nseg * p.cps;
+  double* scr = p.scratch + static_cast<size_t>(blockIdx.x) * NW * BM2;   // [column][TMEM lane]
+
+  if (tid == 0) {
+    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], 2 * NDRAIN_WARPS); }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (nchunk > 0) {
+    if (warp == 0 && lane == 0) {
+      // ---------------- TMA producer: A' (hi, lo) of the segment's slot, S (hi, lo) of the tile
+      constexpr uint32_t bytes = 2 * SLICE_AW + 2 * SLICE_SW;
+      int issued = 0, sg = 0, cin = 0, st = 0, ph = 0;
+      int t = p.seg_slot[seg0] * p.tiles_per_slot + mt;
+      for (int c = 0; c < nchunk; ++c) {
+        if (c >= NST && !mbar_wait(&empty[st], ph ^ 1, abort_flag)) break;
+        issued = c + 1;
+        mbar_expect_tx(&full[st], bytes);
+        unsigned char* a = sA + st * 2 * SLICE_AW;
+        unsigned char* s = sS + st * 2 * SLICE_SW;
+        const int x = cin * KCW;
+        tma_load_4d(a, &mapA, &full[st], x, 0, 0, t);
+        tma_load_4d(a + SLICE_AW, &mapA, &full[st], x, 0, 0, p.lo_tile_off + t);
+        tma_load_2d(s, &mapS, &full[st], x, nt * NW);
+        tma_load_2d(s + SLICE_SW, &mapS, &full[st], x, p.lo_row_off + nt * NW);
+        if (++cin == p.cps) {
+          cin = 0;
+          if (++sg < nseg) t = p.seg_slot[seg0 + sg] * p.tiles_per_slot + mt;
+        }
+        if (++st == NST) { st = 0; ph ^= 1; }
+      }
+      for (int c = max(0, issued - NST); c < issued; ++c) mbar_drain(&full[c % NST], (c / NST) & 1);
+    } else if (warp == 1 && lane == 0) {
+      // ---------------- MMA issuer: one accumulator per segment, alternating
+      int seg = 0, cin = 0, st = 0, ph = 0;
+      for (int c = 0; c < nchunk && !*abort_flag; ++c) {
+        const int ab = seg & 1;
+        const bool first = cin == 0, last = cin == p.cps - 1;
+        if (first && seg >= 2 && !mbar_wait(&accempty[ab], ((seg >> 1) - 1) & 1, abort_flag)) break;
+        if (!mbar_wait(&full[st], ph, abort_flag)) break;
+        tc_fence_after();
+        const uint32_t a_hi = smem_u32(sA + st * 2 * SLICE_AW), a_lo = a_hi + SLICE_AW;
+        const uint32_t b_hi = smem_u32(sS + st * 2 * SLICE_SW), b_lo = b_hi + SLICE_SW;
+        const uint32_t d = tmem + static_cast<uint32_t>(ab * NW);
+#pragma unroll
+        for (int kk = 0; kk < KCW / 16; ++kk) {
+          const uint32_t ko = kk * 32;
+          umma_f16_w(d, sw64_desc(a_hi + ko), sw64_desc(b_hi + ko), (first && kk == 0) ? 0u : 1u);
+          umma_f16_w(d, sw64_desc(a_hi + ko), sw64_desc(b_lo + ko), 1u);
+          umma_f16_w(d, sw64_desc(a_lo + ko), sw64_desc(b_hi + ko), 1u);
+        }
+        umma_commit(&empty[st]);
+        if (last) umma_commit(&accfull[ab]);
+        if (++st == NST) { st = 0; ph ^= 1; }
+        if (++cin == p.cps) { cin = 0; ++seg; }
+      }
+      umma_commit(done);
+      mbar_drain(done, 0);
+    } else if (warp >= CONV_W0) {
+      // ---------------- drain (warps 2..17): TMEM lanes 32 (warp mod 4) .. +31, 64 columns a warp
+      const int dw = warp - CONV_W0;
+      const int quad = warp & 3;
+      const int c_lo = (dw >> 2) * 64;
+      const int row = quad * 32 + lane;                   // accumulator row: 0..63 re, 64..127 im
+      const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
+      double* wsm = reinterpret_cast<double*>(sW + dw * 64 * sizeof(double));
+      bool ok = true;
+      for (int seg = 0; seg < nseg; ++seg) {
+        const int ab = seg & 1;
+        const ZSeg zs = p.segs[seg0 + seg];
+        __syncwarp();                                     // the previous segment's reads of wsm are done
+        for (int j = lane; j < 64; j += 32) {
+          const int col = p.tile_cols[nt * NW + c_lo + j];
+          wsm[j] = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] : 0.0;
+        }
+        __syncwarp();
+        if (!mbar_wait_warp(&accfull[ab], (seg >> 1) & 1, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+#pragma unroll 1
+        for (int cb = 0; cb < 64; cb += 32) {
+          uint32_t fa[16], fb[16];
+          tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NW + c_lo + cb), fa);
+          tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NW + c_lo + cb + 16), fb);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            const double v = static_cast<double>(__uint_as_float(i < 16 ? fa[i] : fb[i - 16]));
+            double* q = scr + static_cast<size_t>(c_lo + cb + i) * BM2 + row;
+            *q = (seg == 0) ? v * wsm[cb + i] : fma(v, wsm[cb + i], *q);
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&accempty[ab]);
+      }
+      if (ok && !*abort_flag) {
+        const int m = mt * BMC + (row & 63);
+        const bool im_part = row >= 64;
+        const double inv = 1.0 / (p.scales[0] * p.scales[1]);
+        if (m < p.M) {
+#pragma unroll 4
+          for (int j = 0; j < 64; ++j) {
+            const long long col = p.tile_cols[nt * NW + c_lo + j];
+            if (col < 0) continue;
+            const double v = scr[static_cast<size_t>(c_lo + j) * BM2 + row] * inv;
+            atomicAdd(reinterpret_cast<double*>(p.C + m + col * p.ldc) + (im_part ? 1 : 0), v);
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  if (*abort_flag && tid == 0) atomicExch(p.err, 2);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
 // ------------------------------------------------------------------ Sigma_c on CTA pairs
 // The same Sigma_c contraction on pairs of SMs (a cluster of two CTAs) with
 // tcgen05.mma.cta_group::2: one MMA of M = 256 real rows (two 64-complex-row
@@ -980,7 +1187,7 @@ static EncodeTiledFn encode_fn() {
 }
 
 static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides_bytes,
-                    const cuuint32_t* box) {
+                    const cuuint32_t* box, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled is not available from the driver");
@@ -992,7 +1199,7 @@ static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* di
   }
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, rank, base, dims, strides_bytes, box, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (%d)", static_cast<int>(r));
@@ -1043,15 +1250,35 @@ static int launch_pair(const CUtensorMap& ma, const CUtensorMap& ms, const Param
   return QSGW_OK;
 }
 
-// Sigma_c kernel choice: one CTA per tile (default, the faster on B200) or CTA pairs;
-// QSGW_SIGC_PAIR=1 selects the pairs at load time
-static int g_sigc_pair = -1;
-static bool sigc_pair() {
-  if (g_sigc_pair < 0) {
-    const char* e = std::getenv("QSGW_SIGC_PAIR");
-    g_sigc_pair = (e && e[0] == '1') ? 1 : 0;
+// Sigma_c kernel: 0 = one CTA per 64 x 128 tile (default, the fastest on B200), 1 = CTA pairs
+// over 128-column tiles, 2 = one CTA per 64 x 256 tile; QSGW_SIGC_KERNEL=<n> sets it at load time
+static int g_sigc_kind = -1;
+static int sigc_kind() {
+  if (g_sigc_kind < 0) {
+    const char* e = std::getenv("QSGW_SIGC_KERNEL");
+    g_sigc_kind = (e && (e[0] == '1' || e[0] == '2') && e[1] == '\0') ? e[0] - '0' : 0;
   }
-  return g_sigc_pair == 1;
+  return g_sigc_kind;
+}
+
+static DevBuf g_scr;                      // FP64 sums of the 256-column kernel
+
+static int launch_wide(const CUtensorMap& ma, const CUtensorMap& ms, Params p, dim3 grid, cudaStream_t s,
+                       const char* tag) {
+  static bool attr = false;
+  if (!attr) {
+    QSGW_CUDA(cudaFuncSetAttribute(sigc_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WideCfg::SMEM_BYTES));
+    attr = true;
+  }
+  int rc = g_scr.ensure(static_cast<size_t>(grid.x) * NW * BM2 * sizeof(double));
+  if (rc) return rc;
+  p.scratch = g_scr.as<double>();
+  const int pi = prof_begin(tag, s);
+  sigc_wide_kernel<<<grid, NTHREADS, WideCfg::SMEM_BYTES, s>>>(ma, ms, p);
+  prof_end(pi, s);
+  count_launch();
+  QSGW_LAUNCH_CHECK("sigc_wide_kernel");
+  return QSGW_OK;
 }
 
 static int launch_split(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s,
@@ -1177,7 +1404,11 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   const long long Kp = ((2LL * ngb + KC - 1) / KC) * KC;
   const int nslot = a.nimag + a.nreal;
   const int ntiles = static_cast<int>(a.tile_group.size());
-  const long long nrows = static_cast<long long>(ntiles) * NC;
+  const int kind = sigc_kind();
+  const int tw = (kind == 2) ? NW : NC;                   // columns per tile (as the tables were cut)
+  QSGW_ARG(a.tile_cols.size() == static_cast<size_t>(ntiles) * tw, "sigc split: %zu tile columns for %d tiles of %d",
+           a.tile_cols.size(), ntiles, tw);
+  const long long nrows = static_cast<long long>(ntiles) * tw;
   const long long slice_a = static_cast<long long>(nslot) * T * 128 * Kp;
   const long long slice_s = nrows * Kp;
   int rc = g_a.ensure(2 * slice_a * sizeof(__half));
@@ -1249,20 +1480,23 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   const cuuint64_t dima[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(2LL * nslot * T)};
   const cuuint64_t stra[3] = {static_cast<cuuint64_t>(Kp * 2), static_cast<cuuint64_t>(Kp * 2 * 64),
                               static_cast<cuuint64_t>(Kp * 2 * 128)};
-  const cuuint32_t boxa[4] = {KC, 64, 2, 1};
-  rc = make_map(&ma, A, 4, dima, stra, boxa);
+  // 64 x 256 tiles: 32-element K chunks in 64-byte swizzled rows; the others: 64 in 128-byte rows
+  const int kch = (kind == 2) ? KCW : KC;
+  const CUtensorMapSwizzle swz = (kind == 2) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+  const cuuint32_t boxa[4] = {static_cast<cuuint32_t>(kch), 64, 2, 1};
+  rc = make_map(&ma, A, 4, dima, stra, boxa, swz);
   if (rc) return rc;
   const cuuint64_t dims_[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(2 * nrows)};
   const cuuint64_t strs[1] = {static_cast<cuuint64_t>(Kp * 2)};
-  const bool pair = sigc_pair();
-  const cuuint32_t boxs[2] = {KC, static_cast<cuuint32_t>(pair ? NC / 2 : NC)};   // a pair CTA loads half of the S tile
-  rc = make_map(&ms, S, 2, dims_, strs, boxs);
+  // a CTA loads its whole S tile; a pair CTA half of it
+  const cuuint32_t boxs[2] = {static_cast<cuuint32_t>(kch), static_cast<cuuint32_t>(kind == 1 ? NC / 2 : tw)};
+  rc = make_map(&ms, S, 2, dims_, strs, boxs, swz);
   if (rc) return rc;
   Params p{};
   p.mode = MODE_SEG;
   p.M = ngb; p.N = 0;
   p.ntm = T; p.ntn = ntiles;
-  p.cps = static_cast<int>(Kp / KC);
+  p.cps = static_cast<int>(Kp / kch);
   p.kch_total = 0; p.kch_per_split = 0;
   p.tile_group = d_tg; p.tile_cols = d_cols; p.group_seg_off = d_gso; p.group_nseg = d_gns;
   p.seg_slot = d_slot; p.segs = d_segs;
@@ -1273,18 +1507,21 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   p.scales = g_sc.as<double>();
   p.err = ctx().d_flags + 1;
   QSGW_CUDA(cudaMemsetAsync(a.out, 0, static_cast<size_t>(ngb) * a.ncol * sizeof(double2), s));
-  if (pair) return launch_pair(ma, ms, p, dim3(static_cast<unsigned>(2 * ((T + 1) / 2) * ntiles), 1, 1), s, "sigc_seg_tc");
+  if (kind == 1) return launch_pair(ma, ms, p, dim3(static_cast<unsigned>(2 * ((T + 1) / 2) * ntiles), 1, 1), s, "sigc_seg_tc");
   dim3 grid(static_cast<unsigned>(T * ntiles), 1, 1);
+  if (kind == 2) return launch_wide(ma, ms, p, grid, s, "sigc_seg_tc");
   return launch_split(ma, ms, p, grid, s, "sigc_seg_tc");
 }
 
+int sigc_split_tile_width() { return sigc_kind() == 2 ? NW : NC; }
+
 }  // namespace qsgw
 
-extern "C" int qsgw_set_sigc_kernel(int pair) {
-  if (pair != 0 && pair != 1) {
-    qsgw::set_error("qsgw_set_sigc_kernel: %d (0 = one CTA per tile, 1 = CTA pairs)", pair);
+extern "C" int qsgw_set_sigc_kernel(int kind) {
+  if (kind < 0 || kind > 2) {
+    qsgw::set_error("qsgw_set_sigc_kernel: %d (0 = 64 x 128 tiles, 1 = CTA pairs, 2 = 64 x 256 tiles)", kind);
     return QSGW_ERR_ARG;
   }
-  qsgw::tc::g_sigc_pair = pair;
+  qsgw::tc::g_sigc_kind = kind;
   return QSGW_OK;
 }

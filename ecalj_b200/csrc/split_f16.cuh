@@ -21,10 +21,12 @@ struct SigcSplitArgs {
   const double2* zmel; long long ncol; // zmel columns (ngb each)
   const double* wgt; long long nwgt;   // every imaginary weight (for the scale)
   const double* w3; long long nw3;     // every pole weight
-  std::vector<int> tile_cols, tile_group, group_seg_off, group_nseg, seg_slot;  // 128-column tiles
+  std::vector<int> tile_cols, tile_group, group_seg_off, group_nseg, seg_slot;  // sigc_split_tile_width() columns
   std::vector<ZSeg> segs;
   double2* out;                        // (ngb, ncol), overwritten
 };
 int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s);
+// columns per tile of the selected split Sigma_c kernel (the tables are cut to it)
+int sigc_split_tile_width();
 
 }  // namespace qsgw

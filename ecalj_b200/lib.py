@@ -250,9 +250,13 @@ def set_host_async(on):
     _chk(load().qsgw_set_host_async(1 if on else 0))
 
 
-def set_sigc_kernel(pair):
-    """Split-precision Sigma_c kernel: False = one CTA per tile (default), True = CTA pairs."""
-    _chk(load().qsgw_set_sigc_kernel(1 if pair else 0))
+SIGC_NARROW, SIGC_PAIR, SIGC_WIDE = 0, 1, 2
+
+
+def set_sigc_kernel(kind):
+    """Split-precision Sigma_c kernel: SIGC_NARROW (one CTA per 64 x 128 tile, default),
+    SIGC_PAIR (CTA pairs over 128-column tiles), SIGC_WIDE (one CTA per 64 x 256 tile)."""
+    _chk(load().qsgw_set_sigc_kernel(int(kind)))
 
 
 def get_precision():

@@ -30,9 +30,9 @@ module m_qsgw_b200
       import :: c_int
       integer(c_int), value :: on
     end function
-    integer(c_int) function qsgw_set_sigc_kernel(pair) bind(C, name='qsgw_set_sigc_kernel')
+    integer(c_int) function qsgw_set_sigc_kernel(kind) bind(C, name='qsgw_set_sigc_kernel')
       import :: c_int
-      integer(c_int), value :: pair
+      integer(c_int), value :: kind
     end function
     integer(c_int) function qsgw_last_error(buf, len) bind(C, name='qsgw_last_error')
       import :: c_int, c_char

@@ -88,9 +88,9 @@ def _sigc_problem(ngb, ntq, nm, niw, nreal, seed):
 
 @pytest.mark.parametrize("ngb", [150, 256])
 def test_sigc_split_kernels_multi_tile(split, ngb):
-    """Both split Sigma_c kernels (CTA pairs over two row tiles, one CTA per
-    tile) against the oracle; 150 rows = 3 row tiles, so one pair has a
-    padding tile."""
+    """The three split Sigma_c kernels (64 x 256 tiles, CTA pairs over two
+    row tiles of 128 columns, 64 x 128 tiles) against the oracle and each
+    other; 150 rows = 3 row tiles, so one pair has a padding tile."""
     s = _sigc_problem(ngb, 8, 60, 6, 12, seed=ngb)
     t = s['t']
     nwxi, nwx, ntmax = sigc_window(t, s['ntq'])
@@ -101,21 +101,22 @@ def test_sigc_split_kernels_multi_tile(split, ngb):
                            t['freq_r'])
     outs = {}
     try:
-        for pair in (True, False):
-            split.set_sigc_kernel(pair)
+        for kind in (split.SIGC_WIDE, split.SIGC_PAIR, split.SIGC_NARROW):
+            split.set_sigc_kernel(kind)
             got = np.zeros((s['ntq'], s['ntq']), complex, order='F')
             split.sxcf_correlation(got, s['z'], 1, s['nm'], ns2r, nwxi, nwx, s['ntq'], s['wi'], s['wr'],
                                    t['omega'], t['ekc'], t['nctot'], t['ef'], t['esmr'], 1.0 / 64, t['ua'], t['x'],
                                    t['wx'], t['expa'], t['freq_r'])
-            outs[pair] = got
+            outs[kind] = got
     finally:
-        split.set_sigc_kernel(False)
-    for pair, got in outs.items():
+        split.set_sigc_kernel(split.SIGC_NARROW)
+    for kind, got in outs.items():
         err = rel_fro(got, ref)
         dqp = np.max(np.abs(np.real(np.diag(got) - np.diag(ref)))) * HARTREE_MEV
-        print(f"sigc split ngb={ngb} pair={pair}: rel err {err:.2e}, max QP shift {dqp:.3e} meV")
+        print(f"sigc split ngb={ngb} kernel={kind}: rel err {err:.2e}, max QP shift {dqp:.3e} meV")
         assert err < TOL
         assert dqp < 1.0
-    d = rel_fro(outs[True], outs[False])
-    print(f"pair vs single CTA: rel difference {d:.2e}")
-    assert d < 1e-6
+    for kind in (split.SIGC_PAIR, split.SIGC_WIDE):
+        d = rel_fro(outs[kind], outs[split.SIGC_NARROW])
+        print(f"kernel {kind} vs 64 x 128 tiles: rel difference {d:.2e}")
+        assert d < 1e-6
