@@ -99,18 +99,27 @@ __global__ void unpack_upper_kernel(double2* __restrict__ w, const double2* __re
 }
 
 // (W + W^H)/2 of selected records (:573)
+// out[q](i, j) = (W_recs[q](i, j) + conj(W_recs[q](j, i))) / 2: block (32, 8) per 32 x 32 tile
+// (grid x, y) of record q (grid z); the transposed tile goes through shared memory so both
+// reads are coalesced
 __global__ void hermitize_kernel(double2* __restrict__ out, const double2* __restrict__ in,
                                  const int* __restrict__ recs, int n, long long ld, int nrec) {
-  const long long tot = static_cast<long long>(n) * n * nrec;
-  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int i = static_cast<int>(e % n);
-    const long long r = e / n;
-    const int j = static_cast<int>(r % n);
-    const int q = static_cast<int>(r / n);
-    const double2* W = in + static_cast<long long>(recs[q]) * ld * ld;
-    const double2 a = W[i + j * ld], b = W[j + i * ld];
-    out[static_cast<long long>(q) * ld * ld + i + j * ld] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+  __shared__ double2 tile[32][33];
+  const int q = blockIdx.z;
+  const double2* W = in + static_cast<long long>(recs[q]) * ld * ld;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int b = threadIdx.y; b < 32; b += 8) {          // tile[x][b] = W(j0 + x, i0 + b)
+    const int jj = j0 + threadIdx.x, ii = i0 + b;
+    if (jj < n && ii < n) tile[threadIdx.x][b] = W[jj + static_cast<long long>(ii) * ld];
+  }
+  __syncthreads();
+  for (int b = threadIdx.y; b < 32; b += 8) {
+    const int i = i0 + threadIdx.x, j = j0 + b;
+    if (i < n && j < n) {
+      const double2 a = W[i + static_cast<long long>(j) * ld], t = tile[b][threadIdx.x];   // t = W(j, i)
+      out[static_cast<long long>(q) * ld * ld + i + static_cast<long long>(j) * ld] =
+          make_double2(0.5 * (a.x + t.x), 0.5 * (a.y - t.y));
+    }
   }
 }
 
@@ -289,7 +298,7 @@ int sxcf_device(const qsgw_sxcf_args& a) {
       }
     } else {
       if ((rc = h2d(g_sc_recs.p, recs.data(), nrec * sizeof(int), s))) return rc;
-      hermitize_kernel<<<grid_for(static_cast<long long>(ngb) * ngb * nrec), 256, 0, s>>>(
+      hermitize_kernel<<<dim3((ngb + 31) / 32, (ngb + 31) / 32, nrec), dim3(32, 8), 0, s>>>(
           g_sc_wr.as<double2>(), wr_src, g_sc_recs.as<int>(), ngb, ldw, nrec);
       count_launch();
       QSGW_LAUNCH_CHECK("hermitize_kernel");

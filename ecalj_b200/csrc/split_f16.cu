@@ -1064,18 +1064,33 @@ __device__ __forceinline__ void split2(double x, double sig, __half& hi, __half&
 }
 
 // max |re|, |im| over a strided complex set -> atomicMax on the bit pattern
+// max |Re|, |Im| over a (rows x cols, column stride ld): columns by block (x), a column's rows by
+// thread, split over blockIdx.y when there are few columns; one atomic per block (256 threads)
 __global__ void absmax_c128_kernel(const double2* __restrict__ a, long long rows, long long cols, long long ld,
                                    unsigned long long* out) {
+  __shared__ double red[8];
   double m = 0.0;
-  const long long tot = rows * cols;
-  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long r = e % rows, c = e / rows;
-    const double2 v = a[r + c * ld];
-    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  const long long rchunk = (rows + gridDim.y - 1) / gridDim.y;
+  const long long r0 = blockIdx.y * rchunk, r1 = min(rows, r0 + rchunk);
+  for (long long c = blockIdx.x; c < cols; c += gridDim.x) {
+    const double2* col = a + c * ld;
+    for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const double2 v = col[r];
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
   }
   for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __double_as_longlong(m));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; ++w) m = fmax(m, red[w]);
+    atomicMax(out, __double_as_longlong(m));
+  }
+}
+static dim3 absmax_grid(long long rows, long long cols, int sms) {
+  const long long gx = std::max<long long>(1, std::min<long long>(cols, 8LL * sms));
+  const long long gy = std::max<long long>(1, std::min<long long>((rows + 1023) / 1024, (8LL * sms + gx - 1) / gx));
+  return dim3(static_cast<unsigned>(gx), static_cast<unsigned>(std::min<long long>(gy, 65535)), 1);
 }
 __global__ void absmax_f64_rows_kernel(const double* __restrict__ a, long long n, long long stride, int nrow,
                                        unsigned long long* out) {
@@ -1102,20 +1117,24 @@ __global__ void make_scales_kernel(const unsigned long long* mx, double* scales,
 // A' of the M-doubled real GEMM from a complex getter, into
 // [slice][slot*T + t][half][64][Kp] FP16 (slice 0 = hi, 1 = lo).
 // getter 0 (chi0): a(m, k) = conj(Z[m + k*ld]);  getter 1 (Sigma_c): a(m, k) = conj(W_slot[k + m*ld]).
+// Block (32, 8); the tile (slot, t) runs over blockIdx.y (grid-stride), (mm, k) over the block
+// and blockIdx.x: getter 0 puts mm on threadIdx.x (Z columns are contiguous in m), getter 1 puts
+// k on threadIdx.x (W rows are contiguous in k), so the loads coalesce.
 template <int GET>
 __global__ void presplit_a_kernel(__half* __restrict__ out, const double2* __restrict__ src, long long ld,
                                   long long slot_stride, int M, long long K, int T, int nslot, long long Kp,
                                   const double* __restrict__ scales, long long slice_elems, int slot_out0 = 0) {
   const double sig = scales[0];
-  const long long per_slot = static_cast<long long>(T) * 64 * (Kp / 2);
-  const long long tot = per_slot * nslot;      // one thread per (slot, t, mm, k)
-  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
-    long long r = e;
-    const long long k = r % (Kp / 2); r /= (Kp / 2);
-    const int mm = static_cast<int>(r % 64); r /= 64;
-    const int t = static_cast<int>(r % T);
-    const int slot = static_cast<int>(r / T);
+  const long long KH = Kp / 2;
+  for (long long st = blockIdx.y; st < static_cast<long long>(nslot) * T; st += gridDim.y) {
+  const int t = static_cast<int>(st % T);
+  const int slot = static_cast<int>(st / T);
+  for (int it = 0; it < (GET == 0 ? 2 : 8); ++it) {
+    int mm;
+    long long k;
+    if (GET == 0) { mm = threadIdx.x + 32 * it; k = blockIdx.x * 8LL + threadIdx.y; }
+    else { mm = threadIdx.y + 8 * it; k = blockIdx.x * 32LL + threadIdx.x; }
+    if (k >= KH) continue;
     const int m = t * 64 + mm;
     double ar = 0.0, ai = 0.0;
     if (m < M && k < K) {
@@ -1126,13 +1145,24 @@ __global__ void presplit_a_kernel(__half* __restrict__ out, const double2* __res
     }
     const long long row0 = ((static_cast<long long>(slot + slot_out0) * T + t) * 2 + 0) * 64 + mm;
     const long long row1 = row0 + 64;
-    __half h, l;
-    // half 0: [Re a, -Im a]; half 1: [Im a, Re a]
-    split2(ar, sig, h, l); out[row0 * Kp + 2 * k] = h; out[slice_elems + row0 * Kp + 2 * k] = l;
-    split2(-ai, sig, h, l); out[row0 * Kp + 2 * k + 1] = h; out[slice_elems + row0 * Kp + 2 * k + 1] = l;
-    split2(ai, sig, h, l); out[row1 * Kp + 2 * k] = h; out[slice_elems + row1 * Kp + 2 * k] = l;
-    split2(ar, sig, h, l); out[row1 * Kp + 2 * k + 1] = h; out[slice_elems + row1 * Kp + 2 * k + 1] = l;
+    // half 0: [Re a, -Im a]; half 1: [Im a, Re a]; each pair is one 4-byte store per slice
+    __half h0, l0, h1, l1;
+    split2(ar, sig, h0, l0);
+    split2(-ai, sig, h1, l1);
+    *reinterpret_cast<__half2*>(out + row0 * Kp + 2 * k) = __halves2half2(h0, h1);
+    *reinterpret_cast<__half2*>(out + slice_elems + row0 * Kp + 2 * k) = __halves2half2(l0, l1);
+    split2(ai, sig, h0, l0);
+    split2(ar, sig, h1, l1);
+    *reinterpret_cast<__half2*>(out + row1 * Kp + 2 * k) = __halves2half2(h0, h1);
+    *reinterpret_cast<__half2*>(out + slice_elems + row1 * Kp + 2 * k) = __halves2half2(l0, l1);
   }
+  }
+}
+template <int GET>
+static dim3 presplit_a_grid(long long Kp, long long tiles) {
+  const long long KH = Kp / 2;
+  const long long gx = (GET == 0) ? (KH + 7) / 8 : (KH + 31) / 32;
+  return dim3(static_cast<unsigned>(gx), static_cast<unsigned>(std::min<long long>(tiles, 65535)), 1);
 }
 
 // B source rows (K-major): row r = column cols[r] of Z (k contiguous), [Re b, Im b] per k,
@@ -1140,20 +1170,23 @@ __global__ void presplit_a_kernel(__half* __restrict__ out, const double2* __res
 __global__ void presplit_s_kernel(__half* __restrict__ out, const double2* __restrict__ z, long long ld, long long K,
                                   const int* __restrict__ cols, long long nrows, long long ncols_valid, long long Kp,
                                   const double* __restrict__ scales, long long slice_elems) {
+  // block (32, 8): k on threadIdx.x (z columns are contiguous in k), rows over threadIdx.y and
+  // blockIdx.y (grid-stride)
   const double sig = scales[1];
-  const long long tot = nrows * (Kp / 2);
-  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < tot;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long k = e % (Kp / 2), r = e / (Kp / 2);
+  const long long k = blockIdx.x * 32LL + threadIdx.x;
+  if (k >= Kp / 2) return;
+  for (long long r = blockIdx.y * 8LL + threadIdx.y; r < nrows; r += 8LL * gridDim.y) {
     const long long c = cols ? cols[r] : (r < ncols_valid ? r : -1);
     double br = 0.0, bi = 0.0;
     if (c >= 0 && k < K) {
       const double2 v = z[k + c * ld];
       br = v.x; bi = v.y;
     }
-    __half h, l;
-    split2(br, sig, h, l); out[r * Kp + 2 * k] = h; out[slice_elems + r * Kp + 2 * k] = l;
-    split2(bi, sig, h, l); out[r * Kp + 2 * k + 1] = h; out[slice_elems + r * Kp + 2 * k + 1] = l;
+    __half h0, l0, h1, l1;
+    split2(br, sig, h0, l0);
+    split2(bi, sig, h1, l1);
+    *reinterpret_cast<__half2*>(out + r * Kp + 2 * k) = __halves2half2(h0, h1);
+    *reinterpret_cast<__half2*>(out + slice_elems + r * Kp + 2 * k) = __halves2half2(l0, l1);
   }
 }
 
@@ -1316,7 +1349,7 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   if (rc) return rc;
   unsigned long long* mx = g_mx.as<unsigned long long>();
   QSGW_CUDA(cudaMemsetAsync(mx, 0, (2 + niw) * sizeof(unsigned long long), s));
-  absmax_c128_kernel<<<grid1(static_cast<long long>(npr) * npair), 256, 0, s>>>(zcols, npr, npair, ldz, mx);
+  absmax_c128_kernel<<<absmax_grid(npr, npair, ctx().sm_count), 256, 0, s>>>(zcols, npr, npair, ldz, mx);
   count_launch();
   QSGW_LAUNCH_CHECK("absmax_c128_kernel");
   QSGW_CUDA(cudaMemcpyAsync(mx + 1, mx, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s));
@@ -1336,7 +1369,7 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   QSGW_LAUNCH_CHECK("scale_weights_kernel");
   __half* a = g_a.as<__half>();
   QSGW_CUDA(cudaMemsetAsync(a, 0, 2 * slice_elems * sizeof(__half), s));
-  presplit_a_kernel<0><<<grid1(static_cast<long long>(T) * 64 * (Kp / 2)), 256, 0, s>>>(
+  presplit_a_kernel<0><<<presplit_a_grid<0>(Kp, T), dim3(32, 8), 0, s>>>(
       a, zcols, ldz, 0, npr, npair, T, 1, Kp, g_sc.as<double>(), slice_elems);
   count_launch();
   QSGW_LAUNCH_CHECK("presplit_a_kernel");
@@ -1422,15 +1455,15 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   unsigned long long* mx = g_mx.as<unsigned long long>();
   QSGW_CUDA(cudaMemsetAsync(mx, 0, 3 * sizeof(unsigned long long), s));
   // magnitudes: W stack (sigma_A), zmel (sigma_S), every weight (sigma_B)
-  absmax_c128_kernel<<<grid1(static_cast<long long>(ngb) * ngb * a.nimag), 256, 0, s>>>(
+  absmax_c128_kernel<<<absmax_grid(ngb, static_cast<long long>(ngb) * a.nimag, ctx().sm_count), 256, 0, s>>>(
       a.wi, ngb, static_cast<long long>(ngb) * a.nimag, a.ldw, mx);
   count_launch();
   if (a.nreal > 0) {
-    absmax_c128_kernel<<<grid1(static_cast<long long>(ngb) * ngb * a.nreal), 256, 0, s>>>(
+    absmax_c128_kernel<<<absmax_grid(ngb, static_cast<long long>(ngb) * a.nreal, ctx().sm_count), 256, 0, s>>>(
         a.wr, ngb, static_cast<long long>(ngb) * a.nreal, a.ldw, mx);
     count_launch();
   }
-  absmax_c128_kernel<<<grid1(static_cast<long long>(ngb) * a.ncol), 256, 0, s>>>(a.zmel, ngb, a.ncol, ngb, mx + 1);
+  absmax_c128_kernel<<<absmax_grid(ngb, a.ncol, ctx().sm_count), 256, 0, s>>>(a.zmel, ngb, a.ncol, ngb, mx + 1);
   count_launch();
   absmax_f64_rows_kernel<<<dim3(64, 1), 256, 0, s>>>(a.wgt, a.nwgt, 0, 1, mx + 2);
   count_launch();
@@ -1443,11 +1476,11 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   QSGW_LAUNCH_CHECK("sigc split scales");
   // pre-split A' slots: imag W first, then the symmetrised real-axis records
   __half* A = g_a.as<__half>();
-  presplit_a_kernel<1><<<grid1(static_cast<long long>(a.nimag) * T * 64 * (Kp / 2)), 256, 0, s>>>(
+  presplit_a_kernel<1><<<presplit_a_grid<1>(Kp, static_cast<long long>(a.nimag) * T), dim3(32, 8), 0, s>>>(
       A, a.wi, a.ldw, a.ldw * a.ldw, ngb, ngb, T, a.nimag, Kp, g_sc.as<double>(), slice_a, 0);
   count_launch();
   if (a.nreal > 0) {
-    presplit_a_kernel<1><<<grid1(static_cast<long long>(a.nreal) * T * 64 * (Kp / 2)), 256, 0, s>>>(
+    presplit_a_kernel<1><<<presplit_a_grid<1>(Kp, static_cast<long long>(a.nreal) * T), dim3(32, 8), 0, s>>>(
         A, a.wr, a.ldw, a.ldw * a.ldw, ngb, ngb, T, a.nreal, Kp, g_sc.as<double>(), slice_a, a.nimag);
     count_launch();
   }
@@ -1472,7 +1505,9 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
   const int* d_slot = reinterpret_cast<const int*>(put(a.seg_slot.data(), a.seg_slot.size() * sizeof(int)));
   if (cprc) return cprc;
   __half* S = g_s.as<__half>();
-  presplit_s_kernel<<<grid1(nrows * (Kp / 2)), 256, 0, s>>>(S, a.zmel, ngb, ngb, d_cols, nrows, 0, Kp,
+  presplit_s_kernel<<<dim3(static_cast<unsigned>((Kp / 2 + 31) / 32),
+                          static_cast<unsigned>(std::min<long long>((nrows + 7) / 8, 65535))),
+                      dim3(32, 8), 0, s>>>(S, a.zmel, ngb, ngb, d_cols, nrows, 0, Kp,
                                                             g_sc.as<double>(), slice_s);
   count_launch();
   QSGW_LAUNCH_CHECK("sigc presplit");
