@@ -105,3 +105,22 @@ def test_chi0_and_sigc_async_interleaved(qsgw):
         assert _same(o, r)
     for zg, zr in zip(zgot, zref):
         assert _same(zg, zr)
+
+
+def test_async_with_pageable_arrays(qsgw):
+    """Plain numpy (pageable) host arrays in the asynchronous mode: the copies
+    stop overlapping, the results stay those of the synchronous calls."""
+    s = inputs()['sc']
+    ntq = s['ntq']
+    ref = np.zeros((ntq, ntq), complex, order='F')
+    for task in range(2):
+        _sigc_call(qsgw, ref, s, s['z'], s['wi'], s['wr'], 0.5 * (task + 1))
+    got = np.zeros((ntq, ntq), complex, order='F')
+    qsgw.set_host_async(True)
+    try:
+        for task in range(2):
+            _sigc_call(qsgw, got, s, s['z'], s['wi'], s['wr'], 0.5 * (task + 1))
+        qsgw.synchronize()
+    finally:
+        qsgw.set_host_async(False)
+    assert _same(got, ref)
