@@ -15,6 +15,7 @@
 //     zxqi = rcxq . B[:, imag],   zxq = rcxq . B[:, real].
 // rcxq is not modified (the reference leaves chi0(w_r) in rcxq(:, :, 0:nw);
 // here it goes to zxq).
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -59,6 +60,47 @@ void hilbertmat_h(cd z, int nwhis, const std::vector<double>& L, const std::vect
   }
 }
 
+// The transform matrix B (rows = rcxq slots 0..nwhis, columns = niw imaginary then nw+1 real
+// frequencies, column-major): imatt and rmatt of dpsion_init (dpsion5.f90:93-107, 123-128) with
+// the bin normalisation -wfac / (R - L) (:215-220) and the i rcxq(t) term (:255) folded in.
+void build_transform(int nwhis, const double* frhis, int niw, const double* freq_i, int nw, const double* freq_r,
+                     double ecut, std::vector<cd>& B) {
+  // bins -nwhis..nwhis (dpsion5.f90:87-89)
+  std::vector<double> L(2 * nwhis + 1), R(2 * nwhis + 1), C(2 * nwhis + 1);
+  for (int i = 1; i <= nwhis; ++i) {
+    L[nwhis + i] = frhis[i - 1];
+    R[nwhis + i] = frhis[i];
+    L[nwhis - i] = -frhis[i];
+    R[nwhis - i] = -frhis[i - 1];
+  }
+  L[nwhis] = R[nwhis] = 0.0;
+  for (int k = 0; k <= 2 * nwhis; ++k) C[k] = 0.5 * (L[k] + R[k]);
+  // bin normalisation (dpsion5.f90:215-220)
+  std::vector<double> fnorm(nwhis + 1, 1.0);
+  for (int i = 1; i <= nwhis; ++i) {
+    const double c = C[nwhis + i];
+    const double wfac = (ecut < 1e9) ? std::exp(-(c / ecut) * (c / ecut)) : 1.0;
+    fnorm[i] = -wfac / (R[nwhis + i] - L[nwhis + i]);
+  }
+  // B: rows = rcxq slots 0..nwhis, columns = niw imaginary then nw+1 real frequencies
+  const int K = nwhis + 1, ncol = niw + (nw + 1);
+  B.assign(static_cast<size_t>(K) * ncol, cd(0.0, 0.0));
+  std::vector<cd> rm;
+  const double pi = 3.14159265358979323846;
+  for (int j = 0; j < niw; ++j) {                  // imatt (dpsion5.f90:123-128)
+    hilbertmat_h(cd(0.0, freq_i[j]), nwhis, L, C, R, rm);
+    for (int i = 1; i <= nwhis; ++i)
+      B[static_cast<size_t>(j) * K + i] = fnorm[i] * (std::real(rm[nwhis + i] - rm[nwhis - i]) / pi);
+  }
+  for (int t = 0; t <= nw; ++t) {                  // rmatt (dpsion5.f90:93-107) and i rcxq(t) (:255)
+    hilbertmat_h(cd(freq_r[t], 0.0), nwhis, L, C, R, rm);
+    cd* col = B.data() + static_cast<size_t>(niw + t) * K;
+    for (int i = 1; i <= nwhis; ++i)
+      col[i] = fnorm[i] * (std::real(rm[nwhis + i]) / pi - std::real(rm[nwhis - i]) / pi);
+    col[t] += cd(0.0, fnorm[t]);                   // slot 0 is not normalised: fnorm[0] = 1
+  }
+}
+
 }  // namespace
 
 static DevBuf g_dp_b;
@@ -86,40 +128,9 @@ extern "C" int qsgw_dpsion_chiq_d(const double* rcxq, int npr, int npr_col, int 
   QSGW_ARG(M <= INT_MAX, "dpsion_chiq: npr*npr_col = %lld too large", M);
   QSGW_ARG(((reinterpret_cast<uintptr_t>(rcxq) | reinterpret_cast<uintptr_t>(zxqi) |
              reinterpret_cast<uintptr_t>(zxq)) & 15) == 0, "dpsion_chiq: complex arrays must be 16-byte aligned");
-  // bins -nwhis..nwhis (dpsion5.f90:87-89)
-  std::vector<double> L(2 * nwhis + 1), R(2 * nwhis + 1), C(2 * nwhis + 1);
-  for (int i = 1; i <= nwhis; ++i) {
-    L[nwhis + i] = frhis[i - 1];
-    R[nwhis + i] = frhis[i];
-    L[nwhis - i] = -frhis[i];
-    R[nwhis - i] = -frhis[i - 1];
-  }
-  L[nwhis] = R[nwhis] = 0.0;
-  for (int k = 0; k <= 2 * nwhis; ++k) C[k] = 0.5 * (L[k] + R[k]);
-  // bin normalisation (dpsion5.f90:215-220)
-  std::vector<double> fnorm(nwhis + 1, 1.0);
-  for (int i = 1; i <= nwhis; ++i) {
-    const double c = C[nwhis + i];
-    const double wfac = (ecut < 1e9) ? std::exp(-(c / ecut) * (c / ecut)) : 1.0;
-    fnorm[i] = -wfac / (R[nwhis + i] - L[nwhis + i]);
-  }
-  // B: rows = rcxq slots 0..nwhis, columns = niw imaginary then nw+1 real frequencies
-  const int K = nwhis + 1, ncol = niw + (nw + 1);
-  std::vector<cd> B(static_cast<size_t>(K) * ncol, cd(0.0, 0.0));
-  std::vector<cd> rm;
-  const double pi = 3.14159265358979323846;
-  for (int j = 0; j < niw; ++j) {                  // imatt (dpsion5.f90:123-128)
-    hilbertmat_h(cd(0.0, freq_i[j]), nwhis, L, C, R, rm);
-    for (int i = 1; i <= nwhis; ++i)
-      B[static_cast<size_t>(j) * K + i] = fnorm[i] * (std::real(rm[nwhis + i] - rm[nwhis - i]) / pi);
-  }
-  for (int t = 0; t <= nw; ++t) {                  // rmatt (dpsion5.f90:93-107) and i rcxq(t) (:255)
-    hilbertmat_h(cd(freq_r[t], 0.0), nwhis, L, C, R, rm);
-    cd* col = B.data() + static_cast<size_t>(niw + t) * K;
-    for (int i = 1; i <= nwhis; ++i)
-      col[i] = fnorm[i] * (std::real(rm[nwhis + i]) / pi - std::real(rm[nwhis - i]) / pi);
-    col[t] += cd(0.0, fnorm[t]);                   // slot 0 is not normalised: fnorm[0] = 1
-  }
+  std::vector<cd> B;
+  build_transform(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, B);
+  const int K = nwhis + 1;
   cudaStream_t s = ctx().stream;
   rc = g_dp_b.ensure(B.size() * sizeof(cd));
   if (rc) return rc;
@@ -137,5 +148,19 @@ extern "C" int qsgw_dpsion_chiq_d(const double* rcxq, int npr, int npr_col, int 
                    reinterpret_cast<double2*>(zxq), M, 0, 1, s);
     if (rc) return rc;
   }
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_dpsion_matrix(int nwhis, const double* frhis, int niw, const double* freq_i, int nw,
+                                  const double* freq_r, double ecut, double* b) {
+  QSGW_ARG(frhis && b && nwhis >= 1 && niw >= 0 && nw >= -1 && nw < nwhis,
+           "dpsion_matrix: nwhis=%d niw=%d nw=%d", nwhis, niw, nw);
+  QSGW_ARG(niw == 0 || freq_i, "dpsion_matrix: niw=%d needs freq_i", niw);
+  QSGW_ARG(nw < 0 || (freq_r && freq_r[0] == 0.0), "dpsion_matrix: freq_r must start at 0");
+  for (int i = 0; i < nwhis; ++i)
+    QSGW_ARG(frhis[i + 1] > frhis[i], "dpsion_matrix: frhis not increasing at bin %d", i + 1);
+  std::vector<cd> B;
+  build_transform(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, B);
+  std::copy(B.begin(), B.end(), reinterpret_cast<cd*>(b));
   return QSGW_OK;
 }

@@ -74,6 +74,7 @@ _SIGS = {
     "qsgw_set_host_async": [c_int],
     "qsgw_x0_lists": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                       c_vp, c_vp, c_vp],
+    "qsgw_dpsion_matrix": [c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_vp],
     "qsgw_dpsion_chiq_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_vp, c_vp],
     "qsgw_get_precision": [c_ip, c_ip],
     "qsgw_last_error": [ctypes.c_char_p, c_int],
@@ -348,6 +349,18 @@ def chi0_lorentz_d(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, zcols, l
     f = load().qsgw_chi0_lorentz if host else load().qsgw_chi0_lorentz_d
     _chk(f(_p(chi0), npr, niw, _p(fi), nk, _p(no), _p(nu), _p(eo), _p(eu), _p(zcols), ldz or npr))
     return chi0
+
+
+def dpsion_matrix(frhis, freq_i, freq_r=None, ecut=1e10):
+    """The Hilbert transform matrix of dpsion_chiq_d on the host (no GPU): complex
+    (nwhis+1, niw + nw + 1), chi0 = rcxq . b."""
+    fh, fi = _f64(frhis), _f64(freq_i)
+    nwhis, niw = len(fh) - 1, len(fi)
+    nw = -1 if freq_r is None else len(freq_r) - 1
+    fr = _f64(freq_r) if freq_r is not None else np.zeros(1)
+    b = np.zeros((nwhis + 1, niw + nw + 1), np.complex128, order='F')
+    _chk(load().qsgw_dpsion_matrix(nwhis, _p(fh), niw, _p(fi), nw, _p(fr), ecut, _p(b)))
+    return b
 
 
 def dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, freq_i, freq_r=None, ecut=1e10, zxqi=None, zxq=None):

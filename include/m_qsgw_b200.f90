@@ -89,6 +89,15 @@ module m_qsgw_b200
       real(c_double), intent(in) :: frhis(*), freq_i(*), freq_r(*)
       real(c_double), value :: ecut
     end function
+    ! its transform matrix on the host (complex (nwhis+1) x (niw+nw+1); no GPU needed)
+    integer(c_int) function qsgw_dpsion_matrix(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, b) &
+         bind(C, name='qsgw_dpsion_matrix')
+      import :: c_int, c_double, c_ptr
+      integer(c_int), value :: nwhis, niw, nw
+      real(c_double), intent(in) :: frhis(*), freq_i(*), freq_r(*)
+      real(c_double), value :: ecut
+      type(c_ptr), value :: b
+    end function
     ! the same with host chi0 and zcols (c_loc of the Fortran arrays)
     integer(c_int) function qsgw_chi0_lorentz(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, &
          zcols, ldz) bind(C, name='qsgw_chi0_lorentz')

@@ -132,6 +132,14 @@ int qsgw_dpsion_chiq_d(const double *rcxq, int npr, int npr_col, int nwhis,
                        const double *frhis, int niw, const double *freq_i,
                        int nw, const double *freq_r, double ecut,
                        double *zxqi, double *zxq);
+/* The transform matrix that call applies, on the host (no GPU needed): b
+ * (complex, (nwhis+1) x (niw + nw + 1), column-major) with b(0, j) = 0 and
+ * b(i, j) = f_i imatt(j, i) for the imaginary columns, b(i, niw + t) =
+ * f_i rmatt(t, i) + i f_i [i == t] (f_0 = 1) for the real ones, f_i =
+ * -wfac / (R_i - L_i) the bin normalisation: chi0 = rcxq . b.              */
+int qsgw_dpsion_matrix(int nwhis, const double *frhis, int niw,
+                       const double *freq_i, int nw, const double *freq_r,
+                       double ecut, double *b);
 
 /* ---- chi0 rank-k accumulation: drop-in for x0gemm (x0gemm.f90:2-97) ----
  * rcxq(npr, npr_col, (1-npm)*nwhis : nwhis) += sum over pairs of

@@ -80,3 +80,27 @@ def test_real_axis_imaginary_part_is_the_bin_average():
         assert np.allclose(zxq[:, :, t], 1j * norm * rcxq[:, :, t] + hil)
     assert np.allclose(zxq[:, :, 0], 1j * rcxq[:, :, 0] + np.einsum(
         'abk,k->ab', rcxq[:, :, 1:] * (-1.0 / (R[nwhis + 1:] - L[nwhis + 1:])), rmatt[0]))
+
+
+@pytest.mark.parametrize("ecut", [1e10, 0.05])
+def test_library_transform_matrix_vs_oracle(ecut):
+    """qsgw_dpsion_matrix (host C++, the matrix the GPU contraction applies)
+    against the oracle's imatt, rmatt and bin normalisation."""
+    from ecalj_b200 import lib
+    fr = _mesh(25)
+    nwhis = len(fr) - 1
+    freq_i = np.array([0.01, 0.2, 1.5])
+    freq_r = np.concatenate([[0.0], 0.5 * (fr[:8] + fr[1:9])])
+    b = lib.dpsion_matrix(fr, freq_i, freq_r, ecut)
+    L, C, R = dp.histogram_bins(fr)
+    imatt, rmatt = dp.transform_matrices(fr, freq_i, freq_r)
+    c = C[nwhis + 1:]
+    f = -(np.exp(-(c / ecut) ** 2) if ecut < 1e9 else 1.0) / (R[nwhis + 1:] - L[nwhis + 1:])
+    niw = len(freq_i)
+    assert np.all(b[0, :niw] == 0)
+    assert np.allclose(b[1:, :niw], (f[:, None] * imatt.T), rtol=1e-13, atol=0)
+    real = f[:, None] * rmatt.T + 0j
+    for t in range(1, len(freq_r)):
+        real[t - 1, t] += 1j * f[t - 1]
+    assert np.allclose(b[1:, niw:], real, rtol=1e-13, atol=1e-300)
+    assert b[0, niw] == 1j and np.all(b[0, niw + 1:] == 0)
