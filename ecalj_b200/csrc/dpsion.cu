@@ -1,6 +1,6 @@
 // Hilbert transform of the chi0 histogram: drop-in for dpsion_init +
-// dpsion_chiq (dpsion5.f90:77-137, 215-292) with time reversal (npm = 1),
-// no chi+- and no SmearX0 filter.
+// dpsion_chiq (dpsion5.f90:77-137, 174-292) with time reversal (npm = 1),
+// no chi+-, with the optional SmearX0 Gaussian filter.
 //
 // x0gemm leaves rcxq(npr, npr_col, 0:nwhis) = spectral weights on the
 // histogram bins [frhis(i), frhis(i+1)].  The reference normalises the bins
@@ -64,7 +64,7 @@ void hilbertmat_h(cd z, int nwhis, const std::vector<double>& L, const std::vect
 // frequencies, column-major): imatt and rmatt of dpsion_init (dpsion5.f90:93-107, 123-128) with
 // the bin normalisation -wfac / (R - L) (:215-220) and the i rcxq(t) term (:255) folded in.
 void build_transform(int nwhis, const double* frhis, int niw, const double* freq_i, int nw, const double* freq_r,
-                     double ecut, std::vector<cd>& B) {
+                     double ecut, double smear, std::vector<cd>& B) {
   // bins -nwhis..nwhis (dpsion5.f90:87-89)
   std::vector<double> L(2 * nwhis + 1), R(2 * nwhis + 1), C(2 * nwhis + 1);
   for (int i = 1; i <= nwhis; ++i) {
@@ -99,6 +99,32 @@ void build_transform(int nwhis, const double* frhis, int niw, const double* freq
       col[i] = fnorm[i] * (std::real(rm[nwhis + i]) / pi - std::real(rm[nwhis - i]) / pi);
     col[t] += cd(0.0, fnorm[t]);                   // slot 0 is not normalised: fnorm[0] = 1
   }
+  // SmearX0 (dpsion5.f90:174-193): rcxq(bins) <- rcxq(bins) . gfmat^T before the normalisation,
+  // folded in as B(bins, :) <- gfmat^T B(bins, :); gfmat(j, i) = exp(-(c_i - c_j)^2 / (2 smear^2))
+  // normalised over j (gaussianfilterhis, :459-483)
+  if (std::fabs(smear) > 1e-15) {
+    std::vector<double> c(nwhis), g(static_cast<size_t>(nwhis) * nwhis);
+    for (int i = 0; i < nwhis; ++i) c[i] = 0.5 * (frhis[i] + frhis[i + 1]);
+    for (int i = 0; i < nwhis; ++i) {
+      double sum = 0.0;
+      for (int j = 0; j < nwhis; ++j) {
+        const double d = c[i] - c[j];
+        g[j + static_cast<size_t>(nwhis) * i] = std::exp(-d * d / (2.0 * smear * smear));
+        sum += g[j + static_cast<size_t>(nwhis) * i];
+      }
+      for (int j = 0; j < nwhis; ++j) g[j + static_cast<size_t>(nwhis) * i] /= sum;
+    }
+    std::vector<cd> tmp(nwhis);
+    for (int col = 0; col < ncol; ++col) {
+      cd* bc = B.data() + static_cast<size_t>(col) * K;
+      for (int k = 0; k < nwhis; ++k) {          // new row k+1 = sum_b gfmat(b, k) old row b+1
+        cd acc(0.0, 0.0);
+        for (int b = 0; b < nwhis; ++b) acc += g[b + static_cast<size_t>(nwhis) * k] * bc[b + 1];
+        tmp[k] = acc;
+      }
+      for (int k = 0; k < nwhis; ++k) bc[k + 1] = tmp[k];
+    }
+  }
 }
 
 }  // namespace
@@ -111,7 +137,7 @@ using namespace qsgw;
 
 extern "C" int qsgw_dpsion_chiq_d(const double* rcxq, int npr, int npr_col, int nwhis, const double* frhis,
                                   int niw, const double* freq_i, int nw, const double* freq_r, double ecut,
-                                  double* zxqi, double* zxq) {
+                                  double smearx0, double* zxqi, double* zxq) {
   int rc = require_init();
   if (rc) return rc;
   QSGW_ARG(rcxq && frhis && npr >= 1 && npr_col >= 1 && nwhis >= 1 && niw >= 0 && nw >= -1,
@@ -129,7 +155,7 @@ extern "C" int qsgw_dpsion_chiq_d(const double* rcxq, int npr, int npr_col, int 
   QSGW_ARG(((reinterpret_cast<uintptr_t>(rcxq) | reinterpret_cast<uintptr_t>(zxqi) |
              reinterpret_cast<uintptr_t>(zxq)) & 15) == 0, "dpsion_chiq: complex arrays must be 16-byte aligned");
   std::vector<cd> B;
-  build_transform(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, B);
+  build_transform(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, smearx0, B);
   const int K = nwhis + 1;
   cudaStream_t s = ctx().stream;
   rc = g_dp_b.ensure(B.size() * sizeof(cd));
@@ -152,7 +178,7 @@ extern "C" int qsgw_dpsion_chiq_d(const double* rcxq, int npr, int npr_col, int 
 }
 
 extern "C" int qsgw_dpsion_matrix(int nwhis, const double* frhis, int niw, const double* freq_i, int nw,
-                                  const double* freq_r, double ecut, double* b) {
+                                  const double* freq_r, double ecut, double smearx0, double* b) {
   QSGW_ARG(frhis && b && nwhis >= 1 && niw >= 0 && nw >= -1 && nw < nwhis,
            "dpsion_matrix: nwhis=%d niw=%d nw=%d", nwhis, niw, nw);
   QSGW_ARG(niw == 0 || freq_i, "dpsion_matrix: niw=%d needs freq_i", niw);
@@ -160,7 +186,7 @@ extern "C" int qsgw_dpsion_matrix(int nwhis, const double* frhis, int niw, const
   for (int i = 0; i < nwhis; ++i)
     QSGW_ARG(frhis[i + 1] > frhis[i], "dpsion_matrix: frhis not increasing at bin %d", i + 1);
   std::vector<cd> B;
-  build_transform(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, B);
+  build_transform(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, smearx0, B);
   std::copy(B.begin(), B.end(), reinterpret_cast<cd*>(b));
   return QSGW_OK;
 }

@@ -74,8 +74,8 @@ _SIGS = {
     "qsgw_set_host_async": [c_int],
     "qsgw_x0_lists": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                       c_vp, c_vp, c_vp],
-    "qsgw_dpsion_matrix": [c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_vp],
-    "qsgw_dpsion_chiq_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_vp, c_vp],
+    "qsgw_dpsion_matrix": [c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_dbl, c_vp],
+    "qsgw_dpsion_chiq_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_dbl, c_vp, c_vp],
     "qsgw_get_precision": [c_ip, c_ip],
     "qsgw_last_error": [ctypes.c_char_p, c_int],
     "qsgw_profile": [c_int],
@@ -351,7 +351,7 @@ def chi0_lorentz_d(chi0, npr, niw, freq_i, nk, nocc, nun, eocc, eunocc, zcols, l
     return chi0
 
 
-def dpsion_matrix(frhis, freq_i, freq_r=None, ecut=1e10):
+def dpsion_matrix(frhis, freq_i, freq_r=None, ecut=1e10, smearx0=0.0):
     """The Hilbert transform matrix of dpsion_chiq_d on the host (no GPU): complex
     (nwhis+1, niw + nw + 1), chi0 = rcxq . b."""
     fh, fi = _f64(frhis), _f64(freq_i)
@@ -359,11 +359,12 @@ def dpsion_matrix(frhis, freq_i, freq_r=None, ecut=1e10):
     nw = -1 if freq_r is None else len(freq_r) - 1
     fr = _f64(freq_r) if freq_r is not None else np.zeros(1)
     b = np.zeros((nwhis + 1, niw + nw + 1), np.complex128, order='F')
-    _chk(load().qsgw_dpsion_matrix(nwhis, _p(fh), niw, _p(fi), nw, _p(fr), ecut, _p(b)))
+    _chk(load().qsgw_dpsion_matrix(nwhis, _p(fh), niw, _p(fi), nw, _p(fr), ecut, smearx0, _p(b)))
     return b
 
 
-def dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, freq_i, freq_r=None, ecut=1e10, zxqi=None, zxq=None):
+def dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, freq_i, freq_r=None, ecut=1e10, zxqi=None, zxq=None,
+                  smearx0=0.0):
     """Hilbert transform of the chi0 histogram (dpsion5.f90:77-137, 215-292), npm = 1.
     rcxq, zxqi, zxq: device complex128 tensors (zxqi, zxq allocated when None).
     Returns (zxqi, zxq); zxq is None without freq_r."""
@@ -377,7 +378,7 @@ def dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, freq_i, freq_r=None, ecut=1e
         zxqi = torch.empty(M * niw, dtype=torch.complex128, device=rcxq.device)
     if zxq is None and nw >= 0:
         zxq = torch.empty(M * (nw + 1), dtype=torch.complex128, device=rcxq.device)
-    _chk(load().qsgw_dpsion_chiq_d(_p(rcxq), npr, npr_col, nwhis, _p(fh), niw, _p(fi), nw, _p(fr), ecut,
+    _chk(load().qsgw_dpsion_chiq_d(_p(rcxq), npr, npr_col, nwhis, _p(fh), niw, _p(fi), nw, _p(fr), ecut, smearx0,
                                    _p(zxqi) if zxqi is not None else None, _p(zxq) if zxq is not None else None))
     return zxqi, zxq
 

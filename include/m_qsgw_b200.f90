@@ -82,20 +82,20 @@ module m_qsgw_b200
     end function
     ! Hilbert transform of the chi0 histogram (dpsion_init + dpsion_chiq, npm = 1)
     integer(c_int) function qsgw_dpsion_chiq_d(rcxq, npr, npr_col, nwhis, frhis, niw, freq_i, nw, freq_r, &
-         ecut, zxqi, zxq) bind(C, name='qsgw_dpsion_chiq_d')
+         ecut, smearx0, zxqi, zxq) bind(C, name='qsgw_dpsion_chiq_d')
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: rcxq, zxqi, zxq
       integer(c_int), value :: npr, npr_col, nwhis, niw, nw
       real(c_double), intent(in) :: frhis(*), freq_i(*), freq_r(*)
-      real(c_double), value :: ecut
+      real(c_double), value :: ecut, smearx0
     end function
     ! its transform matrix on the host (complex (nwhis+1) x (niw+nw+1); no GPU needed)
-    integer(c_int) function qsgw_dpsion_matrix(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, b) &
+    integer(c_int) function qsgw_dpsion_matrix(nwhis, frhis, niw, freq_i, nw, freq_r, ecut, smearx0, b) &
          bind(C, name='qsgw_dpsion_matrix')
       import :: c_int, c_double, c_ptr
       integer(c_int), value :: nwhis, niw, nw
       real(c_double), intent(in) :: frhis(*), freq_i(*), freq_r(*)
-      real(c_double), value :: ecut
+      real(c_double), value :: ecut, smearx0
       type(c_ptr), value :: b
     end function
     ! the same with host chi0 and zcols (c_loc of the Fortran arrays)

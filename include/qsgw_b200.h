@@ -120,26 +120,29 @@ int qsgw_zminv_hpd_batched_noalloc_d(double *a, int n, int lda, int nbatch,
                                      void *stream);
 
 /* ---- Hilbert transform of the chi0 histogram: drop-in for dpsion_init +
- * dpsion_chiq (dpsion5.f90:77-137, 215-292; hilbertmat.f90:14-79), time
- * reversal (npm = 1), no chi+- and no SmearX0 filter.
+ * dpsion_chiq (dpsion5.f90:77-137, 174-292; hilbertmat.f90:14-79), time
+ * reversal (npm = 1), no chi+-.
  * rcxq (device, npr*npr_col x (nwhis+1) complex, slots 0..nwhis as x0gemm
  * leaves them), frhis (host, nwhis+1 increasing bin edges, Hartree), freq_i
  * (host, niw), freq_r (host, nw+1, freq_r[0] = 0; nw = -1 skips the real
- * axis), ecut (>= 1e9: no Gaussian cut).  zxqi (device, npr*npr_col x niw)
+ * axis), ecut (>= 1e9: no Gaussian cut), smearx0 (GWinput SmearX0: the
+ * Gaussian filter of the bins, gaussianfilterhis dpsion5.f90:459-483; 0 =
+ * off).  zxqi (device, npr*npr_col x niw)
  * = chi0(i freq_i), zxq (device, npr*npr_col x (nw+1)) = chi0(freq_r): the
  * reference leaves the latter in rcxq(:, :, 0:nw); rcxq is not modified here. */
 int qsgw_dpsion_chiq_d(const double *rcxq, int npr, int npr_col, int nwhis,
                        const double *frhis, int niw, const double *freq_i,
                        int nw, const double *freq_r, double ecut,
-                       double *zxqi, double *zxq);
+                       double smearx0, double *zxqi, double *zxq);
 /* The transform matrix that call applies, on the host (no GPU needed): b
  * (complex, (nwhis+1) x (niw + nw + 1), column-major) with b(0, j) = 0 and
  * b(i, j) = f_i imatt(j, i) for the imaginary columns, b(i, niw + t) =
  * f_i rmatt(t, i) + i f_i [i == t] (f_0 = 1) for the real ones, f_i =
- * -wfac / (R_i - L_i) the bin normalisation: chi0 = rcxq . b.              */
+ * -wfac / (R_i - L_i) the bin normalisation, then (smearx0 != 0) rows 1..
+ * nwhis replaced by gfmat^T b: chi0 = rcxq . b.                            */
 int qsgw_dpsion_matrix(int nwhis, const double *frhis, int niw,
                        const double *freq_i, int nw, const double *freq_r,
-                       double ecut, double *b);
+                       double ecut, double smearx0, double *b);
 
 /* ---- chi0 rank-k accumulation: drop-in for x0gemm (x0gemm.f90:2-97) ----
  * rcxq(npr, npr_col, (1-npm)*nwhis : nwhis) += sum over pairs of

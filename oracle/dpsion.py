@@ -8,8 +8,9 @@ numpy restatement of
   the bins [his_L, his_R] on both sides of zero, imatt(j, i) =
   Re[rmat(i) - rmat(-i)] / pi at z = i freq_i(j), rmatt(it, i) =
   Re[rmat(i) - rmat(-i)] / pi at z = freq_r(it);
-* dpsion_chiq (dpsion5.f90:215-292), npm = 1, no chi+- and no SmearX0
-  filter: rcxq(bin) <- -wfac / (R - L) rcxq(bin) for bins 1..nwhis, then
+* dpsion_chiq (dpsion5.f90:174-292), npm = 1, no chi+-: the optional SmearX0
+  filter rcxq(bins) <- rcxq(bins) . gfmat^T (:174-193, gaussianfilterhis
+  :459-483), rcxq(bin) <- -wfac / (R - L) rcxq(bin) for bins 1..nwhis, then
   zxqi = rcxq . imatt^T and, on the real axis, chi0(freq_r(it)) =
   i rcxq(it) + rcxq . rmatt(it, :)^T.
 
@@ -82,13 +83,24 @@ def transform_matrices(frhis, freq_i, freq_r=None):
     return imatt, rmatt
 
 
-def dpsion_chiq(rcxq, frhis, freq_i, freq_r=None, ecut=1e10):
+def gaussian_filter(frhis, smear):
+    """gfmat (nwhis, nwhis) of gaussianfilterhis (dpsion5.f90:459-483): column i is
+    exp(-(c_i - c_j)^2 / (2 smear^2)) over j, normalised to sum 1, c = bin centres."""
+    frhis = np.asarray(frhis, dtype=np.float64)
+    c = 0.5 * (frhis[:-1] + frhis[1:])
+    g = np.exp(-(c[None, :] - c[:, None]) ** 2 / (2.0 * smear ** 2))   # g[j, i]
+    return g / g.sum(axis=0)[None, :]
+
+
+def dpsion_chiq(rcxq, frhis, freq_i, freq_r=None, ecut=1e10, smear=0.0):
     """rcxq (npr, npr_col, nwhis+1): the x0gemm histogram, slots 0..nwhis.
     Returns zxqi (npr, npr_col, niw) and, with freq_r, zxq (npr, npr_col,
     nw+1) = the real-axis chi0 the reference leaves in rcxq(:, :, 0:nw)."""
     L, C, R = histogram_bins(frhis)
     nwhis = len(frhis) - 1
     r = np.array(rcxq, dtype=np.complex128, copy=True)
+    if abs(smear) > 1e-15:                              # :174-193: rcxq(:, :, 1:) . gfmat^T
+        r[:, :, 1:] = np.einsum('abk,jk->abj', r[:, :, 1:], gaussian_filter(frhis, smear))
     for iw in range(1, nwhis + 1):
         k = iw + nwhis
         wfac = np.exp(-(C[k] / ecut) ** 2) if ecut < 1e9 else 1.0

@@ -104,3 +104,22 @@ def test_library_transform_matrix_vs_oracle(ecut):
         real[t - 1, t] += 1j * f[t - 1]
     assert np.allclose(b[1:, niw:], real, rtol=1e-13, atol=1e-300)
     assert b[0, niw] == 1j and np.all(b[0, niw + 1:] == 0)
+
+
+def test_library_matrix_with_smear_applies_the_filter():
+    """With SmearX0 the library matrix applied to rcxq equals the oracle's filtered transform."""
+    from ecalj_b200 import lib
+    fr = _mesh(30)
+    nwhis = len(fr) - 1
+    rng = np.random.default_rng(8)
+    rcxq = rng.standard_normal((3, 2, nwhis + 1)) + 1j * rng.standard_normal((3, 2, nwhis + 1))
+    freq_i = np.array([0.05, 0.4])
+    freq_r = np.concatenate([[0.0], 0.5 * (fr[:9] + fr[1:10])])
+    smear = 0.01
+    b = lib.dpsion_matrix(fr, freq_i, freq_r, 1e10, smear)
+    got = np.einsum('abk,kj->abj', rcxq, b)
+    ri, rr = dp.dpsion_chiq(rcxq, fr, freq_i, freq_r, smear=smear)
+    ref = np.concatenate([ri, rr], axis=2)
+    assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    g = dp.gaussian_filter(fr, smear)
+    assert np.allclose(g.sum(axis=0), 1.0)

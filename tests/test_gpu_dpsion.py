@@ -1,7 +1,7 @@
 """qsgw_dpsion_chiq_d (Hilbert transform of the chi0 histogram) against
 oracle/dpsion.py: relative Frobenius error <= 1e-11 on chi0(i w) and
-chi0(w_r), with and without the Gaussian cut ecut, odd sizes, the imaginary
-axis alone, and the reference's argument checks."""
+chi0(w_r), with and without the Gaussian cut ecut and the SmearX0 filter,
+odd sizes, the imaginary axis alone, and the reference's argument checks."""
 import numpy as np
 import pytest
 
@@ -26,10 +26,10 @@ def _case(npr, npr_col, nwhis, niw, nw, seed):
     return frhis, rcxq, freq_i, freq_r
 
 
-def _run(qsgw, npr, npr_col, nwhis, frhis, rcxq, freq_i, freq_r, ecut):
+def _run(qsgw, npr, npr_col, nwhis, frhis, rcxq, freq_i, freq_r, ecut, smear=0.0):
     import torch
     d = torch.from_numpy(np.asfortranarray(rcxq).reshape(-1, order='F')).to('cuda')
-    zi, zr = qsgw.dpsion_chiq_d(d, npr, npr_col, nwhis, frhis, freq_i, freq_r, ecut)
+    zi, zr = qsgw.dpsion_chiq_d(d, npr, npr_col, nwhis, frhis, freq_i, freq_r, ecut, smearx0=smear)
     qsgw.synchronize()
     niw = len(freq_i)
     gi = zi.cpu().numpy().reshape((npr, npr_col, niw), order='F') if zi is not None else None
@@ -37,16 +37,17 @@ def _run(qsgw, npr, npr_col, nwhis, frhis, rcxq, freq_i, freq_r, ecut):
     return gi, gr
 
 
-@pytest.mark.parametrize("npr,npr_col,nwhis,niw,nw,ecut", [
-    (37, 29, 40, 12, 15, 1e10),
-    (37, 29, 40, 12, 15, 0.03),
-    (64, 1, 7, 3, 0, 1e10),
-    (200, 200, 150, 24, 60, 1e10),
+@pytest.mark.parametrize("npr,npr_col,nwhis,niw,nw,ecut,smear", [
+    (37, 29, 40, 12, 15, 1e10, 0.0),
+    (37, 29, 40, 12, 15, 0.03, 0.0),
+    (37, 29, 40, 12, 15, 1e10, 0.005),
+    (64, 1, 7, 3, 0, 1e10, 0.0),
+    (200, 200, 150, 24, 60, 1e10, 0.0),
 ])
-def test_dpsion_vs_oracle(qsgw, npr, npr_col, nwhis, niw, nw, ecut):
+def test_dpsion_vs_oracle(qsgw, npr, npr_col, nwhis, niw, nw, ecut, smear):
     frhis, rcxq, freq_i, freq_r = _case(npr, npr_col, nwhis, niw, nw, seed=npr + nwhis)
-    ri, rr = dp.dpsion_chiq(rcxq, frhis, freq_i, freq_r, ecut)
-    gi, gr = _run(qsgw, npr, npr_col, nwhis, frhis, rcxq, freq_i, freq_r, ecut)
+    ri, rr = dp.dpsion_chiq(rcxq, frhis, freq_i, freq_r, ecut, smear)
+    gi, gr = _run(qsgw, npr, npr_col, nwhis, frhis, rcxq, freq_i, freq_r, ecut, smear)
     print(f"dpsion {npr}x{npr_col} nwhis={nwhis}: imag {rel_fro(gi, ri):.2e} real {rel_fro(gr, rr):.2e}")
     assert rel_fro(gi, ri) < TOL
     assert rel_fro(gr, rr) < TOL
