@@ -51,6 +51,23 @@ int main(int argc, char** argv) {
                     whwc[3] == 1.0 && kmin[0] == 1 && kmax[0] == 1 && kmin[1] == 2 && kmax[1] == 2;
     if (!ok) return fail("qsgw_x0_lists tables");
   }
+  {
+    // host-only: the Hilbert transform matrix; chi0(i w) of one bin of weight 1 is b(bin, j)
+    const int nwhis = 6, niw = 2, nw = 2;
+    const double frhis[nwhis + 1] = {0.0, 0.01, 0.03, 0.06, 0.1, 0.15, 0.21};
+    const double freq_i[niw] = {0.05, 0.5}, freq_r[nw + 1] = {0.0, 0.005, 0.02};
+    std::vector<cd> b(static_cast<size_t>(nwhis + 1) * (niw + nw + 1));
+    if (qsgw_dpsion_matrix(nwhis, frhis, niw, freq_i, nw, freq_r, 1e10, 0.0, reinterpret_cast<double*>(b.data())) !=
+        QSGW_OK)
+      return fail("qsgw_dpsion_matrix");
+    // a positive weight (x0gemm's sign) gives chi0(i w) < 0, decreasing in magnitude with w
+    const cd c0 = b[3 + 0 * (nwhis + 1)], c1 = b[3 + 1 * (nwhis + 1)];
+    if (!(c0.real() < 0.0 && c1.real() < 0.0 && std::abs(c1) < std::abs(c0) && c0.imag() == 0.0))
+      return fail("qsgw_dpsion_matrix values");
+    if (qsgw_dpsion_matrix(nwhis, frhis, niw, freq_i, nwhis, freq_r, 1e10, 0.0,
+                           reinterpret_cast<double*>(b.data())) != QSGW_ERR_ARG)   // nw >= nwhis
+      return fail("qsgw_dpsion_matrix argument check");
+  }
   if (argc < 2 || std::strcmp(argv[1], "gpu") != 0) {
     std::printf("OK cpu\n");
     return 0;

@@ -123,3 +123,15 @@ def test_library_matrix_with_smear_applies_the_filter():
     assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
     g = dp.gaussian_filter(fr, smear)
     assert np.allclose(g.sum(axis=0), 1.0)
+
+
+def test_library_matrix_argument_checks():
+    """The reference's checks (dpsion5.f90:208-209) and the mesh's: errors, no output."""
+    from ecalj_b200 import lib
+    fr = _mesh(10)
+    with pytest.raises(lib.QSGWError):                       # nwhis <= nw
+        lib.dpsion_matrix(fr, [0.1], np.concatenate([[0.0], fr[:10]]))
+    with pytest.raises(lib.QSGWError):                       # freq_r(0) /= 0
+        lib.dpsion_matrix(fr, [0.1], np.array([0.01, 0.02]))
+    with pytest.raises(lib.QSGWError):                       # bins not increasing
+        lib.dpsion_matrix(fr[::-1].copy(), [0.1])

@@ -51,3 +51,13 @@ def test_lists_empty_and_capacity():
     rc = lib.load().qsgw_x0_lists(w.ctypes.data, 3, 2, 2, 5, 1, ctypes.byref(nc), ctypes.byref(nt),
                                   *[arr.ctypes.data] * 6, np.zeros(1).ctypes.data, arr.ctypes.data, arr.ctypes.data)
     assert lib.STATUS[rc] == "ERR_ARG"
+
+
+def test_lists_argument_checks():
+    import ctypes
+    w = np.zeros((2, 2, 2, 3))
+    nc, nt = ctypes.c_int(0), ctypes.c_int(0)
+    f = lib.load().qsgw_x0_lists
+    assert lib.STATUS[f(w.ctypes.data, 2, 2, 2, 3, 2, ctypes.byref(nc), ctypes.byref(nt), *([None] * 9))] == "ERR_ARG"
+    assert lib.STATUS[f(w.ctypes.data, 0, 2, 2, 3, 0, ctypes.byref(nc), ctypes.byref(nt), *([None] * 9))] == "ERR_ARG"
+    assert lib.STATUS[f(w.ctypes.data, 2, 2, 2, 3, 1, ctypes.byref(nc), ctypes.byref(nt), *([None] * 9))] == "ERR_ARG"
