@@ -147,7 +147,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     } else if (warp == 1 && lane == 0) {
       // ---------------- MMA issuer
       constexpr bool seg_mode = SEG;
-      // counters instead of divisions: this thread's issue latency paces the tensor pipe
+      // counters instead of divisions, and descriptors built once: this thread's issue latency
+      // paces the tensor pipe.  A descriptor's address field is the shared address / 16, so the
+      // descriptor of (stage, slice, K step) is the base descriptor plus that offset / 16.
+      const uint64_t dA0 = sw128_desc(smem_u32(sA));
+      const uint64_t dB0 = seg_mode ? sw128_desc(smem_u32(sS)) : sw128_desc(smem_u32(sB));
+      constexpr uint32_t A_ST = (2 * SLICE_A) >> 4, A_LO = SLICE_A >> 4;
+      constexpr uint32_t B_ST = (2 * (seg_mode ? SLICE_S : SLICE_B)) >> 4, B_LO = (seg_mode ? SLICE_S : SLICE_B) >> 4;
       int per = 0, cin = 0, cin_p = 0, b = 0, bph = 0;
       for (int c = 0; c < nchunk && !*abort_flag; ++c) {
         const int st = c % NST;
@@ -160,17 +166,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         // weight is applied to the FP32 period sums by the drain warps)
         if (!seg_mode && !mbar_wait(&bfull[b], bph, abort_flag)) break;
         tc_fence_after();
-        const uint32_t a_hi = smem_u32(sA + st * 2 * SLICE_A), a_lo = a_hi + SLICE_A;
-        const uint32_t b_hi = seg_mode ? smem_u32(sS + st * 2 * SLICE_S) : smem_u32(sB + b * 2 * SLICE_B);
-        const uint32_t b_lo = b_hi + (seg_mode ? SLICE_S : SLICE_B);
+        const uint64_t a_hi = dA0 + static_cast<uint32_t>(st) * A_ST, a_lo = a_hi + A_LO;
+        const uint64_t b_hi = dB0 + static_cast<uint32_t>(seg_mode ? st : b) * B_ST, b_lo = b_hi + B_LO;
         const uint32_t d = tmem + static_cast<uint32_t>(ab * NC);
 #pragma unroll
         for (int kk = 0; kk < KC / 16; ++kk) {
-          const uint32_t ko = kk * 32;               // 16 FP16 = 32 B along K
+          const uint32_t ko = kk * 2;                // 16 FP16 = 32 B along K = 2 descriptor units
           const uint32_t acc0 = (first_of_period && kk == 0) ? 0u : 1u;
-          umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_hi + ko), acc0);
-          umma_f16(d, sw128_desc(a_hi + ko), sw128_desc(b_lo + ko), 1u);
-          umma_f16(d, sw128_desc(a_lo + ko), sw128_desc(b_hi + ko), 1u);
+          umma_f16(d, a_hi + ko, b_hi + ko, acc0);
+          umma_f16(d, a_hi + ko, b_lo + ko, 1u);
+          umma_f16(d, a_lo + ko, b_hi + ko, 1u);
         }
         if (!seg_mode) umma_commit(&bempty[b]);
         umma_commit(&empty[st]);
