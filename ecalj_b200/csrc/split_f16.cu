@@ -552,13 +552,13 @@ static int launch_mode(const CUtensorMap& ma, const CUtensorMap& ms, const Param
   return QSGW_OK;
 }
 
-// Sigma_c kernel: 0 = one CTA per 64 x 128 tile (default, the fastest on B200), 1 = CTA pairs
-// over 128-column tiles, 2 = one CTA per 64 x 256 tile; QSGW_SIGC_KERNEL=<n> sets it at load time
+// Sigma_c kernel: 0 = one CTA per 64 x 128 tile, 1 = CTA pairs over 128-column tiles, 2 = one
+// CTA per 64 x 256 tile (default, the fastest on B200); QSGW_SIGC_KERNEL=<n> sets it at load time
 static int g_sigc_kind = -1;
 static int sigc_kind() {
   if (g_sigc_kind < 0) {
     const char* e = std::getenv("QSGW_SIGC_KERNEL");
-    g_sigc_kind = (e && (e[0] == '1' || e[0] == '2') && e[1] == '\0') ? e[0] - '0' : 0;
+    g_sigc_kind = (e && (e[0] == '0' || e[0] == '1' || e[0] == '2') && e[1] == '\0') ? e[0] - '0' : 2;
   }
   return g_sigc_kind;
 }

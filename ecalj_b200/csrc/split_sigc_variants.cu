@@ -1,7 +1,7 @@
-// Opt-in variants of the split-FP16 Sigma_c contraction (qsgw_set_sigc_kernel):
-// CTA pairs (tcgen05 cta_group::2) and 64 x 256 tiles (N = 256 MMAs with the
-// FP64 period sums in a global scratch tile).  Both compute the sums of the
-// default 64 x 128 kernel of split_f16.cu.
+// Variants of the split-FP16 Sigma_c contraction (qsgw_set_sigc_kernel): 64 x
+// 256 tiles (N = 256 MMAs with the FP64 period sums in a global scratch tile;
+// the default) and CTA pairs (tcgen05 cta_group::2, opt-in).  Both compute the
+// sums of the 64 x 128 kernel of split_f16.cu.
 #include "split_common.cuh"
 
 namespace qsgw {
@@ -10,11 +10,12 @@ namespace tc {
 // ------------------------------------------------------------------ Sigma_c on 256-column tiles
 // The Sigma_c contraction with N = 256 MMAs (64 complex rows x 256 columns per
 // CTA): twice the work per instruction, four 48 KB stages of 32-element K
-// chunks (64-byte swizzled rows).  Measured on B200 (8 tasks of 600 x 600 at
-// 1965 MHz): 35.4 ms against 31.0 ms for the 64 x 128 kernel (37.3 ms with two
-// 96 KB stages of 64-element chunks), although a bare stream of N = 256 MMAs
-// does twice the work of the N = 128 stream in 1.36 times the time; so it is
-// the opt-in variant.  The two FP32
+// chunks (64-byte swizzled rows).  The default Sigma_c kernel: measured on
+// B200 (8 tasks of 600 x 600 at 1965 MHz) 29.05 ms against 30.5 ms for the
+// 64 x 128 kernel, whose single MMA-issuing thread cannot keep up with
+// 128 x 128 x 16 MMAs (about 80 clocks of issue per 64 clocks of math).  The
+// drain loads the 16 previous sums of a column block before updating them (one
+// L2 round trip instead of one per column).  The two FP32
 // accumulators (one per segment, alternating) fill TMEM's 512 columns, so the
 // FP64 sums over segments live in a per-CTA scratch tile in global memory
 // (L2-resident while the CTA runs, [column][TMEM lane], coalesced per warp):
@@ -169,16 +170,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (!mbar_wait_warp(&accfull[ab], (seg >> 1) & 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
 #pragma unroll 1
-        for (int cb = 0; cb < 64; cb += 32) {
-          uint32_t fa[16], fb[16];
+        for (int cb = 0; cb < 64; cb += 16) {
+          // the 16 previous sums are loaded together (one L2 round trip), then updated
+          uint32_t fa[16];
+          double prev[16];
           tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NW + c_lo + cb), fa);
-          tmem_ld16(tmem + lane_base + static_cast<uint32_t>(ab * NW + c_lo + cb + 16), fb);
+          double* q = scr + static_cast<size_t>(c_lo + cb) * BM2 + row;
+          if (seg > 0) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) prev[i] = q[static_cast<size_t>(i) * BM2];
+          }
           tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            const double v = static_cast<double>(__uint_as_float(i < 16 ? fa[i] : fb[i - 16]));
-            double* q = scr + static_cast<size_t>(c_lo + cb + i) * BM2 + row;
-            *q = (seg == 0) ? v * wsm[cb + i] : fma(v, wsm[cb + i], *q);
+          for (int i = 0; i < 16; ++i) {
+            const double v = static_cast<double>(__uint_as_float(fa[i]));
+            q[static_cast<size_t>(i) * BM2] = (seg == 0) ? v * wsm[cb + i] : fma(v, wsm[cb + i], prev[i]);
           }
         }
         tc_fence_before();

@@ -255,8 +255,8 @@ SIGC_NARROW, SIGC_PAIR, SIGC_WIDE = 0, 1, 2
 
 
 def set_sigc_kernel(kind):
-    """Split-precision Sigma_c kernel: SIGC_NARROW (one CTA per 64 x 128 tile, default),
-    SIGC_PAIR (CTA pairs over 128-column tiles), SIGC_WIDE (one CTA per 64 x 256 tile)."""
+    """Split-precision Sigma_c kernel: SIGC_NARROW (one CTA per 64 x 128 tile), SIGC_PAIR
+    (CTA pairs over 128-column tiles), SIGC_WIDE (one CTA per 64 x 256 tile, default)."""
     _chk(load().qsgw_set_sigc_kernel(int(kind)))
 
 

@@ -66,11 +66,11 @@ int qsgw_set_host_async(int on);
 int qsgw_set_precision(int mode, int nslices);
 int qsgw_get_precision(int *mode, int *nslices);
 /* Kernel of the split-precision Sigma_c contraction: 0 = one CTA per
- * 64 x 128 output tile (the default, the fastest on B200), 1 = CTA pairs over
- * 128-column tiles (tcgen05 cta_group::2, M = 256 over two SMs, each loading
- * half of the B tile), 2 = one CTA per 64 x 256 tile (N = 256 MMAs, FP64 sums
- * in a global scratch tile).  All compute the same sums; the environment
- * variable QSGW_SIGC_KERNEL=<kind> sets it at load time. */
+ * 64 x 128 output tile, 1 = CTA pairs over 128-column tiles (tcgen05
+ * cta_group::2, M = 256 over two SMs, each loading half of the B tile), 2 =
+ * one CTA per 64 x 256 tile (N = 256 MMAs, FP64 sums in a global scratch
+ * tile; the default, the fastest on B200).  All compute the same sums; the
+ * environment variable QSGW_SIGC_KERNEL=<kind> sets it at load time. */
 int qsgw_set_sigc_kernel(int kind);
 /* Copies the last error message (NUL-terminated, truncated to len). */
 int qsgw_last_error(char *buf, int len);

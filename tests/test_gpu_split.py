@@ -109,7 +109,7 @@ def test_sigc_split_kernels_multi_tile(split, ngb):
                                    t['wx'], t['expa'], t['freq_r'])
             outs[kind] = got
     finally:
-        split.set_sigc_kernel(split.SIGC_NARROW)
+        split.set_sigc_kernel(split.SIGC_WIDE)
     for kind, got in outs.items():
         err = rel_fro(got, ref)
         dqp = np.max(np.abs(np.real(np.diag(got) - np.diag(ref)))) * HARTREE_MEV
