@@ -37,7 +37,7 @@ METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err 
 # DRAM bytes (read + write) of one split-precision Sigma_c task launch
 # (N=600, 40 x 400 states, 25 imaginary slots + real-axis pole columns),
 # measured with ncu on that launch: 1.975 GB read + 0.240 GB written.
-SIGC_TC_TRAFFIC = 2.215e9
+SIGC_TC_TRAFFIC = 3.315e9
 
 
 def load_peaks():
@@ -428,7 +428,7 @@ def main():
             "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if achieved else None,
             "traffic": SIGC_TC_TRAFFIC if prec == "split" else None,
             "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one Sigma_c task launch "
-                               "(same shape) from ncu" if prec == "split" else "not captured"),
+                               "(same shape, sigc_wide_kernel) from ncu" if prec == "split" else "not captured"),
             "kernel": dom_tag, "launch_ms": round(per_launch_ms, 4), "peak_source": peak_note,
             "algorithmic_flops_per_launch": dom_flops * args.steps / max(k_n, 1)}
 
