@@ -24,14 +24,14 @@ static int copy_stream(cudaStream_t* cs) {
 }
 
 // pinned arena of the asynchronous mode's host tables (NSEC sections, one per call in turn)
-constexpr size_t ARENA_HALF = size_t(16) << 20;     // bytes of one section
+constexpr size_t ARENA_SECTION = size_t(16) << 20;     // bytes of one section
 constexpr int NSEC = 16;
 static char* g_arena = nullptr;
 static DevBuf g_darena;                    // device image of the arena: tables land here first
-static size_t g_arena_off[NSEC] = {};
-static int g_half = 0;                     // section of the current call
-static cudaEvent_t g_half_done[NSEC] = {};
-static bool g_half_used[NSEC] = {};
+static size_t g_sec_off[NSEC] = {};
+static int g_sec = 0;                     // section of the current call
+static cudaEvent_t g_sec_done[NSEC] = {};
+static bool g_sec_used[NSEC] = {};
 
 // Host -> device copy ordered for the asynchronous mode: on the copy stream, after the compute
 // stream's work so far (the destination may still be read there) and ahead of the next call's
@@ -74,29 +74,29 @@ __global__ void table_copy_kernel(unsigned char* __restrict__ dst, const unsigne
 // a new host-pointer call: close the current section, open the next once the GPU is past it
 static int arena_next_call() {
   if (!g_arena) return QSGW_OK;
-  QSGW_CUDA(cudaEventRecord(g_half_done[g_half], ctx().stream));
-  g_half_used[g_half] = true;
-  g_half = (g_half + 1) % NSEC;
-  if (g_half_used[g_half]) QSGW_CUDA(cudaEventSynchronize(g_half_done[g_half]));
-  g_arena_off[g_half] = 0;
+  QSGW_CUDA(cudaEventRecord(g_sec_done[g_sec], ctx().stream));
+  g_sec_used[g_sec] = true;
+  g_sec = (g_sec + 1) % NSEC;
+  if (g_sec_used[g_sec]) QSGW_CUDA(cudaEventSynchronize(g_sec_done[g_sec]));
+  g_sec_off[g_sec] = 0;
   return QSGW_OK;
 }
 
 int async_table_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   if (!g_arena) {
-    int rc = g_darena.ensure(NSEC * ARENA_HALF);
+    int rc = g_darena.ensure(NSEC * ARENA_SECTION);
     if (rc) return rc;
-    QSGW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&g_arena), NSEC * ARENA_HALF, cudaHostAllocDefault));
-    for (auto& e : g_half_done) QSGW_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    QSGW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&g_arena), NSEC * ARENA_SECTION, cudaHostAllocDefault));
+    for (auto& e : g_sec_done) QSGW_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
-  if (bytes > ARENA_HALF)                  // larger than a section: copied from the caller's memory
+  if (bytes > ARENA_SECTION)                  // larger than a section: copied from the caller's memory
     return ordered_h2d(dst, src, bytes, s, true);
-  size_t& off = g_arena_off[g_half];
-  if (off + bytes > ARENA_HALF) {          // this call's section is full: let the GPU catch up
+  size_t& off = g_sec_off[g_sec];
+  if (off + bytes > ARENA_SECTION) {          // this call's section is full: let the GPU catch up
     QSGW_CUDA(cudaStreamSynchronize(s));
     off = 0;
   }
-  const size_t at = static_cast<size_t>(g_half) * ARENA_HALF + off;
+  const size_t at = static_cast<size_t>(g_sec) * ARENA_SECTION + off;
   std::memcpy(g_arena + at, src, bytes);
   off += (bytes + 255) & ~size_t(255);
   // pinned section -> device section on the copy stream (no reader of this section is left:
@@ -198,12 +198,12 @@ void host_stage_release() {
   g_arena = nullptr;
   g_darena.release();
   for (int h = 0; h < NSEC; ++h) {
-    if (g_half_done[h]) cudaEventDestroy(g_half_done[h]);
-    g_half_done[h] = nullptr;
-    g_half_used[h] = false;
-    g_arena_off[h] = 0;
+    if (g_sec_done[h]) cudaEventDestroy(g_sec_done[h]);
+    g_sec_done[h] = nullptr;
+    g_sec_used[h] = false;
+    g_sec_off[h] = 0;
   }
-  g_half = 0;
+  g_sec = 0;
   for (auto& e : g_ord) {
     if (e) cudaEventDestroy(e);
     e = nullptr;
