@@ -119,6 +119,10 @@ _SIGS = {
                           c_vp, c_vp],
     "qsgw_wv_write_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int],
     "qsgw_wv_read_d": [ctypes.c_char_p, c_vp, c_int, c_int, c_int, c_int, c_int, c_int],
+    "qsgw_vcoud_write": [ctypes.c_char_p, c_int, c_vp, c_vp, c_vp],
+    "qsgw_vcoud_read": [ctypes.c_char_p, c_int, c_ip, c_vp, c_vp, c_vp, c_vp],
+    "qsgw_sigma_write": [ctypes.c_char_p, c_vp, c_int, c_vp, c_vp],
+    "qsgw_sigma_read": [ctypes.c_char_p, c_vp, c_int, c_int, c_vp, c_vp, c_vp],
     "qsgw_wsurr_init": [ctypes.c_ulonglong],
     "qsgw_wsurr_nparam": [],
     "qsgw_wsurr_params": [c_vp, c_int],
@@ -609,6 +613,56 @@ def wv_read_d(path, out, nblochpmx, rec0, nrec, kind4=False, pack=0, ngb=0):
     upper triangle of (W + W^H)/2 (2) of the leading ngb x ngb block."""
     _chk(load().qsgw_wv_read_d(os.fsencode(path), _p(out), nblochpmx, rec0, nrec, int(kind4), pack, ngb))
     return out
+
+
+# ---------------------------------------------------------------- sequential unformatted files (host)
+def vcoud_write(path, q, vcoud, zcousq):
+    """__Vcoud.<iq>: ngb | q(3) | vcoud(ngb) | zcousq(ngb, ngb) (main_hvccfp0.f90:396-400)."""
+    v = _f64(vcoud)
+    z = np.asfortranarray(np.asarray(zcousq, dtype=np.complex128))
+    n = v.size
+    if z.shape != (n, n):
+        raise ValueError(f"zcousq must be ({n}, {n}), got {z.shape}")
+    _chk(load().qsgw_vcoud_write(os.fsencode(path), n, _p(_f64(q)), _p(v), _p(z)))
+
+
+def vcoud_read(path):
+    """Readvcoud (m_readVcoud.f90:30-40): returns q, vcoud, vcousq, zcousq (Fortran order)."""
+    f = load().qsgw_vcoud_read
+    n = ctypes.c_int(0)
+    q = np.zeros(3)
+    _chk(f(os.fsencode(path), 0, ctypes.byref(n), _p(q), None, None, None))
+    v, vs = np.zeros(n.value), np.zeros(n.value)
+    z = np.zeros((n.value, n.value), np.complex128, order='F')
+    _chk(f(os.fsencode(path), n.value, ctypes.byref(n), _p(q), _p(v), _p(vs), _p(z)))
+    return q, v, vs, z
+
+
+def sigma_write(path, head, is_, qibz, zsec):
+    """SEX2U / SEXcore2U / SEC2U: head (nspin, nq, ntq, nqbz, nqibz, n1, n2, n3), qibz (3, nq),
+    zsec (ntq, ntq, nq) complex (main_hsfp0.sc.f90:322, 333, 340, 359)."""
+    h = np.ascontiguousarray(np.asarray(head, dtype=np.int32))
+    if h.size != 8:
+        raise ValueError("head holds 8 integers")
+    nq, ntq = int(h[1]), int(h[2])
+    q = np.asfortranarray(np.asarray(qibz, dtype=np.float64))
+    z = np.asfortranarray(np.asarray(zsec, dtype=np.complex128))
+    if q.shape != (3, nq) or z.shape != (ntq, ntq, nq):
+        raise ValueError(f"qibz {q.shape} / zsec {z.shape} do not match nq={nq} ntq={ntq}")
+    _chk(load().qsgw_sigma_write(os.fsencode(path), _p(h), is_, _p(q), _p(z)))
+
+
+def sigma_read(path):
+    """Returns head, isx (nq), qibz (3, nq), zsec (ntq, ntq, nq) (main_hqpe.sc.f90:132-148)."""
+    f = load().qsgw_sigma_read
+    h = np.zeros(8, np.int32)
+    _chk(f(os.fsencode(path), _p(h), 0, 0, None, None, None))
+    nq, ntq = int(h[1]), int(h[2])
+    isx = np.zeros(max(nq, 1), np.int32)
+    q = np.zeros((3, max(nq, 1)), order='F')
+    z = np.zeros((max(ntq, 1), max(ntq, 1), max(nq, 1)), np.complex128, order='F')
+    _chk(f(os.fsencode(path), _p(h), nq, ntq, _p(isx), _p(q), _p(z)))
+    return h, isx[:nq], q[:, :nq], z[:, :, :nq]
 
 
 # ---------------------------------------------------------------- W_c frequency surrogate

@@ -165,6 +165,48 @@ module m_qsgw_b200
       type(c_ptr), value :: zw
       integer(c_int), value :: nblochpmx, rec0, nrec, kind4
     end function
+    integer(c_int) function qsgw_wv_read_d(path, out, nblochpmx, rec0, nrec, kind4, pack, ngb) &
+         bind(C, name='qsgw_wv_read_d')
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), intent(in) :: path(*)
+      type(c_ptr), value :: out
+      integer(c_int), value :: nblochpmx, rec0, nrec, kind4, pack, ngb
+    end function
+    ! __Vcoud.<iq> and SEX2U / SEXcore2U / SEC2U: the same 4-byte-marker records
+    ! the Fortran sequential unformatted writes of these files produce, so
+    ! either side can write a file the other reads
+    integer(c_int) function qsgw_vcoud_write(path, ngb, q, vcoud, zcousq) bind(C, name='qsgw_vcoud_write')
+      import :: c_int, c_char, c_double, c_double_complex
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), value :: ngb
+      real(c_double), intent(in) :: q(3), vcoud(*)
+      complex(c_double_complex), intent(in) :: zcousq(*)
+    end function
+    integer(c_int) function qsgw_vcoud_read(path, ngb_cap, ngb, q, vcoud, vcousq, zcousq) &
+         bind(C, name='qsgw_vcoud_read')
+      import :: c_int, c_char, c_double, c_ptr
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), value :: ngb_cap
+      integer(c_int), intent(out) :: ngb
+      real(c_double), intent(out) :: q(3)
+      type(c_ptr), value :: vcoud, vcousq, zcousq
+    end function
+    integer(c_int) function qsgw_sigma_write(path, head, is, qibz, zsec) bind(C, name='qsgw_sigma_write')
+      import :: c_int, c_char, c_double, c_double_complex
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), intent(in) :: head(8)
+      integer(c_int), value :: is
+      real(c_double), intent(in) :: qibz(3, *)
+      complex(c_double_complex), intent(in) :: zsec(*)
+    end function
+    integer(c_int) function qsgw_sigma_read(path, head, nq_cap, ntq_cap, isx, qibz, zsec) &
+         bind(C, name='qsgw_sigma_read')
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), intent(out) :: head(8)
+      integer(c_int), value :: nq_cap, ntq_cap
+      type(c_ptr), value :: isx, qibz, zsec
+    end function
     integer(c_int) function qsgw_graph_begin() bind(C, name='qsgw_graph_begin')
       import :: c_int
     end function

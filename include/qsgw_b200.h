@@ -438,6 +438,36 @@ int qsgw_wv_write_d(const char *path, const double *zw_d, int nblochpmx, int rec
 int qsgw_wv_read_d(const char *path, double *out_d, int nblochpmx, int rec0,
                    int nrec, int kind4, int pack, int ngb);
 
+/* ---- Sequential unformatted files (host memory, no GPU needed): a record
+ * is a 4-byte length, the payload and the length again (the gfortran /
+ * ifort / nvfortran default), 4-byte integers, at most 2^31-1 bytes.
+ *
+ * __Vcoud.<iq>, the Coulomb eigenproblem's output: records ngb | q(3) |
+ * vcoud(ngb) | zcousq(ngb, ngb) complex(8), as main_hvccfp0.f90:396-400
+ * writes them and Readvcoud (m_readVcoud.f90:30-40) reads them.
+ * read: *ngb and q (if non-NULL) from the first two records; with vcoud,
+ * vcousq and zcousq all NULL it stops there (a size query), else ngb <=
+ * ngb_cap is required and each non-NULL array is filled; vcousq =
+ * sqrt(vcoud) as Readvcoud forms it.  A record whose length does not match
+ * this layout is an error (QSGW_ERR_ARG with the record number).          */
+int qsgw_vcoud_write(const char *path, int ngb, const double *q,
+                     const double *vcoud, const double *zcousq);
+int qsgw_vcoud_read(const char *path, int ngb_cap, int *ngb, double *q,
+                    double *vcoud, double *vcousq, double *zcousq);
+/* SEX2U, SEXcore2U, SEC2U (D for spin 2), the self-energy matrices: a
+ * header record head[8] = nspin, nq, ntq, nqbz, nqibz, n1, n2, n3, then for
+ * ip = 1..nq one record is, qibz(1:3, ip), zsec(1:ntq, 1:ntq, ip)
+ * (main_hsfp0.sc.f90:322, 333, 340, 359; read at main_hqpe.sc.f90:132-148).
+ * write: nq = head[1], ntq = head[2]; qibz (3, nq) real(8); zsec (ntq, ntq,
+ * nq) complex(8); every record carries the spin index is.
+ * read: head from the header; with isx, qibz and zsec all NULL it stops
+ * there, else nq <= nq_cap and ntq <= ntq_cap are required and the non-NULL
+ * arrays are filled (isx (nq): each record's spin index).                  */
+int qsgw_sigma_write(const char *path, const int *head, int is,
+                     const double *qibz, const double *zsec);
+int qsgw_sigma_read(const char *path, int *head, int nq_cap, int ntq_cap,
+                    int *isx, double *qibz, double *zsec);
+
 /* ---- Learned W_c(q, i w) frequency interpolator.  No counterpart in the
  * reference: it stands in for computing chi0 and W at every frequency of
  * the imaginary grid.  One sample = one real channel of one element of

@@ -1,13 +1,15 @@
 // A C++ caller of libqsgw_b200 written the way a Fortran or C host would use it:
 // plain pointers to column-major complex(8) arrays, status codes, no torch.
 //   cabi_caller          checks that calls before qsgw_init fail cleanly and builds x0gemm
-//                        pair/bin lists with the host-only qsgw_x0_lists (no GPU needed)
+//                        pair/bin lists with the host-only qsgw_x0_lists, and writes and
+//                        reads a __Vcoud file (no GPU needed)
 //   cabi_caller gpu      also multiplies Fortran-layout matrices with qsgw_zmm (host
 //                        pointers, op(A) = A^H) and compares with a plain triple loop
 #include <cmath>
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 #include "qsgw_b200.h"
 
@@ -67,6 +69,31 @@ int main(int argc, char** argv) {
     if (qsgw_dpsion_matrix(nwhis, frhis, niw, freq_i, nwhis, freq_r, 1e10, 0.0,
                            reinterpret_cast<double*>(b.data())) != QSGW_ERR_ARG)   // nw >= nwhis
       return fail("qsgw_dpsion_matrix argument check");
+  }
+  {
+    // host-only: a __Vcoud file written and read back beside this executable
+    const std::string path = std::string(argv[0]) + ".Vcoud.1";
+    const int ngb = 5;
+    const double q[3] = {0.125, -0.25, 0.5};
+    std::vector<double> v(ngb);
+    std::vector<cd> z(static_cast<size_t>(ngb) * ngb);
+    for (int i = 0; i < ngb; ++i) v[i] = 0.5 + i * i;
+    for (size_t i = 0; i < z.size(); ++i) z[i] = cd(std::cos(0.7 * i), std::sin(0.3 * i));
+    if (qsgw_vcoud_write(path.c_str(), ngb, q, v.data(), reinterpret_cast<const double*>(z.data())) != QSGW_OK)
+      return fail("qsgw_vcoud_write");
+    int n = 0;
+    double q2[3];
+    std::vector<double> v2(ngb), vs(ngb);
+    std::vector<cd> z2(z.size());
+    if (qsgw_vcoud_read(path.c_str(), ngb, &n, q2, v2.data(), vs.data(), reinterpret_cast<double*>(z2.data())) !=
+        QSGW_OK)
+      return fail("qsgw_vcoud_read");
+    bool ok = n == ngb && q2[0] == q[0] && q2[1] == q[1] && q2[2] == q[2] && v2 == v && z2 == z;
+    for (int i = 0; i < ngb; ++i) ok = ok && vs[i] == std::sqrt(v[i]);
+    if (!ok) return fail("qsgw_vcoud_read values");
+    if (qsgw_vcoud_read(path.c_str(), ngb - 1, &n, q2, v2.data(), nullptr, nullptr) != QSGW_ERR_ARG)
+      return fail("qsgw_vcoud_read capacity check");
+    std::remove(path.c_str());
   }
   if (argc < 2 || std::strcmp(argv[1], "gpu") != 0) {
     std::printf("OK cpu\n");
