@@ -6,7 +6,10 @@
 // and the corner accumulation of tetwt5x_dtet4 (:304-341, npm = 1, wtet = 1/4):
 //     w(ihis, jb, ib, k) += wtthis(ihis) * pi / (4 voltot)   for each corner k.
 // The reference's sparse (ibjb, ihw, nhw, jhw, whw) storage is replaced by this
-// dense array; its symmetrisation over degenerate bands is not applied.
+// dense array.  Its symmetrisation over degenerate bands (tetwt5.f90:347-423) is
+// the host-only qsgw_tetwt_symmetrize, applied to the host copy of the array
+// that qsgw_x0_lists reads.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 #include "common.cuh"
@@ -298,5 +301,48 @@ extern "C" int qsgw_x0_lists(const double* w, int nk, int nocc, int nunocc, int 
   QSGW_ARG(icount <= 2147483647LL, "x0_lists: %lld weights exceed the int range", icount);
   *ncoun = static_cast<int>(icoun);
   *ncount = static_cast<int>(icount);
+  return QSGW_OK;
+}
+
+// Degenerate groups of chkdgn (tetwt5.f90:868-912): a new group wherever two neighbouring levels
+// differ by more than 1e-4; start[g] .. start[g+1]-1 is group g.
+static void degenerate_groups(const double* e, int n, std::vector<int>& start) {
+  start.clear();
+  if (n < 1) return;
+  start.push_back(0);
+  for (int i = 1; i < n; ++i)
+    if (std::fabs(e[i] - e[i - 1]) > 1e-4) start.push_back(i);
+  start.push_back(n);
+}
+
+extern "C" int qsgw_tetwt_symmetrize(double* w, int nk, int nocc, int nunocc, int nwhis, const double* ek,
+                                     const double* ekq, int nband) {
+  QSGW_ARG(w && ek && ekq && nk >= 1 && nocc >= 0 && nunocc >= 0 && nwhis >= 1 && nband >= nocc && nband >= nunocc,
+           "tetwt_symmetrize: nk=%d nocc=%d nunocc=%d nwhis=%d nband=%d", nk, nocc, nunocc, nwhis, nband);
+  std::vector<int> ga, gb;
+  std::vector<double> acc(nwhis);
+  const size_t pair = static_cast<size_t>(nwhis);
+  for (int k = 0; k < nk; ++k) {
+    degenerate_groups(ek + static_cast<size_t>(nband) * k, nocc, ga);
+    degenerate_groups(ekq + static_cast<size_t>(nband) * k, nunocc, gb);
+    double* wk = w + pair * nunocc * nocc * k;
+    for (size_t a = 0; a + 1 < ga.size(); ++a)
+      for (size_t b = 0; b + 1 < gb.size(); ++b) {
+        const int i0 = ga[a], i1 = ga[a + 1], j0 = gb[b], j1 = gb[b + 1];
+        const int cnt = (i1 - i0) * (j1 - j0);
+        if (cnt == 1) continue;
+        // tetwt5.f90:403-423: the block's histograms summed ib-major, then divided by its size
+        std::fill(acc.begin(), acc.end(), 0.0);
+        for (int ib = i0; ib < i1; ++ib)
+          for (int jb = j0; jb < j1; ++jb) {
+            const double* p = wk + pair * (jb + static_cast<size_t>(nunocc) * ib);
+            for (int h = 0; h < nwhis; ++h) acc[h] = acc[h] + p[h];
+          }
+        for (int h = 0; h < nwhis; ++h) acc[h] = acc[h] / cnt;
+        for (int ib = i0; ib < i1; ++ib)
+          for (int jb = j0; jb < j1; ++jb)
+            std::copy(acc.begin(), acc.end(), wk + pair * (jb + static_cast<size_t>(nunocc) * ib));
+      }
+  }
   return QSGW_OK;
 }

@@ -74,6 +74,7 @@ _SIGS = {
     "qsgw_set_host_async": [c_int],
     "qsgw_x0_lists": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                       c_vp, c_vp, c_vp],
+    "qsgw_tetwt_symmetrize": [c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int],
     "qsgw_dpsion_matrix": [c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_dbl, c_vp],
     "qsgw_dpsion_chiq_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_dbl, c_vp, c_vp],
     "qsgw_get_precision": [c_ip, c_ip],
@@ -584,6 +585,20 @@ def x0_lists(w):
            _p(t["icounkmax"])))
     t["ncoun"], t["ncount"] = nc.value, nt.value
     return t
+
+
+def tetwt_symmetrize(w, ek, ekq):
+    """In place on the host weights w (nk, nocc, nunocc, nwhis) (numpy, the layout of tetwt_hist_d's
+    output): the degenerate-band symmetrisation of tetwt5.f90:347-423; ek, ekq (nk, nband) in Ry."""
+    if not (isinstance(w, np.ndarray) and w.dtype == np.float64 and w.flags.c_contiguous and w.ndim == 4):
+        raise ValueError("w must be a C-contiguous float64 array (nk, nocc, nunocc, nwhis)")
+    a = np.ascontiguousarray(np.asarray(ek, dtype=np.float64))
+    b = np.ascontiguousarray(np.asarray(ekq, dtype=np.float64))
+    nk, nocc, nunocc, nwhis = w.shape
+    if a.shape != b.shape or a.shape[0] != nk:
+        raise ValueError(f"ek {a.shape} / ekq {b.shape} must both be (nk={nk}, nband)")
+    _chk(load().qsgw_tetwt_symmetrize(_p(w), nk, nocc, nunocc, nwhis, _p(a), _p(b), a.shape[1]))
+    return w
 
 
 def tetwt_hist_d(w, idtet, qbzw, ek, ekq, efermi, frhis, nocc, nunocc):

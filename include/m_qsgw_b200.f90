@@ -69,6 +69,14 @@ module m_qsgw_b200
       real(c_double), intent(in) :: freq_i(*), eocc(*), eunocc(*)
       integer(c_int), intent(in) :: nocc(*), nun(*)
     end function
+    ! degenerate-band averaging of the dense tetrahedron weights (host arrays, in place)
+    integer(c_int) function qsgw_tetwt_symmetrize(w, nk, nocc, nunocc, nwhis, ek, ekq, nband) &
+         bind(C, name='qsgw_tetwt_symmetrize')
+      import :: c_int, c_double
+      real(c_double), intent(inout) :: w(*)
+      integer(c_int), value :: nk, nocc, nunocc, nwhis, nband
+      real(c_double), intent(in) :: ek(*), ekq(*)
+    end function
     ! x0gemm pair/bin lists from dense tetrahedron weights (host arrays, no GPU needed)
     integer(c_int) function qsgw_x0_lists(w, nk, nocc, nunocc, nwhis, job, ncoun, ncount, itc, itpc, jpmc, &
          iwini, iwend, icouini, whwc, icounkmin, icounkmax) bind(C, name='qsgw_x0_lists')

@@ -402,11 +402,22 @@ int qsgw_zminv_batched_d(double *a, int n, int lda, int nbatch);
  * whose excitation energies leave the histogram sets the status word
  * (qsgw_synchronize returns QSGW_ERR_NUMERIC); the reference stops there.
  * Dense output instead of the reference's (ibjb, ihw, nhw, jhw, whw)
- * storage; its symmetrisation over degenerate bands is not applied.       */
+ * storage; its symmetrisation over degenerate bands is
+ * qsgw_tetwt_symmetrize below.                                             */
 int qsgw_tetwt_hist_d(double *w_d, int nk, int nocc, int nunocc, int nwhis,
                       const int *idtet, int ntet, const double *qbzw,
                       const double *ek, const double *ekq, int nband,
                       double efermi, const double *frhis, double *voltot);
+/* The reference's symmetrisation over degenerate bands (tetwt5.f90:347-423,
+ * job 1, npm = 1, no core states) on the host copy of those weights (w:
+ * nwhis x nunocc x nocc x nk, in place): for every k, the levels ek(1:nocc, k)
+ * and ekq(1:nunocc, k) (nband x nk, Ry) are cut into groups wherever two
+ * neighbours differ by more than 1e-4 (chkdgn, :868-912), and every (ib, jb)
+ * of a group pair gets the pair's mean histogram (summed ib-major, divided
+ * by the group-pair size, as the reference).  A group cut by nocc or nunocc
+ * is averaged over its members inside the array.  Host-only.              */
+int qsgw_tetwt_symmetrize(double *w, int nk, int nocc, int nunocc, int nwhis,
+                          const double *ek, const double *ekq, int nband);
 /* Pair/bin lists of qsgw_x0gemm from those weights copied to the host
  * (w: nwhis x nunocc x nocc x nk): the index accumulation of X0kf_v4hz_init
  * (x0kf_v4h.f90:48-142), npm = 1, no core states, no cRPA.  A pair with any

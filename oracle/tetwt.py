@@ -189,3 +189,41 @@ def tetwt_hist(idtet, qbzw, ek, ekq, efermi, frhis, nocc, nunocc):
                 for c in range(4):
                     w[kk[c], ib, jb] += wt * f
     return w, voltot
+
+
+def chkdgn(ene, epsx=1e-4):
+    """tetwt5.f90:868-912: groups of consecutive levels, a new group wherever
+    |ene(i) - ene(i-1)| > epsx; returns (first, last) pairs, 0-based inclusive."""
+    n = len(ene)
+    if n < 1:
+        return []
+    groups, first = [], 0
+    for i in range(1, n):
+        if abs(ene[i] - ene[i - 1]) > epsx:
+            groups.append((first, i - 1))
+            first = i
+    groups.append((first, n - 1))
+    return groups
+
+
+def symmetrize_degenerate(w, ek, ekq, epsx=1e-4):
+    """tetwt5.f90:347-423, job 1, npm = 1, no core states, on the dense
+    w[k, ib, jb, ihis] of tetwt_hist: for every k, every degenerate group of
+    ek[k, :nocc] and every one of ekq[k, :nunocc], each (ib, jb) of the block
+    gets the block's mean histogram, summed ib-major, jb-minor and divided by
+    the block size as the reference does.  Returns a new array."""
+    w = np.array(w, dtype=np.float64, copy=True)
+    nk, nocc, nunocc, _ = w.shape
+    for k in range(nk):
+        for (i0, i1) in chkdgn(ek[k, :nocc], epsx):
+            for (j0, j1) in chkdgn(ekq[k, :nunocc], epsx):
+                cnt = (i1 - i0 + 1) * (j1 - j0 + 1)
+                if cnt == 1:
+                    continue
+                acc = np.zeros(w.shape[3])
+                for ib in range(i0, i1 + 1):
+                    for jb in range(j0, j1 + 1):
+                        acc = acc + w[k, ib, jb]
+                acc = acc / cnt
+                w[k, i0:i1 + 1, j0:j1 + 1] = acc
+    return w
