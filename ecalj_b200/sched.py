@@ -24,6 +24,16 @@ def _weavx2(e1, e2, ek, esmr):
                                                + np.exp(-(el - ek) ** 2 / sig2)) / wtt
 
 
+def _wfac_levels(omg, ef, e, it, nctot, esmr):
+    """wfacx2(omg, ef, e, esmrx) per level (wfacx.f90:19-36): core levels (it <= nctot) take
+    esmrx = 0, the sharp window el <= e < eh; both vanish when |omg - ef| < 1e-6."""
+    el, eh = min(omg, ef), max(omg, ef)
+    if eh - el < 1e-6:
+        return np.zeros(len(e))
+    sharp = ((el <= e) & (e < eh)).astype(float)
+    return np.where(it <= nctot, sharp, _wfacx2(omg, ef, e, esmr))
+
+
 def nt0pm(ekc, ef, esmr):
     ekc = np.asarray(ekc)
     return int(np.sum(ekc < ef + DDW * esmr)), int(np.sum(ekc < ef - DDW * esmr))
@@ -42,10 +52,7 @@ def get_nwx(omega, ekc, freq_r, ef, esmr, nctot=0, nstate=None):
             continue
         it = np.arange(lo, hi + 1)
         e = ekc[it - 1]
-        es = np.where(it <= nctot, 0.0, esmr)
-        wf = np.where(es == 0.0, ((np.minimum(omg, ef) <= e) & (e < np.maximum(omg, ef))).astype(float),
-                      _wfacx2(omg, ef, e, np.where(es == 0.0, 1.0, es)))
-        keep = wf >= WFACCUT
+        keep = _wfac_levels(omg, ef, e, it, nctot, esmr) >= WFACCUT
         if not np.any(keep):
             continue
         we = np.abs(0.5 * (_weavx2(omg, ef, e[keep], esmr) - omg))
@@ -84,8 +91,7 @@ def pole_bins(omega, ekc, freq_r, ef, esmr, nwxi, nwx, ns2r, nm, ntq, ns1=1, nct
             continue
         it = np.arange(itini, itend + 1)
         e = ekc[it - 1]
-        wf = _wfacx2(omg, ef, e, esmr)
-        keep = wf >= WFACCUT
+        keep = _wfac_levels(omg, ef, e, it, nctot, esmr) >= WFACCUT
         we = 0.5 * np.abs(omg - _weavx2(omg, ef, e[keep], esmr))
         ixs = np.searchsorted(fr[1:nw + 1], we, side='right') + 1
         for i, x in zip(it[keep], ixs):
