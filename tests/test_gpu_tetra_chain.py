@@ -6,7 +6,8 @@ chain with the dense contraction in place of the lists: with the same
 weights, lists + x0gemm + Hilbert transform to relative Frobenius <= 1e-11;
 with the oracle's own weights to <= 1e-10 (the weights agree to ~3e-12, and
 the real-axis chi0 takes single bins, Im part included, without smoothing);
-and chi0(i w) Hermitian negative semidefinite."""
+and chi0(i w) Hermitian negative semidefinite.  The same with bands that
+touch at some k, the weights symmetrised over the degenerate bands."""
 import numpy as np
 import pytest
 
@@ -19,8 +20,22 @@ pytestmark = pytest.mark.gpu
 
 
 def test_tetra_chain_vs_oracle(qsgw):
+    _chain(qsgw, degenerate=False)
+
+
+def test_tetra_chain_degenerate_bands(qsgw):
+    """Bands that touch at some k: the host copy of the GPU weights is
+    symmetrised (qsgw_tetwt_symmetrize) before the lists are built, as
+    tetwt5x_dtet4 does; the oracle chain symmetrises its own weights."""
+    _chain(qsgw, degenerate=True)
+
+
+def _chain(qsgw, degenerate):
     import torch
     idt, qbzw, ek, ekq = synth.tetra_mesh(3)
+    if degenerate:
+        ek[::3, 2] = ek[::3, 1] + 2e-5                  # occupied bands 1, 2 touch at every third k
+        ekq[::2, 4] = ekq[::2, 3]                       # bands 3, 4 at k+q at every second k
     nocc, nunocc, ef, npr = 3, 6, 0.0, 24
     frhis = 1e-3 / 0.08 * (np.exp(0.08 * np.arange(61)) - 1.0)
     nwhis = len(frhis) - 1
@@ -37,6 +52,11 @@ def test_tetra_chain_vs_oracle(qsgw):
     qsgw.tetwt_hist_d(wd, idt, qbzw, ek, ekq, ef, frhis, nocc, nunocc)
     qsgw.synchronize()
     w = wd.cpu().numpy().reshape(nk, nocc, nunocc, nwhis)
+    if degenerate:
+        raw = w.copy()
+        w = qsgw.tetwt_symmetrize(w.copy(), ek, ekq)
+        assert np.array_equal(w, tw.symmetrize_degenerate(raw, ek, ekq))
+        assert not np.array_equal(w, raw)
     t = qsgw.x0_lists(w)
     rcxq = torch.zeros(npr * npr * (nwhis + 1), dtype=torch.complex128, device='cuda')
     for k in range(nk):
@@ -62,6 +82,8 @@ def test_tetra_chain_vs_oracle(qsgw):
     assert rel_fro(gi, ri) < 1e-11
     assert rel_fro(gr, rr) < 1e-11
     wref, _ = tw.tetwt_hist(idt, qbzw, ek, ekq, ef, frhis, nocc, nunocc)
+    if degenerate:
+        wref = tw.symmetrize_degenerate(wref, ek, ekq)
     ri, rr = oracle_chain(wref)                                  # the oracle's weights
     print(f"tetra chain, oracle weights: imag {rel_fro(gi, ri):.2e} real {rel_fro(gr, rr):.2e}")
     assert rel_fro(gi, ri) < 1e-10
