@@ -112,7 +112,7 @@ def dist_setup():
 # ----------------------------------------------------------------------------- workload
 def chi0_config(nk=None):
     from ecalj_b200 import synth
-    c = dict(synth.CONFIGS["c1"])
+    c = dict(synth.CONFIGS["chi0_n600"])
     if nk:
         c["nk"] = nk
     rng = np.random.default_rng(c["seed"])
@@ -126,7 +126,7 @@ def chi0_config(nk=None):
 
 def sigc_config():
     from ecalj_b200 import synth
-    return dict(synth.CONFIGS["c2"])
+    return dict(synth.CONFIGS["sigc_n600"])
 
 
 def device_normal_c128(n, seed, scale):
@@ -139,8 +139,8 @@ def device_normal_c128(n, seed, scale):
 
 
 def build_sigc_inputs(lib, c, log):
-    """W_c(q, iw) for every q from this library's chi0 -> W path (c0-style
-    pair model at N=600, iw = 0 plus the 24 Gauss-Legendre points), a real-axis
+    """W_c(q, iw) for every q from this library's chi0 -> W path (the N=260
+    pair model scaled to N=600, iw = 0 plus the 24 Gauss-Legendre points), a real-axis
     model on the 50-point mesh, and zmel per task.  All device-resident."""
     import torch
     from ecalj_b200 import synth
@@ -218,34 +218,34 @@ def reference_arm(args, ws, rank):
     from threadpoolctl import threadpool_info
     from oracle import sxcf as osx
     from ecalj_b200 import synth
-    c1 = chi0_config()
-    N, niw = c1["N"], c1["niw"]
+    cfg_chi = chi0_config()
+    N, niw = cfg_chi["N"], cfg_chi["niw"]
     rng = np.random.default_rng(1)
     P_s = 3000
     z = synth.zmel_columns(rng, N, P_s)
     de = rng.uniform(0.025, 2.0, P_s)
-    w = -2.0 * de[:, None] / (de[:, None] ** 2 + c1["freq_i"][None, :] ** 2) / c1["nk"]
-    c2 = sigc_config()
+    w = -2.0 * de[:, None] / (de[:, None] ** 2 + cfg_chi["freq_i"][None, :] ** 2) / cfg_chi["nk"]
+    cfg_sig = sigc_config()
     nm_s = 100
-    t = synth.sigc_task(c2["N"], c2["ntq"], nm_s, c2["niw"], c2["nreal"], seed=5, esmr=0.01, ef=0.0)
-    wi = synth.zmel_columns(rng, N, N * (c2["niw"] + 1)).reshape(N, N, c2["niw"] + 1, order="F") * 0.01
+    t = synth.sigc_task(cfg_sig["N"], cfg_sig["ntq"], nm_s, cfg_sig["niw"], cfg_sig["nreal"], seed=5, esmr=0.01, ef=0.0)
+    wi = synth.zmel_columns(rng, N, N * (cfg_sig["niw"] + 1)).reshape(N, N, cfg_sig["niw"] + 1, order="F") * 0.01
     wr = synth.real_axis_model(wi[:, :, 0], t["freq_r"])
     nt0p, nt0m = osx.nt0pm(t["ekc"], t["ef"], t["esmr"])
-    nwxi, nwx, ntmax = osx.get_nwx(t["omega"], c2["ntq"], nt0p, nt0m, nm_s, t["freq_r"], t["esmr"], t["ef"],
+    nwxi, nwx, ntmax = osx.get_nwx(t["omega"], cfg_sig["ntq"], nt0p, nt0m, nm_s, t["freq_r"], t["esmr"], t["ef"],
                                    t["ekc"], 0)
     fl_chi = 8.0 * N * N * P_s * niw
-    npole = len(osx.pole_table(t["omega"], t["ekc"], 0, 1, min(nm_s, ntmax), c2["ntq"], t["ef"], t["esmr"],
+    npole = len(osx.pole_table(t["omega"], t["ekc"], 0, 1, min(nm_s, ntmax), cfg_sig["ntq"], t["ef"], t["esmr"],
                                1.0, t["freq_r"]))
-    fl_sig = 8.0 * N * N * nm_s * c2["ntq"] * (c2["niw"] + 1) + 8.0 * N * N * 3 * npole \
-        + 8.0 * c2["ntq"] ** 2 * N * nm_s
+    fl_sig = 8.0 * N * N * nm_s * cfg_sig["ntq"] * (cfg_sig["niw"] + 1) + 8.0 * N * N * 3 * npole \
+        + 8.0 * cfg_sig["ntq"] ** 2 * N * nm_s
 
     def step():
         acc = np.zeros((N, N), complex)
         zh = z.conj().T.copy()
         for iw in range(niw):                       # x0gemm: one ZGEMM per bin
             acc += zh.T @ (z.T * w[:, iw:iw + 1])
-        zs = np.zeros((c2["ntq"], c2["ntq"]), complex, order="F")
-        osx.correlation_block(zs, t["zmel"], 1, nm_s, min(nm_s, ntmax), nwxi, nwx, c2["ntq"], wi, wr, t["omega"],
+        zs = np.zeros((cfg_sig["ntq"], cfg_sig["ntq"]), complex, order="F")
+        osx.correlation_block(zs, t["zmel"], 1, nm_s, min(nm_s, ntmax), nwxi, nwx, cfg_sig["ntq"], wi, wr, t["omega"],
                               t["ekc"], 0, t["ef"], t["esmr"], 1.0, t["ua"], t["x"], t["wx"], t["expa"], t["freq_r"])
         return acc, zs
 
@@ -257,13 +257,14 @@ def reference_arm(args, ws, rank):
     dt = (time.perf_counter() - t0) / args.steps
     gf = (fl_chi + fl_sig) / dt / 1e9
     threads = max([d.get("num_threads", 1) for d in threadpool_info()] + [1])
-    sample = (f"chi0 {P_s} of {c1['npair']} pairs x {niw} iw at N={N}; Sigma_c 1 task with {nm_s} of "
-              f"{c2['nm']} intermediate states x {c2['ntq']} targets, {c2['niw']}+1 iw, {npole} pole columns")
+    sample = (f"chi0 {P_s} of {cfg_chi['npair']} pairs x {niw} iw at N={N}; Sigma_c 1 task with {nm_s} of "
+              f"{cfg_sig['nm']} intermediate states x {cfg_sig['ntq']} targets, {cfg_sig['niw']}+1 iw, "
+              f"{npole} pole columns")
     cpu = {"value": round(gf, 3), "unit": "GFLOP/s", "cores": threads, "kind": "port", "sample": sample}
     line = {"metric": METRIC, "value": round(gf, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": "c1 chi0 + c2 Sigma_c (bounded CPU sample)", "sample": sample},
+            "config": {"workload": "chi0 N=600 + Sigma_c N=600 (bounded CPU sample)", "sample": sample},
             "impl": "reference", "cpu_baseline": cpu,
             "e2e": {"value": round(gf, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -309,23 +310,24 @@ def main():
 
     # ---- workload set-up (untimed)
     lib.set_precision(lib.PREC_FP64)
-    c1 = chi0_config(args.nk)
-    N, niw = c1["N"], c1["niw"]
-    zc = device_normal_c128(N * c1["npair"], c1["seed"], 1.0 / math.sqrt(N))
+    cfg_chi = chi0_config(args.nk)
+    N, niw = cfg_chi["N"], cfg_chi["niw"]
+    zc = device_normal_c128(N * cfg_chi["npair"], cfg_chi["seed"], 1.0 / math.sqrt(N))
     chi = torch.zeros(N * N * niw, dtype=torch.complex128, device="cuda")
-    c2 = sigc_config()
+    cfg_sig = sigc_config()
     if args.nq:
-        c2["nq"] = args.nq
-    s = build_sigc_inputs(lib, c2, log)
+        cfg_sig["nq"] = args.nq
+    s = build_sigc_inputs(lib, cfg_sig, log)
     for t in s["tasks"]:
         t["zsec"] = torch.zeros(s["ntq"] * s["ntq"], dtype=torch.complex128, device="cuda")
-    fl_chi = 8.0 * N * N * c1["npair"] * niw
+    fl_chi = 8.0 * N * N * cfg_chi["npair"] * niw
     fl_sig, fl_sig_seg = sigc_flops(lib, s)
     flops = fl_chi + fl_sig
 
     def step():
-        lib.chi0_lorentz_d(chi, N, niw, c1["freq_i"], c1["nk"], c1["nocc"], c1["nun"], c1["eocc_h"],
-                           c1["eun_h"], zc)
+        lib.chi0_lorentz_d(chi, N, niw, cfg_chi["freq_i"], cfg_chi["nk"], cfg_chi["nocc"], cfg_chi["nun"],
+                           cfg_chi["eocc_h"],
+                           cfg_chi["eun_h"], zc)
         for t in s["tasks"]:
             t["zsec"].zero_()
         run_sigc(lib, s)
@@ -436,7 +438,7 @@ def main():
     e2e = None
     if not args.no_e2e:
         lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
-        e2e = run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist)
+        e2e = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist)
     sur = None
     if not args.no_surrogate:
         lib.set_autotune(0, None)          # no tuning trials inside the study's timed calls
@@ -450,8 +452,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "c128" if prec == "fp64" else "c128 via split-f16",
                 "data": "synthetic",
-                "config": {"workload": f"c1 chi0 (N=600, nk={c1['nk']}, nocc=9, nunocc U{{100..300}}, 24 iw, "
-                                       f"{c1['npair']} pairs) + c2 Sigma_c ({len(s['tasks'])} tasks, N=600, "
+                "config": {"workload": f"chi0 (N=600, nk={cfg_chi['nk']}, nocc=9, nunocc U{{100..300}}, 24 iw, "
+                                       f"{cfg_chi['npair']} pairs) + Sigma_c ({len(s['tasks'])} tasks, N=600, "
                                        "40x400 states, 24+1 iw, 50-point real mesh)",
                            "precision": prec, "parallelism": f"replicas x{ws}",
                            "execution": "CUDA graph replay" if not args.no_graph else "eager calls",
@@ -476,7 +478,8 @@ def surrogate_summary(lib, log, nq_test=8):
     res = surrogate.study(N=600, nq_train=48, nq_test=nq_test, precision="split", log=log)
     rows = res["rows"]
     mean = lambda k: float(np.mean([r[k] for r in rows]))
-    out = {"workload": "c3: exact W_c on 48 iw x 48 training q at N=600, 8 anchors, 8 held-out, 32 predicted; "
+    out = {"workload": "W_c interpolation: exact W_c on 48 iw x 48 training q at N=600, 8 anchors, 8 held-out, "
+                       "32 predicted; "
                        f"{nq_test} test q",
            "ms_w_plain_fp64": round(mean("ms_plain_fp64"), 3), "ms_w_plain_split": round(mean("ms_plain"), 3),
            "ms_w_surrogate": round(mean("ms_surrogate"), 3),
@@ -517,13 +520,13 @@ def measure_fp64_peak():
     return best
 
 
-def run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist):
+def run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist):
     """Same step through the host-pointer C-ABI entry points: every step copies
     its inputs from pinned host memory and reads the results back.  The calls
     run in the library's asynchronous host mode (each returns once enqueued,
     so one call's copies overlap the previous call's kernels) and every step
     ends with qsgw_synchronize, after which its outputs are on the host."""
-    N, niw = c1["N"], c1["niw"]
+    N, niw = cfg_chi["N"], cfg_chi["niw"]
     zc_h = torch.empty(zc.numel(), dtype=torch.complex128, pin_memory=True)
     zc_h.copy_(zc)
     chi_h = torch.empty(N * N * niw, dtype=torch.complex128, pin_memory=True)
@@ -551,8 +554,9 @@ def run_e2e(lib, torch, c1, zc, s, args, flops, ws, dist):
     def step():
         for d in host["tasks"]:
             d["zsec"][:] = 0
-        lib.chi0_lorentz_d(chi_np, N, niw, c1["freq_i"], c1["nk"], c1["nocc"], c1["nun"], c1["eocc_h"],
-                           c1["eun_h"], zc_np, host=True)
+        lib.chi0_lorentz_d(chi_np, N, niw, cfg_chi["freq_i"], cfg_chi["nk"], cfg_chi["nocc"], cfg_chi["nun"],
+                           cfg_chi["eocc_h"],
+                           cfg_chi["eun_h"], zc_np, host=True)
         run_sigc(lib, s, host=host)
         lib.synchronize()
 

@@ -13,14 +13,14 @@ import numpy as np
 
 CONFIGS = {
     # plain FP64 chi0 + W, Si-diamond-like size
-    "c0": dict(N=260, nk=64, nocc=4, nun=(40, 60), niw=12, seed=20260),
+    "chi0_w_n260": dict(N=260, nk=64, nocc=4, nun=(40, 60), niw=12, seed=20260),
     # split chi0, GaAs-like shape
-    "c1": dict(N=600, nk=216, nocc=9, nun=(100, 300), niw=24, seed=20261),
+    "chi0_n600": dict(N=600, nk=216, nocc=9, nun=(100, 300), niw=24, seed=20261),
     # Sigma_c band sum
-    "c2": dict(N=600, nq=64, niw=24, ntq=40, nm=400, nreal=50, seed=20262,
+    "sigc_n600": dict(N=600, nq=64, niw=24, ntq=40, nm=400, nreal=50, seed=20262,
                chi_nk=64, chi_nocc=4, chi_nun=(40, 60)),
     # all-in: zmel of all k is 369 GB, so it is streamed through the GPU k by k
-    "c4": dict(N=1500, nk=512, nocc=40, nun=(300, 1200), niw=32, seed=20264),
+    "chi0_n1500_streamed": dict(N=1500, nk=512, nocc=40, nun=(300, 1200), niw=32, seed=20264),
 }
 
 

@@ -182,7 +182,8 @@ int qsgw_chi0_lorentz_d(double *chi0_d, int npr, int niw, const double *freq_i,
 /* The same chi0 added into chi0_d (not cleared) for a batch of nkb k-points
  * of an nk_total mesh (weights carry 1/nk_total): calling it once per batch
  * streams the zmel columns through the GPU when all k cannot be resident
- * (configuration c4, N = 1500: 369 GB of zmel).  No autotuning trials.     */
+ * (N = 1500 with 512 k and up to 48 000 pairs per k: 369 GB of zmel).  No
+ * autotuning trials.                                                       */
 int qsgw_chi0_lorentz_acc_d(double *chi0_d, int npr, int niw, const double *freq_i,
                             int nk_total, int nkb, const int *nocc, const int *nun,
                             const double *eocc, const double *eunocc,

@@ -1,4 +1,4 @@
-"""Configuration c4 (N = 1500, nocc = 40, nunocc U{300..1200}, 32 iw): its zmel
+"""chi0 at N = 1500 (nk = 512, nocc = 40, nunocc U{300..1200}, 32 iw): its zmel
 cannot be resident (369 GB for 512 k), so chi0 is accumulated k by k with
 qsgw_chi0_lorentz_acc_d.  Four k-points of the 512-point mesh are streamed one
 at a time and compared with one call over the same four k (FP64), in FP64 and
@@ -14,10 +14,10 @@ from tests.conftest import rel_fro
 pytestmark = pytest.mark.gpu
 
 
-def test_c4_streamed_chi0(qsgw):
+def test_n1500_streamed_chi0(qsgw):
     import torch
     lib = qsgw
-    c = synth.CONFIGS["c4"]
+    c = synth.CONFIGS["chi0_n1500_streamed"]
     N, niw, nkb = c["N"], c["niw"], 4
     rng = np.random.default_rng(c["seed"])
     nocc, nun, eocc, eun = synth.chi0_spectrum(rng, nkb, c["nocc"], c["nun"])

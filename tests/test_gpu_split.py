@@ -24,11 +24,11 @@ def split(qsgw):
     qsgw.set_precision(qsgw.PREC_FP64, 1)
 
 
-@pytest.mark.parametrize("cfg", ["small", "odd", "c0"])
+@pytest.mark.parametrize("cfg", ["small", "odd", "n260"])
 def test_chi0_split_vs_oracle(split, cfg):
     import torch
-    if cfg == "c0":
-        c = synth.CONFIGS["c0"]
+    if cfg == "n260":
+        c = synth.CONFIGS["chi0_w_n260"]
         p = synth.chi0_problem(c['N'], c['nk'], c['nocc'], c['nun'], c['niw'], c['seed'])
     elif cfg == "odd":
         p = synth.chi0_problem(N=131, nk=3, nocc=5, nun=(11, 29), niw=7, seed=8)
