@@ -94,6 +94,39 @@ def freq_r_mesh(nreal, wmax=2.0):
     return fr
 
 
+def getfreq(omg2max, wemax, oratio=1.03, dw=1e-5, epsmode=False):
+    """The histogram bins and the real-axis mesh of Getfreq (m_freq.f90:94-133),
+    Hartree: aa = HistBin_ratio - 1, bb = HistBin_dw / aa; nwhis = (the first
+    iw with bb (exp(aa (iw-1)) - 1) > omg2max + 1e-6) + 2; frhis(iw) =
+    bb (exp(aa (iw-1)) - 1), iw = 1..nwhis+1; nw = the first iw >= 3 with
+    (frhis(iw-2) + frhis(iw-1))/2 > wemax/2, at most nwhis - 1 (nwhis - 1
+    in epsmode); freq_r(0) = 0, freq_r(i) = (frhis(i) + frhis(i+1))/2.
+    Returns dict(frhis (nwhis+1), freq_r (nw+1), nwhis, nw)."""
+    aa = oratio - 1.0
+    bb = dw / aa
+    iw = 0
+    while True:
+        iw += 1
+        if bb * (math.exp(aa * (iw - 1)) - 1.0) > omg2max + 1e-6:
+            break
+    nwhis = iw + 2
+    frhis = bb * (np.exp(aa * np.arange(nwhis + 1)) - 1.0)        # frhis(1..nwhis+1), 0-based here
+    nw = None
+    for iw in range(3, nwhis + 1):
+        if 0.5 * (frhis[iw - 3] + frhis[iw - 2]) > wemax / 2.0:
+            nw = iw
+            break
+    if epsmode:
+        nw = nwhis - 1
+    elif nw is None:
+        raise ValueError("getfreq: wemax/2 beyond the histogram (the reference leaves nw unset)")
+    else:
+        nw = min(nw, nwhis - 1)
+    freq_r = np.zeros(nw + 1)
+    freq_r[1:] = 0.5 * (frhis[:nw] + frhis[1:nw + 1])
+    return dict(frhis=frhis, freq_r=freq_r, nwhis=nwhis, nw=nw)
+
+
 def sigc_task(N, ntq, nm, niw, nreal, seed, nctot=0, esmr=0.01, ef=0.0):
     """Energies and zmel of one Sigma_c task (Ry).  Target energies
     omega = eq(1:ntq) in [-1, 1] Ry; intermediate energies U[-1, 4] Ry."""
