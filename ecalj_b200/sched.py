@@ -1,8 +1,12 @@
-"""Sigma_c task scheduling on the host: the real-axis window and pole-state
-bounds of ``get_nwx`` (sxcf_fal2_count.sc.f90:238-298) and the pole-entry
-census the library's correlation kernel will use (m_sxcf_gemm.f90:511-552).
-Vectorised numpy; energies in Ry, we in Hartree.
+"""Sigma task scheduling on the host, as sxcf_scz_count prepares it: the task
+list over (kx, irot, ip, isp) with its middle-state batches and their size
+from the memory budget (sxcf_fal2_count.sc.f90:86-230), the real-axis window
+and pole-state bounds of ``get_nwx`` (:238-298), and the pole-entry census the
+library's correlation kernel will use (m_sxcf_gemm.f90:511-552).  Vectorised
+numpy; energies in Ry, we in Hartree.
 """
+import math
+
 import numpy as np
 from scipy.special import erfc
 
@@ -98,3 +102,54 @@ def pole_bins(omega, ekc, freq_r, ef, esmr, nwxi, nwx, ns2r, nm, ntq, ns1=1, nct
             ent.append(((i - ns1) + nm * (itp - 1), int(x)))
     recs = sorted({x - 1 + j for _, x in ent for j in range(3) if nwxi <= x - 1 + j <= nwx})
     return ent, recs
+
+
+def nmbatch_size(nstatemax_max, mmax_gb, ngcgp, nbandmx_max, nbloch, ngcmx):
+    """Middle states per batch from the MEMnmbatch budget (GWinput, GB; default 2),
+    sxcf_fal2_count.sc.f90:130-141: the budget less 16 ngcgp max(nbandmx) bytes,
+    over max(nbandmx) (nbloch + 2 ngcmx) complex(8), at most max(nstatemax)."""
+    k3 = 1000.0 ** 3
+    mmm = max(mmax_gb - 16.0 * (ngcgp * nbandmx_max) / k3, 0.0)
+    n = math.floor(min(nstatemax_max + 1e-8, mmm * k3 / (nbandmx_max * (nbloch + ngcmx + ngcmx) * 16) + 1e-8))
+    if n == 0:
+        raise ValueError("nmbatch = 0: the MEMnmbatch budget is too small")
+    return n
+
+
+def middle_batches(nnn, nmbatch):
+    """The [nstti, nstte] ranges (1-based, inclusive) that cut nnn middle states
+    into max((nnn-1)/nmbatch + 1, 1) nearly equal batches, the first nnn mod ndiv
+    of them one state larger (sxcf_fal2_count.sc.f90:147-159)."""
+    ndiv = max(int((nnn - 1) / nmbatch) + 1, 1)          # Fortran division truncates toward zero
+    nloadav = nnn // ndiv
+    nrem = nnn - ndiv * nloadav
+    nload = [nloadav + 1] * nrem + [nloadav] * (ndiv - nrem)
+    ends = np.cumsum(nload)
+    return [(int(e - n + 1), int(e)) for n, e in zip(nload, ends)]
+
+
+def sigma_tasks(irkip, nstatemax, nmbatch):
+    """The icount list of sxcf_scz_count (sxcf_fal2_count.sc.f90:86-230): every
+    nonzero irkip(isp, kx, irot, ip) (a numpy array of that Fortran index order,
+    0-based here) in the loop order kx, irot, ip, isp, each cut into its
+    middle-state batches.  nstatemax(isp, kx, irot, ip, kr) gives the middle-state
+    count of a task (nt0p for exchange, nctot + min(nband, ...) for correlation).
+    Returns dicts with 1-based isp, kx, irot, ip, kr, nstti, nstte."""
+    irkip = np.asarray(irkip)
+    nspin, nqibz, ngrp, nqip = irkip.shape
+    tasks = []
+    for kx in range(nqibz):
+        if not irkip[:, kx].any():
+            continue
+        for irot in range(ngrp):
+            if not irkip[:, kx, irot].any():
+                continue
+            for ip in range(nqip):
+                for isp in range(nspin):
+                    kr = int(irkip[isp, kx, irot, ip])
+                    if kr == 0:
+                        continue
+                    nnn = nstatemax(isp + 1, kx + 1, irot + 1, ip + 1, kr)
+                    for (a, b) in middle_batches(nnn, nmbatch):
+                        tasks.append(dict(isp=isp + 1, kx=kx + 1, irot=irot + 1, ip=ip + 1, kr=kr, nstti=a, nstte=b))
+    return tasks

@@ -49,3 +49,45 @@ def test_pole_bins_match_oracle_entries(seed, nctot):
     assert recs == want
     if nctot:
         assert any(it <= nctot for it, _, _, _ in ref)      # the core window was exercised
+
+
+@pytest.mark.parametrize("nnn,nmb", [(0, 5), (1, 5), (5, 5), (6, 5), (17, 5), (400, 64), (400, 400), (401, 400)])
+def test_middle_batches(nnn, nmb):
+    b = sched.middle_batches(nnn, nmb)
+    ndiv = max((nnn - 1) // nmb + 1, 1) if nnn >= 1 else 1
+    assert len(b) == ndiv
+    sizes = [e - s + 1 for s, e in b]
+    assert sum(sizes) == nnn and max(sizes) <= max(nmb, 1) and max(sizes) - min(sizes) <= 1
+    assert sizes == sorted(sizes, reverse=True)                 # the remainder goes to the first batches
+    assert b[0][0] == 1 and all(b[i + 1][0] == b[i][1] + 1 for i in range(len(b) - 1))
+
+
+def test_middle_batches_known():
+    assert sched.middle_batches(17, 5) == [(1, 5), (6, 9), (10, 13), (14, 17)]
+    assert sched.middle_batches(0, 5) == [(1, 0)]               # one empty batch, as the reference keeps
+
+
+def test_nmbatch_size():
+    # 2 GB less 16 * 3000 * 60 bytes, over 60 * (500 + 2 * 800) * 16 bytes per state
+    n = sched.nmbatch_size(400, 2.0, 3000, 60, 500, 800)
+    assert n == min(400, int((2.0e9 - 16 * 3000 * 60) / (60 * 2100 * 16)))
+    assert sched.nmbatch_size(50, 2.0, 3000, 60, 500, 800) == 50
+    with pytest.raises(ValueError):
+        sched.nmbatch_size(400, 1e-6, 3000, 60, 500, 800)
+
+
+def test_sigma_task_order():
+    """Loop order kx, irot, ip, isp over the nonzero irkip, each task cut into batches."""
+    irkip = np.zeros((2, 3, 2, 3), int)             # (isp, kx, irot, ip)
+    irkip[0, 0, 0, 1] = 4
+    irkip[1, 0, 0, 1] = 4
+    irkip[0, 0, 1, 0] = 7
+    irkip[1, 2, 0, 2] = 9
+    t = sched.sigma_tasks(irkip, lambda isp, kx, irot, ip, kr: 10 * kr % 13 + 1, 4)
+    keys = [(d['kx'], d['irot'], d['ip'], d['isp']) for d in t]
+    order = [(1, 1, 2, 1), (1, 1, 2, 2), (1, 2, 1, 1), (3, 1, 3, 2)]
+    assert sorted(set(keys), key=keys.index) == order
+    for d in t:
+        n = 10 * d['kr'] % 13 + 1
+        assert 1 <= d['nstti'] <= d['nstte'] <= n
+    assert len([d for d in t if d['kr'] == 7]) == len(sched.middle_batches(10 * 7 % 13 + 1, 4))
