@@ -48,6 +48,19 @@ class SeqFile {
     return QSGW_OK;
   }
 
+  // The file must hold exactly `want` bytes (the layout its header implies), checked before
+  // a caller sizes arrays from that header.
+  int check_length(const char* what, long double want) {
+    const long here = std::ftell(f_);
+    QSGW_ARG(here >= 0 && std::fseek(f_, 0, SEEK_END) == 0, "%s: %s: cannot seek", what, path_);
+    const long total = std::ftell(f_);
+    QSGW_ARG(std::fseek(f_, here, SEEK_SET) == 0, "%s: %s: cannot seek", what, path_);
+    QSGW_ARG(static_cast<long double>(total) == want,
+             "%s: %s holds %ld bytes, its header implies %.0Lf (not a file of this layout, or cut short)", what,
+             path_, total, want);
+    return QSGW_OK;
+  }
+
   int put(const char* what, const Piece* pc, int n) {
     size_t len = 0;
     for (int i = 0; i < n; ++i) len += pc[i].bytes;
@@ -125,6 +138,8 @@ extern "C" int qsgw_vcoud_read(const char* path, int ngb_cap, int* ngb, double* 
   Piece r1{&n, 4}, r2{qv, 24};
   if ((rc = f.get("vcoud_read", &r1, 1)) || (rc = f.get("vcoud_read", &r2, 1))) return rc;
   QSGW_ARG(n >= 1, "vcoud_read: %s: ngb = %d", path, n);
+  const long double ln = n;
+  if ((rc = f.check_length("vcoud_read", (4 + 8) + (24 + 8) + (8 * ln + 8) + (16 * ln * ln + 8)))) return rc;
   *ngb = n;
   if (q) std::memcpy(q, qv, sizeof qv);
   if (!vcoud && !vcousq && !zcousq) return QSGW_OK;        // header query
@@ -170,10 +185,13 @@ extern "C" int qsgw_sigma_read(const char* path, int* head, int nq_cap, int ntq_
   int32_t h[8];
   Piece r1{h, 32};
   if ((rc = f.get("sigma_read", &r1, 1))) return rc;
-  for (int i = 0; i < 8; ++i) head[i] = h[i];
-  if (!zsec && !qibz && !isx) return QSGW_OK;               // header query
   const int nq = h[1], ntq = h[2];
   QSGW_ARG(nq >= 0 && ntq >= 1, "sigma_read: %s: header nq=%d ntq=%d", path, nq, ntq);
+  const long double lt = ntq;
+  if ((rc = f.check_length("sigma_read", (32 + 8) + static_cast<long double>(nq) * (4 + 24 + 16 * lt * lt + 8))))
+    return rc;
+  for (int i = 0; i < 8; ++i) head[i] = h[i];
+  if (!zsec && !qibz && !isx) return QSGW_OK;               // header query
   QSGW_ARG(nq <= nq_cap && ntq <= ntq_cap, "sigma_read: %s holds nq=%d ntq=%d, the arrays take %d, %d", path, nq,
            ntq, nq_cap, ntq_cap);
   const size_t mat = static_cast<size_t>(ntq) * ntq;

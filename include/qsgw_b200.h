@@ -460,8 +460,10 @@ int qsgw_wv_read_d(const char *path, double *out_d, int nblochpmx, int rec0,
  * read: *ngb and q (if non-NULL) from the first two records; with vcoud,
  * vcousq and zcousq all NULL it stops there (a size query), else ngb <=
  * ngb_cap is required and each non-NULL array is filled; vcousq =
- * sqrt(vcoud) as Readvcoud forms it.  A record whose length does not match
- * this layout is an error (QSGW_ERR_ARG with the record number).          */
+ * sqrt(vcoud) as Readvcoud forms it.  A file whose length is not the one
+ * its header implies, or a record whose length does not match this layout,
+ * is an error (QSGW_ERR_ARG), found before any array is sized from the
+ * header.                                                                  */
 int qsgw_vcoud_write(const char *path, int ngb, const double *q,
                      const double *vcoud, const double *zcousq);
 int qsgw_vcoud_read(const char *path, int ngb_cap, int *ngb, double *q,
@@ -474,7 +476,8 @@ int qsgw_vcoud_read(const char *path, int ngb_cap, int *ngb, double *q,
  * nq) complex(8); every record carries the spin index is.
  * read: head from the header; with isx, qibz and zsec all NULL it stops
  * there, else nq <= nq_cap and ntq <= ntq_cap are required and the non-NULL
- * arrays are filled (isx (nq): each record's spin index).                  */
+ * arrays are filled (isx (nq): each record's spin index).  The file length
+ * is checked against the header first, as for __Vcoud.                    */
 int qsgw_sigma_write(const char *path, const int *head, int is,
                      const double *qibz, const double *zsec);
 int qsgw_sigma_read(const char *path, int *head, int nq_cap, int ntq_cap,

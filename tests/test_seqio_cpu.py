@@ -71,9 +71,14 @@ def test_vcoud_read_rejects_other_layouts(tmp_path):
     rng = np.random.default_rng(7)
     q, v, z = _vcoud_case(rng, 4)
     p = tmp_path / 'v'
-    # complex(4) eigenvectors: record 4 has the wrong length
+    # complex(4) eigenvectors: the file is shorter than its header implies
     _write_records(p, [struct.pack('<i', 4), q.tobytes(), v.tobytes(), z.astype('<c8').tobytes(order='F')])
-    with pytest.raises(lib.QSGWError, match='record 4 holds 128 bytes, expected 256'):
+    with pytest.raises(lib.QSGWError, match='holds 220 bytes, its header implies 348'):
+        lib.vcoud_read(p)
+    # the right total but records cut elsewhere: the record lengths are checked too
+    zb = z.astype('<c16').tobytes(order='F')
+    _write_records(p, [struct.pack('<i', 4), q.tobytes(), v.tobytes() + zb[:16], zb[16:]])
+    with pytest.raises(lib.QSGWError, match='record 3 holds 48 bytes, expected 32'):
         lib.vcoud_read(p)
     # 8-byte record markers (another compiler's option)
     with open(p, 'wb') as f:
@@ -84,7 +89,7 @@ def test_vcoud_read_rejects_other_layouts(tmp_path):
     lib.vcoud_write(p, q, v, z)
     data = open(p, 'rb').read()
     open(p, 'wb').write(data[:-40])
-    with pytest.raises(lib.QSGWError, match='record 4'):
+    with pytest.raises(lib.QSGWError, match='its header implies'):
         lib.vcoud_read(p)
     with pytest.raises(lib.QSGWError, match='cannot open'):
         lib.vcoud_read(tmp_path / 'missing')
@@ -168,7 +173,14 @@ def test_sigma_round_trip_and_errors(tmp_path):
     data = open(p, 'rb').read()
     rec = 8 + 4 + 24 + 16 * 16
     open(p, 'wb').write(data[:len(data) - rec])
-    with pytest.raises(lib.QSGWError, match='record 3 missing'):
+    with pytest.raises(lib.QSGWError, match='holds 332 bytes, its header implies 624'):
+        lib.sigma_read(p)
+    # a header claiming 10^9 q records is refused before any array is sized from it
+    h_big = head.copy()
+    h_big[1] = 10 ** 9
+    data = open(p, 'rb').read()
+    open(p, 'wb').write(struct.pack('<i', 32) + h_big.astype('<i4').tobytes() + struct.pack('<i', 32) + data[40:])
+    with pytest.raises(lib.QSGWError, match='its header implies'):
         lib.sigma_read(p)
     with pytest.raises(ValueError):
         lib.sigma_write(p, head, 1, qibz, zsec[:, :, :1])
