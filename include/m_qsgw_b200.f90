@@ -11,6 +11,22 @@ module m_qsgw_b200
     type(c_ptr) :: omega, ekc, freqx, wwx, expa, freq_r
     type(c_ptr) :: zmel, wc_imag, wc_real, zsec
   end type
+  type, bind(C) :: qsgw_zmel_atom
+    type(c_ptr) :: ppb_d
+    integer(c_int) :: nlnm, nc, nv, ias, ics, ims, mdim, ncore
+    real(c_double) :: phase_re, phase_im
+  end type
+  type, bind(C) :: qsgw_zmel_ipw_args
+    integer(c_int) :: ngc, ngp1, ngp2, ngcgp, nggg
+    integer(c_int) :: ntp0, nm1, nm2, nm1v, nm2v
+    integer(c_int) :: ldz, row0
+    integer(c_int) :: nadd(3)
+    type(c_ptr) :: ngvecpB1, ngvecpB2, ngveccR, nvgcgp2, nvggg, ggg, phase, geigq_d
+    integer(c_int) :: ldgq
+    type(c_ptr) :: dgeigqk_d
+    integer(c_int) :: ldgk
+    type(c_ptr) :: zmelt_d
+  end type
   interface
     integer(c_int) function qsgw_init(device) bind(C, name='qsgw_init')
       import :: c_int
@@ -228,6 +244,129 @@ module m_qsgw_b200
       import :: c_int, c_char
       integer(c_int), value :: mode
       character(kind=c_char), intent(in) :: cache_path(*)
+    end function
+    ! ---- the remaining entry points (the W_c interpolator's qsgw_wsurr_* have no
+    ! counterpart in ecalj's drivers and are not bound here)
+    integer(c_int) function qsgw_set_stream(stream) bind(C, name='qsgw_set_stream')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: stream
+    end function
+    integer(c_int) function qsgw_get_precision(mode, nslices) bind(C, name='qsgw_get_precision')
+      import :: c_int
+      integer(c_int), intent(out) :: mode, nslices
+    end function
+    integer(c_long_long) function qsgw_launch_count() bind(C, name='qsgw_launch_count')
+      import :: c_long_long
+    end function
+    integer(c_int) function qsgw_profile(enable) bind(C, name='qsgw_profile')
+      import :: c_int
+      integer(c_int), value :: enable
+    end function
+    integer(c_int) function qsgw_profile_get(tag, ms, launches) bind(C, name='qsgw_profile_get')
+      import :: c_int, c_char, c_double, c_long_long
+      character(kind=c_char), intent(in) :: tag(*)
+      real(c_double), intent(out) :: ms
+      integer(c_long_long), intent(out) :: launches
+    end function
+    integer(c_int) function qsgw_autotune_report(buf, len) bind(C, name='qsgw_autotune_report')
+      import :: c_int, c_char
+      character(kind=c_char), intent(out) :: buf(*)
+      integer(c_int), value :: len
+    end function
+    integer(c_int) function qsgw_graph_destroy() bind(C, name='qsgw_graph_destroy')
+      import :: c_int
+    end function
+    ! zmm_h (m_blas.f90:198) with host arrays
+    integer(c_int) function qsgw_zmm(a, b, c, m, n, k, opa, opb, alpha, beta, lda, ldb, ldc) &
+         bind(C, name='qsgw_zmm')
+      import :: c_int, c_double, c_double_complex
+      complex(c_double_complex), intent(in) :: a(*), b(*)
+      complex(c_double_complex), intent(inout) :: c(*)
+      integer(c_int), value :: m, n, k, opa, opb, lda, ldb, ldc
+      real(c_double), intent(in) :: alpha(2), beta(2)
+    end function
+    integer(c_int) function qsgw_zminv_hpd_batched_noalloc_d(a, n, lda, nbatch, stream) &
+         bind(C, name='qsgw_zminv_hpd_batched_noalloc_d')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: a, stream
+      integer(c_int), value :: n, lda, nbatch
+    end function
+    ! x0gemm (x0gemm.f90:2-97) with host arrays
+    integer(c_int) function qsgw_x0gemm(rcxq, npr, ipr_col, npr_col, nwhis, npm, ns1, ns2, &
+         zmel, nbb, nm1, nm2, nqtot, icounkmink, icounkmaxk, itc, itpc, jpmc, iwini, iwend, &
+         icouini, whwc, ncount) bind(C, name='qsgw_x0gemm')
+      import :: c_int, c_double, c_double_complex
+      complex(c_double_complex), intent(inout) :: rcxq(*)
+      complex(c_double_complex), intent(in) :: zmel(*)
+      integer(c_int), value :: npr, ipr_col, npr_col, nwhis, npm, ns1, ns2, nbb, nm1, nm2, nqtot
+      integer(c_int), value :: icounkmink, icounkmaxk, ncount
+      integer(c_int), intent(in) :: itc(*), itpc(*), jpmc(*), iwini(*), iwend(*), icouini(*)
+      real(c_double), intent(in) :: whwc(*)
+    end function
+    ! chi0 of one batch of k added into chi0 (zmel streamed k by k)
+    integer(c_int) function qsgw_chi0_lorentz_acc_d(chi0, npr, niw, freq_i, nk_total, nkb, nocc, nun, &
+         eocc, eunocc, zcols, ldz) bind(C, name='qsgw_chi0_lorentz_acc_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: chi0, zcols
+      integer(c_int), value :: npr, niw, nk_total, nkb, ldz
+      real(c_double), intent(in) :: freq_i(*), eocc(*), eunocc(*)
+      integer(c_int), intent(in) :: nocc(*), nun(*)
+    end function
+    ! real-axis chi0 of the Lorentzian model (broadening eta)
+    integer(c_int) function qsgw_chi0_lorentz_real_d(chi0, npr, nw, freq_r, eta, nk, nocc, nun, &
+         eocc, eunocc, zcols, ldz) bind(C, name='qsgw_chi0_lorentz_real_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: chi0, zcols
+      integer(c_int), value :: npr, nw, nk, ldz
+      real(c_double), value :: eta
+      real(c_double), intent(in) :: freq_r(*), eocc(*), eunocc(*)
+      integer(c_int), intent(in) :: nocc(*), nun(*)
+    end function
+    ! WVIllwI per-iw block (m_llw.f90:318-373) with host arrays
+    integer(c_int) function qsgw_wvi_llw(zxqi, ngb, niw, nspin, vcousq, m2e, is_x0_m_basis, &
+         is_wc_m_basis, iq, zw, nblochpmx) bind(C, name='qsgw_wvi_llw')
+      import :: c_int, c_double, c_double_complex
+      complex(c_double_complex), intent(inout) :: zxqi(*)
+      complex(c_double_complex), intent(in) :: m2e(*)
+      complex(c_double_complex), intent(inout) :: zw(*)
+      integer(c_int), value :: ngb, niw, nspin, is_x0_m_basis, is_wc_m_basis, iq, nblochpmx
+      real(c_double), intent(in) :: vcousq(*)
+    end function
+    ! imaginary-axis weights of Sigma_c (m_sxcf_gemm.f90:423-458) on the device
+    integer(c_int) function qsgw_sxcf_wgtim_d(wgtim, niw, ns1, ns2, ntqxx, nctot, omega, ekc, nekc, &
+         esmr, wkkr, ua, freqx, wwx, expa) bind(C, name='qsgw_sxcf_wgtim_d')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: wgtim
+      integer(c_int), value :: niw, ns1, ns2, ntqxx, nctot, nekc
+      real(c_double), value :: esmr, wkkr, ua
+      real(c_double), intent(in) :: omega(*), ekc(*), freqx(*), wwx(*), expa(*)
+    end function
+    ! QP energies and Hermitian Sigma (main_hqpe.sc.f90:150-161, 178-180), device arrays
+    integer(c_int) function qsgw_hqpe_d(sex2, sexcore2, sec2, vxc_band, elda, vxc, ntq, ld, nq, &
+         eqp, sigma_herm) bind(C, name='qsgw_hqpe_d')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: sex2, sexcore2, sec2, vxc_band, elda, vxc, eqp, sigma_herm
+      integer(c_int), value :: ntq, ld, nq
+    end function
+    ! get_zmel_init_gemm: muffin-tin part (m_zmel.f90:323-415)
+    integer(c_int) function qsgw_zmel_mt_d(zmelt, nbloch, nm1, nm2, nctot, ntp0, cphim, ldm, cphiq, &
+         ldq, natom, atoms) bind(C, name='qsgw_zmel_mt_d')
+      import :: c_int, c_ptr, qsgw_zmel_atom
+      type(c_ptr), value :: zmelt, cphim, cphiq
+      integer(c_int), value :: nbloch, nm1, nm2, nctot, ntp0, ldm, ldq, natom
+      type(qsgw_zmel_atom), intent(in) :: atoms(*)
+    end function
+    ! interstitial plane-wave part (m_zmel.f90:418-535)
+    integer(c_int) function qsgw_zmel_ipw_d(args) bind(C, name='qsgw_zmel_ipw_d')
+      import :: c_int, qsgw_zmel_ipw_args
+      type(qsgw_zmel_ipw_args), intent(in) :: args
+    end function
+    ! M -> E and conjugation (m_zmel.f90:546-563, 590-594)
+    integer(c_int) function qsgw_zmel_m2e_d(zmel, zmelt, ngb, nbb, nmtot, nqtot, m2e, is_m_basis, &
+         zmelconjg) bind(C, name='qsgw_zmel_m2e_d')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: zmel, zmelt, m2e
+      integer(c_int), value :: ngb, nbb, nmtot, nqtot, is_m_basis, zmelconjg
     end function
   end interface
 end module m_qsgw_b200

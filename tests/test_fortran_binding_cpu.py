@@ -1,10 +1,13 @@
 """The Fortran binding module (include/m_qsgw_b200.f90) cannot be compiled
 here (no Fortran compiler), so it is checked against the C header as text:
 every bind(C) function names a declared entry point with the same number of
-arguments, and the bind(C) type qsgw_sxcf_args lists the C struct's fields
-in the same order with matching kinds (and so does the ctypes mirror)."""
+arguments, and the bind(C) types (qsgw_sxcf_args, qsgw_zmel_atom,
+qsgw_zmel_ipw_args) list the C structs' fields in the same order with
+matching kinds, as do the ctypes mirrors."""
 import os
 import re
+
+import pytest
 
 from ecalj_b200 import lib
 
@@ -42,9 +45,9 @@ def test_every_fortran_binding_matches_a_c_prototype():
         assert nargs == c[name], f"{name}: {nargs} Fortran arguments, {c[name]} in C"
 
 
-def _c_struct_fields():
+def _c_struct_fields(name):
     src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
-    body = re.search(r"typedef struct qsgw_sxcf_args\s*\{(.*?)\}", src, flags=re.S).group(1)
+    body = re.search(r"typedef struct %s\s*\{(.*?)\}" % name, src, flags=re.S).group(1)
     fields = []
     for decl in body.split(";"):
         decl = decl.strip()
@@ -52,24 +55,43 @@ def _c_struct_fields():
             continue
         kind = "ptr" if "*" in decl else ("int" if decl.startswith("int") else "double")
         names = re.sub(r"^(const\s+)?(int|double)\s*", "", decl).replace("*", "")
-        fields += [(n.strip(), kind) for n in names.split(",")]
+        for n in names.split(","):
+            m = re.match(r"\s*(\w+)\s*(?:\[(\d+)\])?", n)
+            fields.append((m.group(1), kind + (f"[{m.group(2)}]" if m.group(2) else "")))
     return fields
 
 
-def _fortran_type_fields():
+def _fortran_type_fields(name):
     src = open(MODULE).read()
-    body = re.search(r"type, bind\(C\) :: qsgw_sxcf_args(.*?)end type", src, flags=re.S).group(1)
+    body = re.search(r"type, bind\(C\) :: %s\n(.*?)end type" % name, src, flags=re.S).group(1)
     kinds = {"integer(c_int)": "int", "real(c_double)": "double", "type(c_ptr)": "ptr"}
     fields = []
     for line in body.strip().splitlines():
         k, names = line.split("::")
-        fields += [(n.strip(), kinds[k.strip()]) for n in names.split(",")]
+        for n in names.split(","):
+            m = re.match(r"\s*(\w+)\s*(?:\((\d+)\))?", n)
+            fields.append((m.group(1), kinds[k.strip()] + (f"[{m.group(2)}]" if m.group(2) else "")))
     return fields
 
 
-def test_sxcf_args_layout_matches():
-    c = _c_struct_fields()
-    assert _fortran_type_fields() == c
-    mirror = [(n, "ptr" if t is lib.c_vp else ("int" if t is lib.c_int else "double"))
-              for n, t in lib.SxcfArgs._fields_]
-    assert mirror == c
+def _ctypes_fields(struct):
+    def kind(t):
+        if t is lib.c_vp:
+            return "ptr"
+        if t is lib.c_int:
+            return "int"
+        if t is lib.c_dbl:
+            return "double"
+        if getattr(t, "_type_", None) is lib.c_int and hasattr(t, "_length_"):
+            return f"int[{t._length_}]"
+        raise AssertionError(t)
+    return [(n, kind(t)) for n, t in struct._fields_]
+
+
+@pytest.mark.parametrize("name,mirror", [("qsgw_sxcf_args", "SxcfArgs"), ("qsgw_zmel_atom", "ZmelAtom"),
+                                         ("qsgw_zmel_ipw_args", "ZmelIpwArgs")])
+def test_struct_layouts_match(name, mirror):
+    c = _c_struct_fields(name)
+    assert len(c) >= 10
+    assert _fortran_type_fields(name) == c
+    assert _ctypes_fields(getattr(lib, mirror)) == c
