@@ -73,7 +73,8 @@ def test_graph_replay_matches_eager(qsgw, prec):
 def test_graph_refuses_scratch_growth(qsgw):
     import torch
     lib = qsgw
-    # more pairs x frequencies than any other test uses: the weight scratch must grow
+    # more pairs x frequencies than any test collected before this one (the full-size chi0
+    # test is collected after it): the weight scratch must grow
     p = synth.chi0_problem(N=64, nk=64, nocc=8, nun=(100, 120), niw=12, seed=35)
     N, niw = p["N"], p["niw"]
     chi = torch.zeros(N * N * niw, dtype=torch.complex128, device="cuda")

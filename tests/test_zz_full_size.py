@@ -4,7 +4,10 @@ properties that do not depend on the size.  The split-FP16 result equals the
 plain FP64 result to the split path's gate (relative Frobenius <= 5e-5;
 measured about 1e-6); both are Hermitian in (G, G') and negative
 definite at every iw checked, as chi0(iw) = -sum |z><z| 2 de / (de^2 + w^2) / nk
-with far more pairs than rows must be."""
+with far more pairs than rows must be.  Collected after the other GPU tests:
+it grows the library's device scratch to the full workload, after which the
+graph test's refusal to grow scratch while recording would have nothing to
+refuse."""
 import math
 
 import numpy as np
