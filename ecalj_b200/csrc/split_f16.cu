@@ -455,6 +455,57 @@ __global__ void presplit_a_kernel(__half* __restrict__ out, const double2* __res
   }
   }
 }
+// chi0 A' from Z (getter 0 of presplit_a_kernel, one slot): block (32, 8) converts one 64-row tile t
+// and 32 consecutive k.  The loads run along m (Z's columns are contiguous in m); the four half2 words
+// of each element (row0 / row1 x hi / lo slice) are staged in shared memory, and the stores run
+// along k, so a warp writes 128 contiguous bytes of one output row instead of 32 words 2 Kp bytes
+// apart.  Writes the same halves as presplit_a_kernel<0>.
+__global__ void presplit_z_kernel(__half* __restrict__ out, const double2* __restrict__ src, long long ld, int M,
+                                  long long K, int T, long long Kp, const double* __restrict__ scales,
+                                  long long slice_elems) {
+  __shared__ __half2 st[4][64][33];          // [row0 hi, row0 lo, row1 hi, row1 lo][mm][k - k0]
+  const double sig = scales[0];
+  const long long KH = Kp / 2;
+  const long long k0 = static_cast<long long>(blockIdx.x) * 32;
+  for (int t = blockIdx.y; t < T; t += gridDim.y) {
+    for (int j = 0; j < 4; ++j) {
+      const int kk = threadIdx.y + 8 * j;
+      const long long k = k0 + kk;
+      for (int it = 0; it < 2; ++it) {
+        const int mm = threadIdx.x + 32 * it;
+        const int m = t * 64 + mm;
+        double ar = 0.0, ai = 0.0;
+        if (m < M && k < K) {
+          const double2 v = src[m + k * ld];
+          ar = v.x; ai = -v.y;     // a = conj(v)
+        }
+        // row0: [Re a, -Im a]; row1: [Im a, Re a]
+        __half h0, l0, h1, l1;
+        split2(ar, sig, h0, l0);
+        split2(-ai, sig, h1, l1);
+        st[0][mm][kk] = __halves2half2(h0, h1);
+        st[1][mm][kk] = __halves2half2(l0, l1);
+        split2(ai, sig, h0, l0);
+        split2(ar, sig, h1, l1);
+        st[2][mm][kk] = __halves2half2(h0, h1);
+        st[3][mm][kk] = __halves2half2(l0, l1);
+      }
+    }
+    __syncthreads();
+    const long long k = k0 + threadIdx.x;
+    if (k < KH) {
+      for (int r = threadIdx.y; r < 64; r += 8) {
+        const long long row0 = static_cast<long long>(t) * 128 + r, row1 = row0 + 64;
+        *reinterpret_cast<__half2*>(out + row0 * Kp + 2 * k) = st[0][r][threadIdx.x];
+        *reinterpret_cast<__half2*>(out + slice_elems + row0 * Kp + 2 * k) = st[1][r][threadIdx.x];
+        *reinterpret_cast<__half2*>(out + row1 * Kp + 2 * k) = st[2][r][threadIdx.x];
+        *reinterpret_cast<__half2*>(out + slice_elems + row1 * Kp + 2 * k) = st[3][r][threadIdx.x];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <int GET>
 static dim3 presplit_a_grid(long long Kp, long long tiles) {
   const long long KH = Kp / 2;
@@ -618,10 +669,10 @@ int chi0_split_f16(double2* chi0, int npr, int niw, const double2* zcols, int ld
   QSGW_LAUNCH_CHECK("scale_weights_kernel");
   __half* a = g_a.as<__half>();
   QSGW_CUDA(cudaMemsetAsync(a, 0, 2 * slice_elems * sizeof(__half), s));
-  presplit_a_kernel<0><<<presplit_a_grid<0>(Kp, T), dim3(32, 8), 0, s>>>(
-      a, zcols, ldz, 0, npr, npair, T, 1, Kp, g_sc.as<double>(), slice_elems);
+  presplit_z_kernel<<<dim3(static_cast<unsigned>((Kp / 2 + 31) / 32), static_cast<unsigned>(std::min(T, 65535))),
+                      dim3(32, 8), 0, s>>>(a, zcols, ldz, npr, npair, T, Kp, g_sc.as<double>(), slice_elems);
   count_launch();
-  QSGW_LAUNCH_CHECK("presplit_a_kernel");
+  QSGW_LAUNCH_CHECK("presplit_z_kernel");
   // maps: A' [Kp, 64, 2, 2*Ta] (hi tiles 0..Ta-1, lo tiles Ta..2Ta-1) box {64,64,2,1};
   //       S  same memory, half 0 of two consecutive tiles: box {64,64,1,2}
   CUtensorMap ma, ms;
