@@ -82,3 +82,16 @@ def test_cpp_caller_gpu(so, tmp_path):
     """The same program multiplies Fortran-layout matrices through qsgw_zmm."""
     r = subprocess.run([str(_cabi_caller(tmp_path)), "gpu"], capture_output=True, text=True)
     assert r.returncode == 0 and "OK gpu" in r.stdout, r.stdout + r.stderr
+
+
+def test_header_is_plain_c(tmp_path):
+    """The header compiles as strict C99 (the Fortran ISO_C_BINDING side and C
+    callers see it without a C++ compiler), structs included."""
+    src = tmp_path / "hdr.c"
+    src.write_text('#include "qsgw_b200.h"\n'
+                   "int main(void) { qsgw_sxcf_args a; qsgw_zmel_atom z; qsgw_zmel_ipw_args p;\n"
+                   "  (void)a; (void)z; (void)p; return 0; }\n")
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I",
+                        os.path.join(ROOT, "include"), "-c", str(src), "-o", str(tmp_path / "hdr.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
