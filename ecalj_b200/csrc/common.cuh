@@ -55,6 +55,11 @@ void count_launch(int n = 1);
 int prof_begin(const char* tag, cudaStream_t s);
 void prof_end(int idx, cudaStream_t s);
 
+// cudaFuncSetAttribute acts on the current device only, so a kernel's raised
+// dynamic shared-memory limit is applied once per device: `done` holds one
+// bit per device index (devices beyond 63 set it on every call).
+int smem_limit_once(const void* kernel, int bytes, uint64_t& done);
+
 }  // namespace qsgw
 
 #define QSGW_CUDA(call)                                                   \

@@ -23,6 +23,16 @@ void set_error(const char* fmt, ...) {
 
 void count_launch(int n) { g_launches += n; }
 
+int smem_limit_once(const void* kernel, int bytes, uint64_t& done) {
+  int dev = 0;
+  QSGW_CUDA(cudaGetDevice(&dev));
+  const uint64_t bit = (dev >= 0 && dev < 64) ? (uint64_t{1} << dev) : 0;
+  if (bit && (done & bit)) return QSGW_OK;
+  QSGW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done |= bit;
+  return QSGW_OK;
+}
+
 int check_cuda(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return QSGW_OK;
   set_error("%s: %s", what, cudaGetErrorString(e));

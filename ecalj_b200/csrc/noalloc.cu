@@ -55,11 +55,18 @@ extern "C" int qsgw_zminv_hpd_batched_noalloc_d(double* a, int n, int lda, int n
   QSGW_ARG(static_cast<long long>(n) * nbatch <= kMaxCols,
            "zminv_hpd_noalloc: n*nbatch = %lld exceeds the static scratch limit %lld",
            static_cast<long long>(n) * nbatch, kMaxCols);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  QSGW_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    set_error("zminv_hpd_noalloc: the call waits for its stream to read the status word, so it cannot be "
+              "recorded into a CUDA graph");
+    return QSGW_ERR_UNSUPPORTED;
+  }
   if (n == 0 || nbatch == 0) return QSGW_OK;
   double2* base = nullptr;
   int rc = scratch_for_current_device(&base);
   if (rc) return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   int* status = reinterpret_cast<int*>(base + 2 * kPanelElems);
   QSGW_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));          // the array keeps the last call's status
   rc = zminv_hpd_batched_explicit(reinterpret_cast<double2*>(a), n, lda, static_cast<long long>(lda) * n, nbatch,

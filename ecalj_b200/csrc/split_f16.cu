@@ -593,12 +593,9 @@ static DevBuf g_a, g_s, g_mx, g_sc, g_tabs, g_w32;
 
 template <int MODE>
 static int launch_mode(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    QSGW_CUDA(cudaFuncSetAttribute(split_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   Cfg<MODE>::SMEM_BYTES));
-    attr = true;
-  }
+  static uint64_t attr = 0;                       // one bit per device
+  int rc = smem_limit_once(reinterpret_cast<const void*>(split_gemm_kernel<MODE>), Cfg<MODE>::SMEM_BYTES, attr);
+  if (rc) return rc;
   split_gemm_kernel<MODE><<<grid, NTHREADS, Cfg<MODE>::SMEM_BYTES, s>>>(ma, ms, p);
   return QSGW_OK;
 }

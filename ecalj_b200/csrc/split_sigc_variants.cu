@@ -516,11 +516,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 // Sigma_c on CTA pairs (clusters of two): grid.x = 2 * ceil(row tiles / 2) * column tiles
 int launch_sigc_pair(const CUtensorMap& ma, const CUtensorMap& ms, const Params& p, dim3 grid, cudaStream_t s,
                      const char* tag) {
-  static bool attr = false;
-  if (!attr) {
-    QSGW_CUDA(cudaFuncSetAttribute(split_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PairCfg::SMEM_BYTES));
-    attr = true;
-  }
+  static uint64_t attr = 0;                       // one bit per device
+  int rc = smem_limit_once(reinterpret_cast<const void*>(split_pair_kernel), PairCfg::SMEM_BYTES, attr);
+  if (rc) return rc;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(NTHREADS, 1, 1);
@@ -545,12 +543,10 @@ static DevBuf g_scr;                      // FP64 sums of the 256-column kernel
 
 int launch_sigc_wide(const CUtensorMap& ma, const CUtensorMap& ms, Params p, dim3 grid, cudaStream_t s,
                      const char* tag) {
-  static bool attr = false;
-  if (!attr) {
-    QSGW_CUDA(cudaFuncSetAttribute(sigc_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WideCfg::SMEM_BYTES));
-    attr = true;
-  }
-  int rc = g_scr.ensure(static_cast<size_t>(grid.x) * NW * BM2 * sizeof(double));
+  static uint64_t attr = 0;                       // one bit per device
+  int rc = smem_limit_once(reinterpret_cast<const void*>(sigc_wide_kernel), WideCfg::SMEM_BYTES, attr);
+  if (rc) return rc;
+  rc = g_scr.ensure(static_cast<size_t>(grid.x) * NW * BM2 * sizeof(double));
   if (rc) return rc;
   p.scratch = g_scr.as<double>();
   const int pi = prof_begin(tag, s);

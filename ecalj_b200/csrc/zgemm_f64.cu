@@ -8,12 +8,9 @@ namespace qsgw {
 template <int MODE, bool A_RC, bool B_RC>
 static int launch_kernel(const ZParams& p, dim3 grid, cudaStream_t s) {
   auto kern = zgemm_f64_kernel<MODE, A_RC, B_RC>;
-  static bool attr_done = false;
-  if (!attr_done) {
-    QSGW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(sizeof(ZSmem))));
-    attr_done = true;
-  }
+  static uint64_t attr_done = 0;                  // one bit per device
+  int rc = smem_limit_once(reinterpret_cast<const void*>(kern), static_cast<int>(sizeof(ZSmem)), attr_done);
+  if (rc) return rc;
   const char* tag = MODE == ZM_CHI0 ? "chi0_dmma" : (MODE == ZM_SEG ? "sigc_seg_dmma" : "gemm_dmma");
   const int pi = prof_begin(tag, s);
   kern<<<grid, ZG_THREADS, sizeof(ZSmem), s>>>(p);

@@ -227,12 +227,11 @@ extern "C" int qsgw_zmel_mt_d(double* zmelt_d, int nbloch, int nm1, int nm2, int
     nvmax = std::max(nvmax, a.nv);
   }
   const size_t smem = static_cast<size_t>(3 * nvmax * ZM_T) * sizeof(double2) + static_cast<size_t>(nvmax) * nvmax * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    QSGW_CUDA(cudaFuncSetAttribute(zmel_mt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(3 * ZM_NVMAX * ZM_T * sizeof(double2) + ZM_NVMAX * ZM_NVMAX * sizeof(double))));
-    attr = true;
-  }
+  static uint64_t attr = 0;                       // one bit per device
+  rc = smem_limit_once(reinterpret_cast<const void*>(zmel_mt_kernel),
+                       static_cast<int>(3 * ZM_NVMAX * ZM_T * sizeof(double2) + ZM_NVMAX * ZM_NVMAX * sizeof(double)),
+                       attr);
+  if (rc) return rc;
   cudaStream_t s = ctx().stream;
   rc = g_zm_atoms.ensure(natom * sizeof(ZmelAtomDev));
   if (rc) return rc;

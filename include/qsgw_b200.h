@@ -113,9 +113,11 @@ int qsgw_zminv_hpd_batched_d(double *a, int n, int lda, int nbatch);
  * is done.  Limit: n * nbatch <= 16384 (larger sizes return QSGW_ERR_ARG).
  * The Gauss-Jordan panels and the status word live in one static device
  * array of 16 MiB that every GPU loading the library holds until exit; the
- * first call on a device looks up that array's device address, so make the
- * first call before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race and must not be issued concurrently.        */
+ * first call on a device looks up that array's device address.  Every call
+ * waits for its stream to read the status word, so no call can be recorded
+ * into a CUDA graph: on a capturing stream it returns QSGW_ERR_UNSUPPORTED
+ * before enqueuing anything.  All calls share the array: calls that overlap
+ * on the GPU race and must not be issued concurrently.                     */
 int qsgw_zminv_hpd_batched_noalloc_d(double *a, int n, int lda, int nbatch,
                                      void *stream);
 

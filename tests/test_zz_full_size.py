@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 from ecalj_b200 import synth
+from tests.conftest import rel_fro
 
 pytestmark = pytest.mark.gpu
 
@@ -55,3 +56,94 @@ def test_chi0_n600_split_equals_fp64_and_keeps_its_properties(qsgw):
             a = m[j]
             ev = torch.linalg.eigvalsh(0.5 * (a + a.conj().T)).cpu().numpy()
             assert ev.max() < 0.0                        # 390 834 pairs >> N: negative definite
+
+
+HARTREE_MEV = 27211.386245988
+
+
+def _split_modes(qsgw):
+    """(name, precision mode, slices, gate on the relative Frobenius error) of every split path."""
+    modes = [("split-f16", qsgw.PREC_SPLIT_F16, 2, 5e-5)]
+    if hasattr(qsgw, "PREC_SPLIT_I8"):
+        modes.append(("split-i8x3", qsgw.PREC_SPLIT_I8, 3, 5e-6))
+    return modes
+
+
+def test_chi0_n600_all_pairs_two_frequencies_vs_oracle(qsgw):
+    """The benchmark's chi0 workload at its own size -- N = 600, nk = 216, all
+    390 834 (k, occ, unocc) pairs -- on 2 seeded imaginary frequencies of the 24,
+    against the oracle's x0gemm restatement (x0gemm.f90:37-93 with the
+    Lorentzian pair tables): FP64 to 1e-11, the split paths to their gates."""
+    import torch
+    from oracle import x0
+    c = synth.CONFIGS["chi0_n600"]
+    rng = np.random.default_rng(c["seed"])
+    nocc, nun, eocc, eun = synth.chi0_spectrum(rng, c["nk"], c["nocc"], c["nun"])
+    mesh = synth.imag_mesh(c["niw"])
+    sel = np.sort(np.random.default_rng(c["seed"] + 1).choice(c["niw"], 2, replace=False))
+    freq = mesh["freq_i"][sel]
+    N, nk, niw = c["N"], c["nk"], 2
+    npair = int(np.sum(nocc * nun))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(c["seed"])
+    zc = torch.empty(2 * N * npair, dtype=torch.float64, device="cuda")
+    zc.normal_(0.0, 1.0 / math.sqrt(N), generator=g)
+    zc = zc.view(torch.complex128)
+    zh = zc.cpu().numpy().reshape(N, npair, order="F")
+    eo_h = [e * 0.5 for e in eocc]
+    eu_h = [e * 0.5 for e in eun]
+    zs, c0 = [], 0
+    for k in range(nk):
+        no, nu = int(nocc[k]), int(nun[k])
+        zs.append(zh[:, c0:c0 + no * nu].reshape(N, no, nu, order="F"))
+        c0 += no * nu
+    ref = x0.chi0_direct(zs, x0.lorentz_pair_tables(eo_h, eu_h, niw, freq, nk), N, niw)[:, :, 1:]
+    modes = [("fp64", qsgw.PREC_FP64, 1, 1e-11)] + _split_modes(qsgw)
+    try:
+        for name, prec, ns, tol in modes:
+            qsgw.set_precision(prec, ns)
+            chi = torch.zeros(N * N * niw, dtype=torch.complex128, device="cuda")
+            qsgw.chi0_lorentz_d(chi, N, niw, freq, nk, nocc, nun, np.concatenate(eocc) * 0.5,
+                                np.concatenate(eun) * 0.5, zc)
+            qsgw.synchronize()
+            err = rel_fro(qsgw.from_device(chi, (N, N, niw)), ref)
+            print(f"chi0 N=600, {npair} pairs, iw {list(sel)}: {name} vs oracle {err:.2e}")
+            assert err < tol, (name, err)
+    finally:
+        qsgw.set_precision(qsgw.PREC_FP64, 1)
+
+
+def test_sigc_n600_one_full_task_vs_oracle(qsgw):
+    """One Sigma_c task of the benchmark at its own size -- N = 600, 400
+    intermediate x 40 target states, 24 + 1 imaginary slots and the pole part
+    on the 50-point real mesh -- against the oracle's get_correlation_block
+    restatement (m_sxcf_gemm.f90:423-608): FP64 to 1e-11, the split paths to
+    their gates, with the QP-energy shift of each stated."""
+    from oracle import sxcf
+    c = synth.CONFIGS["sigc_n600"]
+    N, ntq, nm, niw, nreal = c["N"], c["ntq"], c["nm"], c["niw"], c["nreal"]
+    t = synth.sigc_task(N, ntq, nm, niw, nreal, seed=c["seed"], esmr=0.01, ef=0.0)
+    rng = np.random.default_rng(c["seed"] + 5)
+    a = rng.standard_normal((N, N, niw + 1)) + 1j * rng.standard_normal((N, N, niw + 1))
+    wi = np.asfortranarray(-0.01 * (a + np.conj(np.transpose(a, (1, 0, 2)))))     # Hermitian per slot
+    wr = synth.real_axis_model(wi[:, :, 0], t["freq_r"])
+    nt0p, nt0m = sxcf.nt0pm(t["ekc"], t["ef"], t["esmr"])
+    nwxi, nwx, ntmax = sxcf.get_nwx(t["omega"], ntq, nt0p, nt0m, nm, t["freq_r"], t["esmr"], t["ef"], t["ekc"], 0)
+    args = (1, nm, min(nm, ntmax), nwxi, nwx, ntq, wi, wr, t["omega"], t["ekc"], 0, t["ef"], t["esmr"],
+            1.0 / c["nq"], t["ua"], t["x"], t["wx"], t["expa"], t["freq_r"])
+    ref = np.zeros((ntq, ntq), complex, order="F")
+    sxcf.correlation_block(ref, t["zmel"], *args)
+    modes = [("fp64", qsgw.PREC_FP64, 1, 1e-11)] + _split_modes(qsgw)
+    try:
+        for name, prec, ns, tol in modes:
+            qsgw.set_precision(prec, ns)
+            got = np.zeros((ntq, ntq), complex, order="F")
+            qsgw.sxcf_correlation(got, t["zmel"], *args)
+            err = rel_fro(got, ref)
+            dqp = np.max(np.abs(np.real(np.diag(got) - np.diag(ref)))) * HARTREE_MEV
+            scale = np.mean(np.abs(np.real(np.diag(ref)))) * HARTREE_MEV
+            print(f"Sigma_c N=600 task: {name} vs oracle {err:.2e}, max QP shift {dqp:.3e} meV "
+                  f"(mean |Re Sigma_c,nn| {scale:.3e} meV)")
+            assert err < tol, (name, err)
+    finally:
+        qsgw.set_precision(qsgw.PREC_FP64, 1)

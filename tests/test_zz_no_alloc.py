@@ -57,3 +57,73 @@ def test_noalloc_rejects_sizes_beyond_the_limit(qsgw):
     with pytest.raises(qsgw.QSGWError) as e:
         qsgw.zminv_hpd_batched_noalloc_d(t, 8193, 8193, 2)
     assert e.value.code == -1 and "16384" in str(e.value)
+
+
+_NO_INIT_SCRIPT = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, {root!r})
+from ecalj_b200 import lib
+from tests.test_zz_no_alloc import _hpd_batch
+dev = {dev}
+torch.cuda.set_device(dev)
+lib.load()                                   # no qsgw_init: the call needs no library context
+assert not lib.initialized()
+side = torch.cuda.Stream()                   # not the default stream
+for n, nb, seed in [(64, 3, 5), (130, 2, 6)]:
+    a = _hpd_batch(n, nb, seed)
+    with torch.cuda.stream(side):
+        t = torch.from_numpy(a.reshape(-1, order='F').copy()).to('cuda')
+    side.synchronize()
+    lib.zminv_hpd_batched_noalloc_d(t, n, n, nb, side.cuda_stream)
+    got = t.cpu().numpy().reshape(a.shape, order='F')
+    for b in range(nb):
+        ref = np.linalg.inv(a[:, :, b])
+        err = np.linalg.norm(got[:, :, b] - ref) / np.linalg.norm(ref)
+        assert err < 1e-11, (n, b, err)
+print("ok")
+"""
+
+
+def _run_fresh(dev):
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = _NO_INIT_SCRIPT.format(root=root, dev=dev)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]
+
+
+def test_noalloc_without_init_on_a_side_stream_in_a_fresh_process():
+    """The documented use: a caller that never ran qsgw_init, on a stream of
+    its own, in a process where nothing else touched the library."""
+    _run_fresh(0)
+
+
+def test_noalloc_on_a_second_device():
+    """The static array and the raised shared-memory limit of the GEMM kernel
+    are per device: the first call on device 1 must set both up there."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one visible GPU")
+    _run_fresh(1)
+
+
+def test_noalloc_refuses_a_capturing_stream(qsgw):
+    import torch
+    n, nb = 32, 1
+    t = qsgw.to_device(_hpd_batch(n, nb, 7))
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    err = None
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        try:
+            qsgw.zminv_hpd_batched_noalloc_d(t, n, n, nb, s.cuda_stream)
+        except qsgw.QSGWError as e:
+            err = e
+        finally:
+            g.capture_end()
+    assert err is not None and err.code == -7          # QSGW_ERR_UNSUPPORTED
