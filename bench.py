@@ -10,7 +10,7 @@ One step = the hot path over one batch of synthetic input:
 Inputs are seeded synthetic data with the configurations' shapes and value
 distributions; W_c(q, iw) is built by this library's own chi0 -> W path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|split]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision split-i8|split-f16|fp64] [--slices 3]
     python bench.py --impl reference ...   # the reference's CPU path (oracle)
 
 N > 1 runs N independent replicas (the path needs no collective; the
@@ -36,8 +36,8 @@ METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err 
 # ----------------------------------------------------------------------------- helpers
 # DRAM bytes (read + write) of one split-precision Sigma_c task launch
 # (N=600, 40 x 400 states, 25 imaginary slots + real-axis pole columns),
-# measured with ncu on that launch: 1.975 GB read + 0.240 GB written.
-SIGC_TC_TRAFFIC = 3.315e9
+# measured with ncu on that launch, per kernel of the path.
+SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": None}
 
 
 def load_peaks():
@@ -277,8 +277,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="split", choices=["split", "fp64"],
-                    help="headline precision; split also times the FP64 path for the comparison")
+    ap.add_argument("--precision", default="split-i8", choices=["split-i8", "split-f16", "fp64"],
+                    help="headline precision; a split mode also times the FP64 path for the comparison")
+    ap.add_argument("--slices", type=int, default=0,
+                    help="int8 slices per operand of split-i8 (2..4); 0 = chosen per contraction by the "
+                         "library's accuracy targets (QP 1 meV for Sigma_c, 2e-5 relative for chi0)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
@@ -306,6 +309,9 @@ def main():
     if not args.no_autotune:
         lib.set_autotune(1, None)          # the first (untimed) call of each shape picks its split-K
     prec = args.precision
+    split = prec != "fp64"
+    modes = {"fp64": (lib.PREC_FP64, 1), "split-f16": (lib.PREC_SPLIT_F16, 2),
+             "split-i8": (lib.PREC_SPLIT_I8, args.slices)}
     peaks, peak_src = load_peaks()
 
     # ---- workload set-up (untimed)
@@ -336,7 +342,7 @@ def main():
         """Warm-up steps, then `steps` timed steps: eager calls, or replays of
         one step recorded as a CUDA graph (launch count and per-kernel times of
         a replay are those recorded, scaled by the number of replays)."""
-        lib.set_precision(lib.PREC_SPLIT_F16 if mode == "split" else lib.PREC_FP64)
+        lib.set_precision(*modes[mode])
         for _ in range(warmup):
             step()
         torch.cuda.synchronize()
@@ -367,7 +373,7 @@ def main():
         launches = per_step * steps if graph else lib.launch_count() - l0
         ms = ev0.elapsed_time(ev1) / steps
         kt = {tag: lib.profile_get(tag) for tag in ("chi0_dmma", "sigc_seg_dmma", "gemm_dmma", "chi0_tc",
-                                                   "sigc_seg_tc")}
+                                                   "sigc_seg_tc", "chi0_slice_i8", "sigc_slice_i8")}
         if graph:                                        # the latest replay's times, for every replay
             kt = {k: (v[0] * steps, v[1] * steps) for k, v in kt.items()}
             lib.graph_destroy()
@@ -389,7 +395,7 @@ def main():
 
     # ---- the other precision, same workload, same run (the metric compares them)
     compare = None
-    if prec == "split" and not args.no_compare:
+    if split and not args.no_compare:
         ms64, kt64, _, _ = timed("fp64", args.steps, 1, False, graph=not args.no_graph)
         d_chi = float(torch.linalg.vector_norm(chi_main - chi) / torch.linalg.vector_norm(chi))
         num = sum(float(torch.linalg.vector_norm(a - t["zsec"]) ** 2) for a, t in zip(zsec_main, s["tasks"]))
@@ -408,11 +414,12 @@ def main():
         # Sigma_c rescaled to a mean |Re Sigma_c,nn| of 5 eV (Si/GaAs-like).
         dmean = float(np.mean([float(torch.mean(torch.abs(torch.real(t["zsec"]).view(s["ntq"], s["ntq"]).diagonal())))
                                for t in s["tasks"]])) * 27.211386245988
-        compare.update({"sigc_diag_mean_abs_ev": dmean, "qp_err_mev_max_at_5ev_sigma": qp * 5.0 / dmean})
-        lib.set_precision(lib.PREC_SPLIT_F16)
+        compare.update({"sigc_diag_mean_abs_ev": dmean, "qp_err_mev_max_at_5ev_sigma": qp * 5.0 / dmean,
+                        "qp_gate_1mev_met": qp <= 1.0})
+        lib.set_precision(*modes[prec])
 
     # ---- roofline of the dominant kernel
-    if prec == "split":
+    if split:
         dom_tag, dom_flops = "sigc_seg_tc", fl_sig_seg
     else:
         dom_tag, dom_flops = "sigc_seg_dmma", fl_sig_seg
@@ -420,7 +427,17 @@ def main():
     per_launch_ms = k_ms / max(k_n, 1)
     achieved = (dom_flops * args.steps / max(k_n, 1)) / (per_launch_ms * 1e-3) / 1e12 if k_n else None
     fp64_peak = measure_fp64_peak()
-    if prec == "split":
+    i8_peak = None
+    slices_used = chosen_slices(lib, args.slices) if prec == "split-i8" else None
+    if prec == "split-i8":
+        i8_peak = measure_int8_peak()
+        ns_sig = slices_used["sigc"]
+        nprod = ns_sig * (ns_sig + 1) // 2
+        peak = i8_peak["sustained_tops"] / nprod
+        peak_note = (f"int8 tensor peak measured in this run (torch._int_mm, 8192^3, sustained "
+                     f"{i8_peak['sustained_tops']:.1f} TOP/s) / {nprod} (int8 slice products per "
+                     f"FP64-equivalent product at {ns_sig} slices)")
+    elif prec == "split-f16":
         peak = peaks["bf16_tflops_sustained"] / 3.0
         peak_note = (f"{peak_src} bf16 sustained {peaks['bf16_tflops_sustained']} TFLOP/s / 3 "
                      f"(3 FP16 slice products per FP64-equivalent product)")
@@ -429,41 +446,43 @@ def main():
         peak_note = "cuBLAS ZGEMM (complex128, 4096^3) measured in this run; MEASURED_PEAKS.json has no FP64 figure"
     roof = {"bound": "tensor", "achieved": round(achieved, 3) if achieved else None, "peak": round(peak, 3),
             "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if achieved else None,
-            "traffic": SIGC_TC_TRAFFIC if prec == "split" else None,
+            "traffic": SIGC_TC_TRAFFIC.get(prec),
             "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one Sigma_c task launch "
-                               "(same shape, sigc_wide_kernel) from ncu" if prec == "split" else "not captured"),
+                               "(same shape) from ncu" if SIGC_TC_TRAFFIC.get(prec) else "not captured"),
             "kernel": dom_tag, "launch_ms": round(per_launch_ms, 4), "peak_source": peak_note,
             "algorithmic_flops_per_launch": dom_flops * args.steps / max(k_n, 1)}
 
     # ---- end-to-end through the host-pointer entry points (pinned host buffers)
     e2e = None
     if not args.no_e2e:
-        lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
+        lib.set_precision(*modes[prec])
         e2e = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist)
     sur = None
     if not args.no_surrogate:
         lib.set_autotune(0, None)          # no tuning trials inside the study's timed calls
-        sur = surrogate_summary(lib, log)
-        lib.set_precision(lib.PREC_SPLIT_F16 if prec == "split" else lib.PREC_FP64)
+        sur = surrogate_summary(lib, log, precision=prec if split else "fp64", nslices=args.slices)
+        lib.set_precision(*modes[prec])
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline()
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "c128" if prec == "fp64" else "c128 via split-f16",
+                "vs_baseline": None, "dtype": {"fp64": "c128", "split-f16": "c128 via 2 FP16 slices, 3 products",
+                                               "split-i8": "c128 via int8 slices (Ozaki), exact INT32 accumulation"
+                                               }[prec],
                 "data": "synthetic",
                 "config": {"workload": f"chi0 (N=600, nk={cfg_chi['nk']}, nocc=9, nunocc U{{100..300}}, 24 iw, "
                                        f"{cfg_chi['npair']} pairs) + Sigma_c ({len(s['tasks'])} tasks, N=600, "
                                        "40x400 states, 24+1 iw, 50-point real mesh)",
-                           "precision": prec, "parallelism": f"replicas x{ws}",
+                           "precision": prec, "slices": slices_used, "parallelism": f"replicas x{ws}",
                            "execution": "CUDA graph replay" if not args.no_graph else "eager calls",
                            "eager_ms_per_step": round(ms_eager, 3) if ms_eager else None,
                            "l2": "inputs exceed L2 (zmel columns 3.73 GB)",
                            "flops_per_step": flops, "flops_chi0": fl_chi, "flops_sigc": fl_sig},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "kernel_ms": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]},
-                "fp64_peak_tflops": round(fp64_peak, 3), "compare": compare, "surrogate": sur,
+                "fp64_peak_tflops": round(fp64_peak, 3), "int8_peak": i8_peak, "compare": compare, "surrogate": sur,
                 "autotune": lib.autotune_report()}
         if compare and cpu and cpu.get("value"):
             # both FP64: this library's plain GPU path over the CPU restatement (same flop count)
@@ -473,13 +492,13 @@ def main():
         dist.destroy_process_group()
 
 
-def surrogate_summary(lib, log, nq_test=8):
+def surrogate_summary(lib, log, nq_test=8, precision="split-i8", nslices=3):
     """W_c(q, iw) on the 48-point imaginary grid (N=600, Sigma_c configuration
     generator): the plain method (every frequency exact, FP64 and split) against
     the split path with the learned frequency interpolator (17 of 49 slots
     exact, validated, fallback above 1 meV), on q points not trained on."""
     from ecalj_b200 import surrogate
-    res = surrogate.study(N=600, nq_train=48, nq_test=nq_test, precision="split", log=log)
+    res = surrogate.study(N=600, nq_train=48, nq_test=nq_test, precision=precision, log=log, nslices=nslices)
     rows = res["rows"]
     mean = lambda k: float(np.mean([r[k] for r in rows]))
     out = {"workload": "W_c interpolation: exact W_c on 48 iw x 48 training q at N=600, 8 anchors, 8 held-out, "
@@ -505,6 +524,45 @@ def surrogate_summary(lib, log, nq_test=8):
 def mean_d(rows, k):
     return {"full": float(np.mean([r[k]["w_rel"] for r in rows])),
             "dominant_block": float(np.mean([r[k]["w_rel_block"] for r in rows]))}
+
+
+def chosen_slices(lib, requested):
+    """int8 slices per operand of the chi0 and Sigma_c contractions: the requested
+    count, or the automatic choices the library recorded for this workload."""
+    if requested:
+        return {"chi0": requested, "sigc": requested, "products": {"chi0": requested * (requested + 1) // 2,
+                                                                   "sigc": requested * (requested + 1) // 2}}
+    rep = lib.autotune_report()
+    pick = lambda pre: max((v for k, v in rep.items() if k.startswith(pre) and "err@" not in k), default=4)
+    ns = {"chi0": pick("chi0_i8 slices"), "sigc": pick("sigc_i8 slices")}
+    ns["products"] = {k: v * (v + 1) // 2 for k, v in list(ns.items())}
+    ns["estimates"] = {k: v for k, v in rep.items() if "err@" in k}
+    return ns
+
+
+def measure_int8_peak():
+    """int8 tensor throughput of a library GEMM (torch._int_mm, int8 x int8 -> int32,
+    8192^3, 2 n^3 ops): best of 5 (burst) and back to back for 2 s (sustained) --
+    the denominator of the int8 Ozaki path (a measurement only)."""
+    import torch
+    n = 8192
+    a = torch.randint(-64, 65, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-64, 65, (n, n), dtype=torch.int8, device="cuda")
+    torch._int_mm(a, b)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); torch._int_mm(a, b); e1.record(); torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    reps = max(1, int(2.0 / (2.0 * n ** 3 / (best * 1e12))))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        torch._int_mm(a, b)
+    e1.record(); torch.cuda.synchronize()
+    sus = reps * 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    del a, b
+    return {"burst_tops": round(best, 1), "sustained_tops": round(sus, 1), "reps": reps}
 
 
 def measure_fp64_peak():

@@ -19,6 +19,7 @@ TuneSuspend::TuneSuspend() { ++g_suspend; }
 TuneSuspend::~TuneSuspend() { --g_suspend; }
 static std::string g_path;
 static std::map<std::string, int> g_cache;
+static std::map<std::string, double> g_notes;   // error estimates of the slice-count trials (report only)
 
 static void load_cache() {
   std::ifstream f(g_path);
@@ -46,6 +47,18 @@ static std::string cache_json() {
     o += first ? "\"" : ", \"";
     o += kv.first + "\": " + std::to_string(kv.second);
     first = false;
+  }
+  return o + "}";
+}
+
+static std::string report_json() {
+  std::string o = cache_json();
+  if (g_notes.empty()) return o;
+  o.pop_back();                                  // the closing brace
+  char num[64];
+  for (const auto& kv : g_notes) {
+    std::snprintf(num, sizeof(num), "%.6e", kv.second);
+    o += (o.size() > 1 ? ", \"" : "\"") + kv.first + "\": " + num;
   }
   return o + "}";
 }
@@ -90,6 +103,31 @@ int tuned_choice(const std::string& key, const std::vector<int>& cands, int heur
   return QSGW_OK;
 }
 
+int tuned_slices(const std::string& key, const std::vector<int>& cands, int top, double tol,
+                 const std::function<int(int, double*)>& err, int fallback, int* chosen) {
+  *chosen = fallback;
+  auto it = g_cache.find(key);
+  if (it != g_cache.end()) {
+    *chosen = it->second;
+    return QSGW_OK;
+  }
+  if (g_suspend > 0 || ctx().capturing) return QSGW_OK;
+  *chosen = top;
+  for (int c : cands) {
+    double e = 0.0;
+    const int rc = err(c, &e);
+    if (rc) return rc;
+    g_notes[key + " err@" + std::to_string(c)] = e;
+    if (e <= tol) {
+      *chosen = c;
+      break;
+    }
+  }
+  g_cache[key] = *chosen;
+  save_cache();
+  return QSGW_OK;
+}
+
 }  // namespace qsgw
 
 using namespace qsgw;
@@ -106,7 +144,7 @@ extern "C" int qsgw_set_autotune(int mode, const char* cache_path) {
 
 extern "C" int qsgw_autotune_report(char* buf, int len) {
   if (!buf || len <= 0) return QSGW_ERR_ARG;
-  const std::string j = cache_json();
+  const std::string j = report_json();
   std::snprintf(buf, static_cast<size_t>(len), "%s", j.c_str());
   return static_cast<int>(j.size()) < len ? QSGW_OK : QSGW_ERR_ARG;
 }

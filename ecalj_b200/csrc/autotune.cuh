@@ -15,6 +15,14 @@ namespace qsgw {
 int tuned_choice(const std::string& key, const std::vector<int>& cands, int heuristic,
                  const std::function<int(int)>& run, cudaStream_t s, int* chosen, bool* tried);
 
+// Slice count of an int8 Ozaki contraction for problem `key`: the cached choice; else, unless
+// trials are suspended or a graph is being recorded, the first of `cands` (ascending) whose
+// error estimate err(ns, &e) is at most `tol` (the caller measures e against its most
+// accurate count), or the last candidate's successor `top` when none is; else `fallback`.
+// The estimates are kept for qsgw_autotune_report.
+int tuned_slices(const std::string& key, const std::vector<int>& cands, int top, double tol,
+                 const std::function<int(int, double*)>& err, int fallback, int* chosen);
+
 // While one of these lives, tuned_choice runs no trials (for calls that add into
 // an output the caller already holds, which a trial would clear).
 struct TuneSuspend {

@@ -12,6 +12,7 @@
 #include "zgemm_f64.cuh"
 #include "autotune.cuh"
 #include "split_f16.cuh"
+#include "ozaki_i8.cuh"
 #include "hoststage.cuh"
 
 namespace qsgw {
@@ -120,6 +121,27 @@ static int x0gemm_device(double2* rcxq, int npr, int ipr_col, int npr_col, int n
       bt.wts[fill[b]] = whwc[iw - iwini[c] + icouini[c] - 1];   // x0gemm.f90:62
       fill[b]++;
     }
+  }
+  if (ctx().prec_mode == QSGW_PREC_SPLIT_I8) {
+    // the same bins on the int8 tensor-core path: the pair columns and weights go to the device,
+    // each bin's entries form one K range; rcxq accumulates (no tuning trials)
+    int rc = g_x0_idx.ensure(std::max<size_t>(tot, 1) * sizeof(int));
+    if (rc) return rc;
+    rc = g_x0_w.ensure(std::max<size_t>(tot, 1) * sizeof(double));
+    if (rc) return rc;
+    if ((rc = h2d(g_x0_idx.p, bt.colidx.data(), tot * sizeof(int), s))) return rc;
+    if ((rc = h2d(g_x0_w.p, bt.wts.data(), tot * sizeof(double), s))) return rc;
+    OzChi0Bins ob;
+    ob.ebeg = bt.off;
+    ob.cnt = bt.cnt;
+    ob.slab = bt.slab;
+    int classes = 0;
+    for (double w : bt.wts) classes |= (w < 0.0 ? 1 : 0) | (w > 0.0 ? 2 : 0);
+    const bool herm = (ipr_col == 1 && npr_col == npr);
+    const int ns = ctx().nslices > 0 ? ctx().nslices : 4;   // rcxq accumulates: no trials, the accurate count
+    return chi0_split_i8(rcxq, npr, static_cast<long long>(npr) * npr_col, npr, npr_col, ipr_col - 1, herm, zmel, nbb,
+                         static_cast<long long>(nmz) * nqtot, g_x0_idx.as<int>(), g_x0_w.as<double>(), ob, classes,
+                         ns, s, nullptr);
   }
   ZParams p{};
   p.M = npr; p.N = npr_col;
@@ -249,9 +271,10 @@ __global__ void lorentz_real_weight_kernel(double* __restrict__ w, const int* __
 static DevBuf g_lz_map, g_lz_e, g_lz_w, g_lz_bins, g_lz_fi;
 
 // eta < 0: imaginary axis, nw slots of weights; eta >= 0: real axis, 2 nw slots (Re, Im).
+// classes (out): bit 0 when a weight can be negative, bit 1 when one can be positive
 int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc, const int* nun,
                          const double* eocc, const double* eunocc, long long& npair, double*& w_d,
-                         cudaStream_t s, double eta = -1.0, int nk_norm = 0) {
+                         cudaStream_t s, double eta = -1.0, int nk_norm = 0, int* classes = nullptr) {
   const double inv_nk = 1.0 / (nk_norm > 0 ? nk_norm : nk);   // 1/nk of the whole k mesh
   npair = 0;
   long long no_tot = 0, nu_tot = 0;
@@ -273,6 +296,17 @@ int chi0_lorentz_weights(int niw, const double* freq_i, int nk, const int* nocc,
       }
     oo += nocc[k];
     uo += nun[k];
+  }
+  if (classes) {
+    // imaginary axis: w = -2 de / (de^2 + w^2) / nk has the sign of -de; the real axis has both
+    int cl = 0;
+    if (eta >= 0.0) cl = 3;
+    else
+      for (long long i = 0; i < npair && cl != 3; ++i) {
+        const double de = eunocc[peu[i]] - eocc[peo[i]];
+        cl |= (de > 0.0 ? 1 : 0) | (de < 0.0 ? 2 : 0);
+      }
+    *classes = cl;
   }
   int rc = g_lz_map.ensure(2 * std::max<long long>(npair, 1) * sizeof(int));
   if (rc) return rc;
@@ -327,11 +361,12 @@ __global__ void combine_re_im_kernel(double2* __restrict__ chi, const double2* _
 }
 
 static DevBuf g_lzr_h;
+static DevBuf g_lz_ref, g_lz_try;       // chi0 of the slice-count trials
 
 }  // namespace qsgw
 
 static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int ldz, long long npair,
-                    const double* w_d, cudaStream_t s, bool accumulate = false);
+                    const double* w_d, cudaStream_t s, bool accumulate = false, int classes = 3);
 
 extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const double* freq_i, int nk,
                                    const int* nocc, const int* nun, const double* eocc,
@@ -345,21 +380,63 @@ extern "C" int qsgw_chi0_lorentz_d(double* chi0_d, int npr, int niw, const doubl
   cudaStream_t s = ctx().stream;
   long long npair = 0;
   double* w_d = nullptr;
-  rc = chi0_lorentz_weights(niw, freq_i, nk, nocc, nun, eocc, eunocc, npair, w_d, s);
+  int classes = 3;
+  rc = chi0_lorentz_weights(niw, freq_i, nk, nocc, nun, eocc, eunocc, npair, w_d, s, -1.0, 0, &classes);
   if (rc) return rc;
   QSGW_ARG(npair < (1LL << 31), "chi0_lorentz: %lld pairs exceed the 32-bit column index", npair);
-  return chi0_run(chi0_d, npr, niw, zcols_d, ldz, npair, w_d, s);
+  return chi0_run(chi0_d, npr, niw, zcols_d, ldz, npair, w_d, s, false, classes);
 }
 
 // chi0 slots iw = conj(Z) diag(w[iw]) Z^T for precomputed weights w (nslot x npair), in the
 // precision mode of the context; chi0_d is overwritten.
 static int chi0_run(double* chi0_d, int npr, int niw, const double* zcols_d, int ldz, long long npair,
-                    const double* w_d, cudaStream_t s, bool accumulate) {
+                    const double* w_d, cudaStream_t s, bool accumulate, int classes) {
   int rc = QSGW_OK;
   const size_t cbytes = static_cast<size_t>(npr) * npr * niw * 16;
   if (!accumulate) QSGW_CUDA(cudaMemsetAsync(chi0_d, 0, cbytes, s));
   if (npair == 0) return QSGW_OK;
   std::unique_ptr<TuneSuspend> hold(accumulate ? new TuneSuspend() : nullptr);   // trials would clear chi0
+  if (ctx().prec_mode == QSGW_PREC_SPLIT_I8) {
+    // one bin per frequency slot, every pair in every bin in column order (weights w[iw * npair + p])
+    OzChi0Bins ob;
+    for (int iw = 0; iw < niw; ++iw) {
+      ob.ebeg.push_back(static_cast<long long>(iw) * npair);
+      ob.cnt.push_back(static_cast<int>(npair));
+      ob.slab.push_back(iw);
+    }
+    auto run_ns = [&](int ns, double2* out, const char* tune) {
+      return chi0_split_i8(out, npr, static_cast<long long>(npr) * npr, npr, npr, 0, true,
+                           reinterpret_cast<const double2*>(zcols_d), ldz, npair, nullptr, w_d, ob, classes, ns, s,
+                           tune);
+    };
+    int ns = ctx().nslices;
+    if (ns == 0) {
+      // automatic slice count: the smallest whose chi0 stays within the relative target of the
+      // 4-slice one (trials on scratch copies; accumulating calls take the choice already made)
+      const long long nel = static_cast<long long>(npr) * npr * niw;
+      bool have_ref = false;
+      auto err = [&](int n, double* e) -> int {
+        int r = g_lz_ref.ensure(nel * sizeof(double2));
+        if (r) return r;
+        r = g_lz_try.ensure(nel * sizeof(double2));
+        if (r) return r;
+        if (!have_ref) {
+          QSGW_CUDA(cudaMemsetAsync(g_lz_ref.p, 0, nel * sizeof(double2), s));
+          if ((r = run_ns(4, g_lz_ref.as<double2>(), nullptr))) return r;
+          have_ref = true;
+        }
+        QSGW_CUDA(cudaMemsetAsync(g_lz_try.p, 0, nel * sizeof(double2), s));
+        if ((r = run_ns(n, g_lz_try.as<double2>(), nullptr))) return r;
+        return rel_diff_fro(g_lz_try.as<double2>(), g_lz_ref.as<double2>(), nel, s, e);
+      };
+      char key[160];
+      std::snprintf(key, sizeof(key), "chi0_i8 slices npr=%d npair~2^%.3f niw=%d", npr,
+                    std::round(8.0 * std::log2(static_cast<double>(npair))) / 8.0, niw);
+      rc = tuned_slices(key, {2, 3}, 4, ctx().chi0_rel_tol, err, 3, &ns);
+      if (rc) return rc;
+    }
+    return run_ns(ns, reinterpret_cast<double2*>(chi0_d), accumulate ? nullptr : "chi0_lorentz");
+  }
   if (ctx().prec_mode == QSGW_PREC_SPLIT_F16) {
     return chi0_split_f16(reinterpret_cast<double2*>(chi0_d), npr, niw,
                           reinterpret_cast<const double2*>(zcols_d), ldz, npair, w_d, s);
@@ -433,10 +510,11 @@ extern "C" int qsgw_chi0_lorentz_acc_d(double* chi0_d, int npr, int niw, const d
   cudaStream_t s = ctx().stream;
   long long npair = 0;
   double* w_d = nullptr;
-  rc = chi0_lorentz_weights(niw, freq_i, nkb, nocc, nun, eocc, eunocc, npair, w_d, s, -1.0, nk_total);
+  int classes = 3;
+  rc = chi0_lorentz_weights(niw, freq_i, nkb, nocc, nun, eocc, eunocc, npair, w_d, s, -1.0, nk_total, &classes);
   if (rc) return rc;
   QSGW_ARG(npair < (1LL << 31), "chi0_lorentz_acc: %lld pairs exceed the 32-bit column index", npair);
-  return chi0_run(chi0_d, npr, niw, zcols_d, ldz, npair, w_d, s, true);
+  return chi0_run(chi0_d, npr, niw, zcols_d, ldz, npair, w_d, s, true, classes);
 }
 
 extern "C" int qsgw_chi0_lorentz_real_d(double* chi0_d, int npr, int nw, const double* freq_r, double eta, int nk,

@@ -18,7 +18,9 @@ struct Context {
   cudaStream_t stream = nullptr;      // stream every entry point launches on
   bool own_stream = false;
   int prec_mode = QSGW_PREC_FP64;     // runtime precision switch
-  int nslices = 2;
+  int nslices = 2;                    // SPLIT_I8: 0 = chosen per contraction by the accuracy targets
+  double sigc_qp_tol = 1e-3 / 27.211386245988;   // Hartree: largest |Re Sigma_c,nn| change allowed (1 meV)
+  double chi0_rel_tol = 2e-5;         // relative Frobenius error allowed on chi0
   int sm_count = 148;
   int* d_flags = nullptr;             // device-side error/status words
   // CUDA graph of one recorded call sequence (qsgw_graph_*)

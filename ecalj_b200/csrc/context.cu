@@ -219,23 +219,39 @@ extern "C" int qsgw_synchronize(void) {
   QSGW_CUDA(cudaStreamSynchronize(c.stream));
   rc = host_stage_sync();
   if (rc) return rc;
-  int flag = 0;
-  QSGW_CUDA(cudaMemcpy(&flag, c.d_flags, sizeof(int), cudaMemcpyDeviceToHost));
-  if (flag) {
+  int flag[2] = {0, 0};
+  QSGW_CUDA(cudaMemcpy(flag, c.d_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag[0]) {
     QSGW_CUDA(cudaMemset(c.d_flags, 0, sizeof(int)));
     set_error("a pivot block of the Hermitian inverse was singular or not finite");
     return QSGW_ERR_NUMERIC;
+  }
+  if (flag[1]) {   // a tensor-core kernel gave up a bounded wait and skipped its output
+    QSGW_CUDA(cudaMemset(c.d_flags + 1, 0, sizeof(int)));
+    set_error("a split-precision kernel timed out waiting for its pipeline; its output is incomplete");
+    return QSGW_ERR_TIMEOUT;
   }
   return QSGW_OK;
 }
 
 extern "C" int qsgw_set_precision(int mode, int nslices) {
-  QSGW_ARG(mode == QSGW_PREC_FP64 || mode == QSGW_PREC_SPLIT_F16,
+  QSGW_ARG(mode == QSGW_PREC_FP64 || mode == QSGW_PREC_SPLIT_F16 || mode == QSGW_PREC_SPLIT_I8,
            "qsgw_set_precision: unknown mode %d", mode);
-  QSGW_ARG(mode == QSGW_PREC_FP64 || nslices == 2,
+  QSGW_ARG(mode != QSGW_PREC_SPLIT_F16 || nslices == 2,
            "qsgw_set_precision: SPLIT_F16 is built for 2 slices per operand (got %d)", nslices);
+  QSGW_ARG(mode != QSGW_PREC_SPLIT_I8 || nslices == 0 || (nslices >= 2 && nslices <= 4),
+           "qsgw_set_precision: SPLIT_I8 takes 2, 3 or 4 slices per operand, or 0 for automatic (got %d)",
+           nslices);
   ctx().prec_mode = mode;
   ctx().nslices = (mode == QSGW_PREC_FP64) ? 1 : nslices;
+  return QSGW_OK;
+}
+
+extern "C" int qsgw_set_accuracy(double sigc_qp_tol_ha, double chi0_rel_tol) {
+  QSGW_ARG(sigc_qp_tol_ha > 0.0 && chi0_rel_tol > 0.0, "qsgw_set_accuracy: targets must be positive (%g, %g)",
+           sigc_qp_tol_ha, chi0_rel_tol);
+  ctx().sigc_qp_tol = sigc_qp_tol_ha;
+  ctx().chi0_rel_tol = chi0_rel_tol;
   return QSGW_OK;
 }
 

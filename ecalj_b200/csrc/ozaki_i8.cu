@@ -1,0 +1,1170 @@
+// Ozaki-scheme complex contractions on the 5th-generation tensor cores: int8
+// slices, tcgen05.mma kind::i8 with exact INT32 accumulation in TMEM, operands
+// streamed by TMA into 64-byte-swizzled shared memory.
+//
+// Why int8.  The FP32 accumulation of tcgen05 kind::f16 truncates: the split
+// FP16 path carries a bias that grows with the accumulation length (about 4e-8
+// per K step, 3.7e-6 relative on a Sigma_c segment of K' = 1216) whatever the
+// slice count, and a bias in Sigma_c moves every QP energy the same way.
+// Integer products accumulate exactly; the only error left is the rounding of
+// the operands to NS slices, which is unbiased.
+//
+// The scheme.  Every row of A and every column of B gets a power-of-two scale
+// mu >= max |x| over its K range; with t = 64 x / mu in [-64, 64]
+//     s_1 = rint(t), t_1 = 128 (t - s_1), s_2 = rint(t_1), t_2 = 128 (t_1 - s_2), ...
+// every s_i lies in [-64, 64] (one int8) and every step is exact in FP64, so
+//     x = mu (s_1 2^-6 + s_2 2^-13 + ... + s_NS 2^-(7 NS - 1)) + r,  |r| <= mu 2^-(7 NS).
+// The product keeps the slice pairs (p, q) with p + q <= NS + 1 (the dropped
+// ones are below the rounding of the last slice), grouped by level
+// L = p + q - 2 into one INT32 TMEM accumulator per level (NS accumulators of
+// 128 columns); the drain combines the levels exactly in int64,
+//     v = sum_L acc_L 2^(7 (NS - 1 - L)),
+// and scales v by mu_row nu_col 2^-(12 + 7 (NS - 1)) in FP64.  A level holds at
+// most NS products of |s| <= 64 over K' real K, so |acc| < NS 2^12 K', which
+// bounds K' between drains (INT32).
+//
+// A complex product C = A B is one real GEMM with M doubled and K interleaved
+// (k' = 2k + {re, im}): rows (m, re) of A' = [Re a, -Im a], rows (m, im) =
+// [Im a, Re a], B' row n = [Re b, Im b]; lanes 0..63 of an accumulator hold
+// Re C, 64..127 Im C.  Negation commutes with the slicing (rint is symmetric),
+// so the slices of -x are the negated slices of x.
+//
+// Kernels (576 threads, one CTA per SM):
+//     warp 0        TMA producer
+//     warp 1        TMEM owner and MMA issuer (one thread)
+//     warps 2..17   drain (chi0: they also build the (m, im) rows of A' from
+//                   the (m, re) rows in shared memory, a byte shuffle)
+// Every mbarrier wait is bounded; on time-out the CTA records an error, waits
+// (bounded) for its own TMA and MMA work, frees TMEM and exits.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+#include "split_common.cuh"
+#include "ozaki_i8.cuh"
+#include "autotune.cuh"
+
+namespace qsgw {
+namespace oz {
+
+using namespace tc;
+
+constexpr int BM = 128;                  // accumulator rows (64 complex rows x {re, im})
+constexpr int BN = kOzTileN;             // accumulator columns (UMMA N)
+constexpr int K8 = 64;                   // int8 K per chunk: one 64-byte swizzled row
+constexpr int THREADS = 576;
+constexpr int NDW = 16;                  // drain warps 2..17
+constexpr int SLA8 = BM * K8;         // 8 KB: one slice of the A' tile of a stage
+constexpr int SLB8 = BN * K8;         // 8 KB: one slice of the B tile of a stage
+constexpr int STAGE_BUDGET = 192 * 1024;
+constexpr uint32_t TMEM8 = 512;
+
+template <int NS>
+struct Cfg {
+  static constexpr int STAGE = NS * (SLA8 + SLB8);
+  static constexpr int NST = STAGE_BUDGET / STAGE;                // 6, 4, 3 stages for NS = 2, 3, 4
+  static constexpr int OFF_A = 0;                                 // [NST][NS] A' slices
+  static constexpr int OFF_B = OFF_A + NST * NS * SLA8;        // [NST][NS] B slices
+  static constexpr int OFF_W = OFF_B + NST * NS * SLB8;        // drain column factors [16][32]
+  static constexpr int OFF_BAR = OFF_W + NDW * 32 * 8;
+  static constexpr int NBAR = 3 * NST + 3;                        // full, cfull, empty [NST]; accfull, accempty, done
+  static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
+  static constexpr int SMEM = OFF_MISC + 64 + 1024;               // + slack for the 1024-byte alignment
+  // exact INT32 levels: at most NS products of |s| <= 64 per K element
+  static constexpr int MAX_PERIOD = static_cast<int>((1LL << 30) / (NS * 4096LL * K8));
+  static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+  static_assert(NS * BN <= static_cast<int>(TMEM8), "one TMEM accumulator per level");
+};
+
+// kind::i8, A = B = signed 8-bit, D = S32, both K-major, M = 128, N = BN
+constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
+                              (static_cast<uint32_t>(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC_I8), "r"(accumulate));
+}
+
+// 32 lanes x 4 consecutive 32-bit TMEM columns
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+
+__device__ __forceinline__ unsigned char* align1024(unsigned char* p) {
+  return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+
+// the smallest power of two >= m (1 for m = 0 or not finite)
+__host__ __device__ __forceinline__ double pow2_at_least(double m) {
+  if (!(m > 0.0) || !isfinite(m)) return 1.0;
+  int e = 0;
+  frexp(m, &e);                          // m = f 2^e, f in [0.5, 1)
+  return ldexp(1.0, e);
+}
+
+// 2^(6 + 7 (NS - 1)): x / mu in [-1, 1] times this is the integer of NS base-128 digits
+template <int NS>
+__host__ __device__ constexpr double slice_unit() { return static_cast<double>(1LL << (6 + 7 * (NS - 1))); }
+
+// NS slices of x / mu, given scale = slice_unit<NS>() / mu (a power of two, so x * scale is exact):
+// V = rint(x * scale) (|V| <= 64 * 128^(NS-1)) written in base 128 from the bottom with digits
+// d = sign(V) r, r = |V| mod 128 taken in [-63, 64]; the top digit holds the rest.  Every digit
+// lies in [-64, 64] (one int8), negation commutes with the slicing, and the digits rebuild
+// x to mu 2^-(7 NS).  One FP64 multiply and round, then integer work only.
+template <int NS>
+__device__ __forceinline__ void slice(double x, double scale, int (&s)[NS]) {
+  long long v = __double2ll_rn(x * scale);
+#pragma unroll
+  for (int i = NS - 1; i >= 1; --i) {
+    const long long u = v < 0 ? -v : v;
+    int r = static_cast<int>(u & 127);
+    if (r > 64) r -= 128;
+    const int d = v < 0 ? -r : r;
+    s[i] = d;
+    v = (v - d) >> 7;                      // exact: v - d is a multiple of 128
+  }
+  s[0] = static_cast<int>(v);
+}
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+  return (static_cast<uint32_t>(a) & 0xFFu) | ((static_cast<uint32_t>(b) & 0xFFu) << 8) |
+         ((static_cast<uint32_t>(c) & 0xFFu) << 16) | ((static_cast<uint32_t>(d) & 0xFFu) << 24);
+}
+// (re, im) byte pairs -> (-im, re): the (m, im) row of A' from its (m, re) row
+__device__ __forceinline__ uint32_t rotate_pairs(uint32_t w) {
+  const uint32_t sw = __byte_perm(w, 0, 0x2301);           // [im0, re0, im1, re1]
+  return (__vneg4(sw) & 0x00FF00FFu) | (sw & 0xFF00FF00u);
+}
+
+// the extent of the chi0 weights of sign `sign` in bin b (0: the pass has nothing to do there)
+__device__ __forceinline__ double w_extent(const double* wr, int b, double sign) {
+  return sign < 0.0 ? wr[2 * b] : wr[2 * b + 1];
+}
+
+// =====================================================================================
+// Sigma_c: out(:, col) = sum over the segments of the column's group of W_slot^H (w_seg(col) z_col)
+struct SegParams {
+  int M;                      // complex rows (ngb)
+  int ntm;                    // 64-row tiles
+  int cps;                    // chunks per segment
+  int nslot, T;               // A' tile coordinate (q nslot + slot) T + mt
+  int nrows;                  // B rows per slice (tile-ordered columns)
+  const int* tile_group;
+  const int* tile_cols;
+  const int* group_seg_off;
+  const int* group_nseg;
+  const int* seg_slot;
+  const ZSeg* segs;
+  const double* mu_a;         // [slot][T * 64] row scales
+  const double* nu_b;         // [nrows] column scales
+  double post;                // 2^-(12 + 7 (NS - 1))
+  double2* C;
+  long long ldc;
+  int* err;
+};
+
+template <int NS>
+__global__ void __launch_bounds__(THREADS, 1)
+    oz_seg_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                  const SegParams p) {
+  using L = Cfg<NS>;
+  constexpr int NST = L::NST;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* sm = align1024(smem_raw);
+  unsigned char* sA = sm + L::OFF_A;
+  unsigned char* sB = sm + L::OFF_B;
+  double* sW = reinterpret_cast<double*>(sm + L::OFF_W);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::OFF_BAR);
+  uint64_t* full = bar;                  // [NST] TMA -> MMA
+  uint64_t* empty = bar + 2 * NST;       // [NST] MMA -> TMA
+  uint64_t* accfull = bar + 3 * NST;     // MMA -> drain
+  uint64_t* accempty = accfull + 1;      // drain -> MMA
+  uint64_t* done = accempty + 1;         // every MMA of the CTA retired
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::OFF_MISC);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::OFF_MISC + 8);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int mt = blockIdx.x % p.ntm, nt = blockIdx.x / p.ntm;
+  const int group = p.tile_group[nt];
+  const int nseg = p.group_nseg[group];
+  const int seg0 = p.group_seg_off[group];
+  const int nchunk = nseg * p.cps;
+
+  if (tid == 0) {
+    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, NDW);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM8));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (nchunk > 0) {
+    if (warp == 0 && lane == 0) {
+      // ---------------- TMA producer: NS slices of the segment's A' tile and of the B tile
+      constexpr uint32_t bytes = NS * (SLA8 + SLB8);
+      int issued = 0, sg = 0, cin = 0, st = 0, ph = 0;
+      int slot = p.seg_slot[seg0];
+      for (int c = 0; c < nchunk; ++c) {
+        if (c >= NST && !mbar_wait(&empty[st], ph ^ 1, abort_flag)) break;
+        issued = c + 1;
+        mbar_expect_tx(&full[st], bytes);
+        const int x = cin * K8;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          tma_load_4d(sA + (st * NS + q) * SLA8, &mapA, &full[st], x, 0, 0, (q * p.nslot + slot) * p.T + mt);
+          tma_load_3d(sB + (st * NS + q) * SLB8, &mapB, &full[st], x, nt * BN, q);
+        }
+        if (++cin == p.cps) {
+          cin = 0;
+          if (++sg < nseg) slot = p.seg_slot[seg0 + sg];
+        }
+        if (++st == NST) { st = 0; ph ^= 1; }
+      }
+      for (int c = max(0, issued - NST); c < issued; ++c) mbar_drain(&full[c % NST], (c / NST) & 1);
+    } else if (warp == 1 && lane == 0) {
+      // ---------------- MMA issuer: NS level accumulators, one accumulation period per segment
+      const uint64_t dA0 = sw64_desc(smem_u32(sA)), dB0 = sw64_desc(smem_u32(sB));
+      int seg = 0, cin = 0, st = 0, ph = 0;
+      for (int c = 0; c < nchunk && !*abort_flag; ++c) {
+        const bool first = cin == 0, last = cin == p.cps - 1;
+        if (first && seg >= 1 && !mbar_wait(accempty, (seg - 1) & 1, abort_flag)) break;
+        if (!mbar_wait(&full[st], ph, abort_flag)) break;
+        tc_fence_after();
+#pragma unroll
+        for (int kk = 0; kk < K8 / 32; ++kk) {       // 32 int8 = 32 B along K = 2 descriptor units
+#pragma unroll
+          for (int lv = 0; lv < NS; ++lv) {
+#pragma unroll
+            for (int pa = 0; pa <= lv; ++pa) {
+              const int qb = lv - pa;
+              const uint64_t da = dA0 + static_cast<uint32_t>(((st * NS + pa) * SLA8) >> 4) + 2 * kk;
+              const uint64_t db = dB0 + static_cast<uint32_t>(((st * NS + qb) * SLB8) >> 4) + 2 * kk;
+              umma_i8(tmem + static_cast<uint32_t>(lv * BN), da, db, (first && kk == 0 && pa == 0) ? 0u : 1u);
+            }
+          }
+        }
+        umma_commit(&empty[st]);
+        if (last) umma_commit(accfull);
+        if (++st == NST) { st = 0; ph ^= 1; }
+        if (++cin == p.cps) { cin = 0; ++seg; }
+      }
+      umma_commit(done);
+      mbar_drain(done, 0);
+    } else if (warp >= 2) {
+      // ---------------- drain: TMEM lanes 32 (warp mod 4) .. +31, 32 columns a warp, FP64 sums in registers
+      const int dw = warp - 2;
+      const int quad = warp & 3;
+      const int c_lo = (dw >> 2) * 32;
+      const int row = quad * 32 + lane;                 // accumulator row: 0..63 re, 64..127 im
+      const int mloc = row & 63;
+      const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
+      double* wsm = sW + dw * 32;
+      double acc[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+      bool ok = true;
+      const int rtile = nt * BN + c_lo;
+      for (int seg = 0; seg < nseg; ++seg) {
+        const ZSeg zs = p.segs[seg0 + seg];
+        const int slot = p.seg_slot[seg0 + seg];
+        __syncwarp();                                   // the previous segment's reads of wsm are done
+        {
+          const int col = p.tile_cols[rtile + lane];
+          wsm[lane] = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] * p.nu_b[rtile + lane] : 0.0;
+        }
+        const double rf = p.mu_a[static_cast<long long>(slot) * p.T * 64 + mt * 64 + mloc] * p.post;
+        __syncwarp();
+        if (!mbar_wait_warp(accfull, seg & 1, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+#pragma unroll
+        for (int blk = 0; blk < 8; ++blk) {             // 4 columns at a time (96 registers per thread)
+          uint32_t v[NS][4];
+#pragma unroll
+          for (int lv = 0; lv < NS; ++lv)
+            tmem_ld4(tmem + lane_base + static_cast<uint32_t>(lv * BN + c_lo + blk * 4), v[lv]);
+          tmem_wait_ld();
+          if (blk == 7) {                               // every TMEM read of this segment is done
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(accempty);
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            long long comb = static_cast<int>(v[0][j]);
+#pragma unroll
+            for (int lv = 1; lv < NS; ++lv) comb = comb * 128 + static_cast<int>(v[lv][j]);
+            acc[blk * 4 + j] = fma(static_cast<double>(comb) * rf, wsm[blk * 4 + j], acc[blk * 4 + j]);
+          }
+        }
+      }
+      if (ok && !*abort_flag) {
+        const int m = mt * 64 + mloc;
+        const int part = row >= 64 ? 1 : 0;
+        if (m < p.M) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = p.tile_cols[rtile + j];
+            if (col >= 0) reinterpret_cast<double*>(p.C + m + static_cast<long long>(col) * p.ldc)[part] = acc[j];
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  if (*abort_flag && tid == 0) atomicExch(p.err, 2);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM8));
+  }
+}
+
+// =====================================================================================
+// chi0: C(:, :, slab_b) += sign sum_{e in bin b} conj(y_e(0:M)) y_e(row_b0 : row_b0 + N)^T,
+// y_e = sqrt(sign w_e) z_col(e) sliced in HBM as Y8[slice][row][K'] (the (m, re) rows of A' and
+// the rows of B are both rows of Y8; the (m, im) rows are rotated from them in shared memory)
+struct HerkParams {
+  int M, N;                   // output rows / columns
+  int ntm;                    // 64-row tiles
+  int herm;
+  int row_b0;
+  int Rows;                   // rows of Y8 per slice
+  const long long* bin_k0;    // first K chunk of bin b in Y8
+  const int* bin_nch;         // K chunks of bin b
+  const int* bin_slab;
+  const double* wrange;       // [bin][2]: largest -w and largest w (0 when none)
+  const double* mu;           // [bin][Rows] row scales of y
+  double sign;                // -1 or +1: the weight class of this pass
+  double post;
+  double2* C;
+  long long ldc, c_bs;
+  int* err;
+};
+
+template <int NS>
+__global__ void __launch_bounds__(THREADS, 1)
+    oz_herk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                   const HerkParams p) {
+  using L = Cfg<NS>;
+  constexpr int NST = L::NST;
+  constexpr int PER = L::MAX_PERIOD;
+  constexpr int HALF = SLA8 / 2;      // the (m, re) half of an A' slice: 64 rows x 64 B
+  const int mt = blockIdx.x % p.ntm, nt = blockIdx.x / p.ntm;
+  const int bin = blockIdx.y;
+  if (p.herm && mt * 64 + 63 < nt * BN) return;              // strictly upper tile: mirrored
+  if (!(w_extent(p.wrange, bin, p.sign) > 0.0)) return;       // no weight of this sign in the bin
+  const int nch = p.bin_nch[bin];
+  const int per_split = (nch + gridDim.z - 1) / gridDim.z;
+  const int cbeg = blockIdx.z * per_split;
+  const int nchunk = min(nch, cbeg + per_split) - cbeg;
+  if (nchunk <= 0) return;
+  const int kc0 = static_cast<int>(p.bin_k0[bin] + cbeg);    // first chunk of this CTA in Y8
+
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* sm = align1024(smem_raw);
+  unsigned char* sA = sm + L::OFF_A;
+  unsigned char* sB = sm + L::OFF_B;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::OFF_BAR);
+  uint64_t* full = bar;                  // [NST] TMA -> converters
+  uint64_t* cfull = bar + NST;           // [NST] converters -> MMA
+  uint64_t* empty = bar + 2 * NST;       // [NST] MMA -> TMA
+  uint64_t* accfull = bar + 3 * NST;
+  uint64_t* accempty = accfull + 1;
+  uint64_t* done = accempty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::OFF_MISC);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::OFF_MISC + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nper = (nchunk + PER - 1) / PER;
+
+  if (tid == 0) {
+    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&cfull[i], NDW); mbar_init(&empty[i], 1); }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, NDW);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM8));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer: the (m, re) half of the A' tile and the B tile, NS slices each
+    constexpr uint32_t bytes = NS * (HALF + SLB8);
+    int issued = 0, st = 0, ph = 0;
+    for (int c = 0; c < nchunk; ++c) {
+      if (c >= NST && !mbar_wait(&empty[st], ph ^ 1, abort_flag)) break;
+      issued = c + 1;
+      mbar_expect_tx(&full[st], bytes);
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        tma_load_4d(sA + (st * NS + q) * SLA8, &mapA, &full[st], 0, mt * 64, q, kc0 + c);
+        tma_load_4d(sB + (st * NS + q) * SLB8, &mapB, &full[st], 0, p.row_b0 + nt * BN, q, kc0 + c);
+      }
+      if (++st == NST) { st = 0; ph ^= 1; }
+    }
+    for (int c = max(0, issued - NST); c < issued; ++c) mbar_drain(&full[c % NST], (c / NST) & 1);
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer: periods of at most PER chunks (exact INT32 levels)
+    const uint64_t dA0 = sw64_desc(smem_u32(sA)), dB0 = sw64_desc(smem_u32(sB));
+    int st = 0, ph = 0, cin = 0, per = 0;
+    for (int c = 0; c < nchunk && !*abort_flag; ++c) {
+      const bool first = cin == 0;
+      const bool last = cin == PER - 1 || c == nchunk - 1;
+      if (first && per >= 1 && !mbar_wait(accempty, (per - 1) & 1, abort_flag)) break;
+      if (!mbar_wait(&cfull[st], ph, abort_flag)) break;
+      tc_fence_after();
+#pragma unroll
+      for (int kk = 0; kk < K8 / 32; ++kk) {
+#pragma unroll
+        for (int lv = 0; lv < NS; ++lv) {
+#pragma unroll
+          for (int pa = 0; pa <= lv; ++pa) {
+            const int qb = lv - pa;
+            const uint64_t da = dA0 + static_cast<uint32_t>(((st * NS + pa) * SLA8) >> 4) + 2 * kk;
+            const uint64_t db = dB0 + static_cast<uint32_t>(((st * NS + qb) * SLB8) >> 4) + 2 * kk;
+            umma_i8(tmem + static_cast<uint32_t>(lv * BN), da, db, (first && kk == 0 && pa == 0) ? 0u : 1u);
+          }
+        }
+      }
+      umma_commit(&empty[st]);
+      if (last) umma_commit(accfull);
+      if (++st == NST) { st = 0; ph ^= 1; }
+      if (last) { cin = 0; ++per; } else { ++cin; }
+    }
+    umma_commit(done);
+    mbar_drain(done, 0);
+  } else if (warp >= 2) {
+    // ---------------- converters + drain (warps 2..17)
+    const int dw = warp - 2;
+    const int ct = tid - 64;                            // 0..511
+    const int quad = warp & 3;
+    const int c_lo = (dw >> 2) * 32;
+    const int row = quad * 32 + lane;
+    const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
+    long long acc[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc[j] = 0;
+    bool ok = true;
+    int st = 0, ph = 0, cin = 0, per = 0;
+    for (int c = 0; c < nchunk; ++c) {
+      if (!mbar_wait_warp(&full[st], ph, abort_flag)) { ok = false; break; }
+      // the (m, im) rows [-Im y, Re y] from the (m, re) rows [Re y, Im y]: same swizzled offsets
+      // (rows r and r + 64 share their 64-byte swizzle pattern)
+      for (int i = ct; i < NS * (HALF / 16); i += NDW * 32) {
+        const int q = i / (HALF / 16), j = i % (HALF / 16);
+        const uint4 v = *reinterpret_cast<const uint4*>(sA + (st * NS + q) * SLA8 + j * 16);
+        uint4 o;
+        o.x = rotate_pairs(v.x); o.y = rotate_pairs(v.y); o.z = rotate_pairs(v.z); o.w = rotate_pairs(v.w);
+        *reinterpret_cast<uint4*>(sA + (st * NS + q) * SLA8 + HALF + j * 16) = o;
+      }
+      fence_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&cfull[st]);
+      if (++st == NST) { st = 0; ph ^= 1; }
+      const bool last = cin == PER - 1 || c == nchunk - 1;
+      if (!last) { ++cin; continue; }
+      cin = 0;
+      // drain the period: exact int64 sums of the combined levels
+      if (!mbar_wait_warp(accfull, per & 1, abort_flag)) { ok = false; break; }
+      tc_fence_after();
+#pragma unroll
+      for (int blk = 0; blk < 8; ++blk) {
+        uint32_t v[NS][4];
+#pragma unroll
+        for (int lv = 0; lv < NS; ++lv)
+          tmem_ld4(tmem + lane_base + static_cast<uint32_t>(lv * BN + c_lo + blk * 4), v[lv]);
+        tmem_wait_ld();
+        if (blk == 7) {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(accempty);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          long long comb = static_cast<int>(v[0][j]);
+#pragma unroll
+          for (int lv = 1; lv < NS; ++lv) comb = comb * 128 + static_cast<int>(v[lv][j]);
+          acc[blk * 4 + j] += comb;
+        }
+      }
+      ++per;
+    }
+    if (ok && per == nper && !*abort_flag) {
+      const int m = mt * 64 + (row & 63);
+      const int part = row >= 64 ? 1 : 0;
+      if (m < p.M) {
+        const double* mub = p.mu + static_cast<long long>(bin) * p.Rows;
+        const double fm = mub[m] * p.post * p.sign;
+        double2* Cb = p.C + static_cast<long long>(p.bin_slab[bin]) * p.c_bs;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int n = nt * BN + c_lo + j;
+          // the upper part of a Hermitian output comes from the mirror
+          if (n < p.N && !(p.herm && m < n)) {
+            const double val = static_cast<double>(acc[j]) * fm * mub[p.row_b0 + n];
+            atomicAdd(reinterpret_cast<double*>(Cb + m + static_cast<long long>(n) * p.ldc) + part, val);
+            if (p.herm && m > n)                          // C(n, m) = conj(C(m, n))
+              atomicAdd(reinterpret_cast<double*>(Cb + n + static_cast<long long>(m) * p.ldc) + part,
+                        part ? -val : val);
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  if (*abort_flag && tid == 0) atomicExch(p.err, 2);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM8));
+  }
+}
+
+// =====================================================================================
+// operand preparation (HBM-bound)
+
+// out[slot * ncols_out + j] = power-of-two scale of column c = colmap[j] (or j) of the complex
+// column-major matrix src + slot * slot_stride (leading dimension ld): max over k < K of
+// max(|Re|, |Im|); 1 for absent columns.  One warp per column.
+__global__ void oz_colscale_kernel(const double2* __restrict__ src, long long ld, long long slot_stride, int K,
+                                   int ncols_valid, const int* __restrict__ colmap, int ncols_out,
+                                   double* __restrict__ out) {
+  const int slot = blockIdx.y;
+  const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= ncols_out) return;
+  const int c = colmap ? colmap[j] : (j < ncols_valid ? j : -1);
+  double m = 0.0;
+  if (c >= 0) {
+    const double2* col = src + static_cast<long long>(slot) * slot_stride + static_cast<long long>(c) * ld;
+    for (int k = lane; k < K; k += 32) {
+      const double2 v = col[k];
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) out[static_cast<long long>(slot) * ncols_out + j] = pow2_at_least(m);
+}
+
+// Sigma_c A' slices from W: A(m, k) = conj(W_slot[k + m ld]) into
+// [q][slot_out0 + slot][t][half][64][Kp] int8; each thread four consecutive k of one row.
+// grid (ceil(Kp/2 / 128), nslot * T), block 256: warp w rows w, w + 8, ..
+template <int NS>
+__global__ void oz_slice_w_kernel(int8_t* __restrict__ out, const double2* __restrict__ w, long long ld,
+                                  long long slot_stride, int ngb, int T, int nslot_total, int slot_out0, int Kp,
+                                  const double* __restrict__ mu) {
+  const int st = blockIdx.y;                           // slot * T + t of this launch
+  const int t = st % T, slot = st / T;
+  const int k0 = (blockIdx.x * 32 + (threadIdx.x & 31)) * 4;
+  if (k0 >= Kp / 2) return;
+  const int gslot = slot_out0 + slot;
+  for (int mm = threadIdx.x >> 5; mm < 64; mm += 8) {
+    const int m = t * 64 + mm;
+    const double inv = slice_unit<NS>() / mu[static_cast<long long>(gslot) * T * 64 + m];
+    int sr[4][NS], si[4][NS];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int k = k0 + i;
+      double2 v = make_double2(0.0, 0.0);
+      if (m < ngb && k < ngb) v = w[static_cast<long long>(slot) * slot_stride + k + static_cast<long long>(m) * ld];
+      slice<NS>(v.x, inv, sr[i]);                      // Re a
+      slice<NS>(-v.y, inv, si[i]);                     // Im a  (a = conj(W))
+    }
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const long long r0 = ((static_cast<long long>(q) * nslot_total + gslot) * T + t) * 128 + mm;
+      uint2 h0, h1;                                    // half 0: [Re a, -Im a]; half 1: [Im a, Re a]
+      h0.x = pack4(sr[0][q], -si[0][q], sr[1][q], -si[1][q]);
+      h0.y = pack4(sr[2][q], -si[2][q], sr[3][q], -si[3][q]);
+      h1.x = pack4(si[0][q], sr[0][q], si[1][q], sr[1][q]);
+      h1.y = pack4(si[2][q], sr[2][q], si[3][q], sr[3][q]);
+      *reinterpret_cast<uint2*>(out + r0 * Kp + 2 * k0) = h0;
+      *reinterpret_cast<uint2*>(out + (r0 + 64) * Kp + 2 * k0) = h1;
+    }
+  }
+}
+
+// Sigma_c B slices: row r = zmel column cols[r] (-1: zero row), [Re b, Im b] per k, into [q][nrows][Kp].
+// grid (ceil(Kp/2 / 128), ceil(nrows / 8)), block 256: one row per warp
+template <int NS>
+__global__ void oz_slice_z_kernel(int8_t* __restrict__ out, const double2* __restrict__ z, long long ld, int K,
+                                  const int* __restrict__ cols, int nrows, int Kp, const double* __restrict__ nu) {
+  const int r = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int k0 = (blockIdx.x * 32 + (threadIdx.x & 31)) * 4;
+  if (r >= nrows || k0 >= Kp / 2) return;
+  const int c = cols[r];
+  const double inv = slice_unit<NS>() / nu[r];
+  int sr[4][NS], si[4][NS];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int k = k0 + i;
+    double2 v = make_double2(0.0, 0.0);
+    if (c >= 0 && k < K) v = z[k + static_cast<long long>(c) * ld];
+    slice<NS>(v.x, inv, sr[i]);
+    slice<NS>(v.y, inv, si[i]);
+  }
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    uint2 h;
+    h.x = pack4(sr[0][q], si[0][q], sr[1][q], si[1][q]);
+    h.y = pack4(sr[2][q], si[2][q], sr[3][q], si[3][q]);
+    *reinterpret_cast<uint2*>(out + (static_cast<long long>(q) * nrows + r) * Kp + 2 * k0) = h;
+  }
+}
+
+// chi0: per-row max over every column of z (rows < Rows), as the bits of a non-negative double
+__global__ void oz_rowmax_kernel(const double2* __restrict__ z, long long ldz, int Rows, long long ncols,
+                                 unsigned long long* __restrict__ out) {
+  for (int m = threadIdx.x; m < Rows; m += blockDim.x) {
+    double mx = 0.0;
+    for (long long c = blockIdx.x; c < ncols; c += gridDim.x) {
+      const double2 v = z[m + c * ldz];
+      mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+    atomicMax(out + m, static_cast<unsigned long long>(__double_as_longlong(mx)));
+  }
+}
+
+// chi0: the weight extents of every bin, wr[2 b] = max(-w, 0) and wr[2 b + 1] = max(w, 0) over its
+// entries, as the bits of non-negative doubles (atomicMax; zeroed by the caller).  grid (x, bins).
+__global__ void oz_wrange_kernel(const double* __restrict__ ew, const long long* __restrict__ ebeg,
+                                 const int* __restrict__ cnt, unsigned long long* __restrict__ wr) {
+  const int b = blockIdx.y;
+  double neg = 0.0, pos = 0.0;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < cnt[b];
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const double w = ew[ebeg[b] + e];
+    neg = fmax(neg, -w);
+    pos = fmax(pos, w);
+  }
+  for (int o = 16; o; o >>= 1) {
+    neg = fmax(neg, __shfl_xor_sync(0xffffffffu, neg, o));
+    pos = fmax(pos, __shfl_xor_sync(0xffffffffu, pos, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (neg > 0.0) atomicMax(wr + 2 * b, static_cast<unsigned long long>(__double_as_longlong(neg)));
+    if (pos > 0.0) atomicMax(wr + 2 * b + 1, static_cast<unsigned long long>(__double_as_longlong(pos)));
+  }
+}
+
+// chi0: mu[b][m] = 2^e >= sqrt(largest sign * w of bin b) * zmax[m], a bound on |y| over the bin's row m
+__global__ void oz_mu_kernel(const unsigned long long* __restrict__ zmax, const double* __restrict__ wr, int Rows,
+                             int nbins, double sign, double* __restrict__ mu) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i >= static_cast<long long>(Rows) * nbins) return;
+  const int b = static_cast<int>(i / Rows), m = static_cast<int>(i % Rows);
+  mu[i] = pow2_at_least(sqrt(w_extent(wr, b, sign)) * __longlong_as_double(static_cast<long long>(zmax[m])));
+}
+
+// chi0: Y8[q][m][k0_b + 2 e' + {0,1}] = slices of (Re, Im) of sqrt(max(sign w_e, 0)) z_col(e)(m).
+// blockIdx.y = bin; blockIdx.x strides over (entry block of 32, 64-row tile) items of the bin.
+// Thread (row mm, group g) slices the 8 consecutive entries 8 g .. 8 g + 7 of its row (loads
+// coalesced along m), the 16 bytes per slice go to a shared tile with 80-byte rows (no bank
+// conflicts), and 64 rows x 64 bytes per slice leave coalesced along K.
+template <int NS>
+__device__ __forceinline__ void y_tile_pack(int8_t (*tile)[64][80], int mm, int g, const double (&f)[8],
+                                            const double2 (&zv)[8], double scale) {
+  uint32_t w[NS][4];
+#pragma unroll
+  for (int jp = 0; jp < 4; ++jp) {
+    int r0[NS], i0[NS], r1[NS], i1[NS];
+    slice<NS>(f[2 * jp] * zv[2 * jp].x, scale, r0);
+    slice<NS>(f[2 * jp] * zv[2 * jp].y, scale, i0);
+    slice<NS>(f[2 * jp + 1] * zv[2 * jp + 1].x, scale, r1);
+    slice<NS>(f[2 * jp + 1] * zv[2 * jp + 1].y, scale, i1);
+#pragma unroll
+    for (int q = 0; q < NS; ++q) w[q][jp] = pack4(r0[q], i0[q], r1[q], i1[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < NS; ++q)
+    *reinterpret_cast<uint4*>(&tile[q][mm][g * 16]) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+}
+
+// Y8 is chunk-major: [chunk][slice][row][64 bytes], so one TMA box (64 or 128 rows of one chunk
+// and slice) is one contiguous block of HBM
+template <int NS>
+__device__ __forceinline__ void y_tile_store(int8_t* __restrict__ y8, const int8_t (*tile)[64][80], int Rows, int rt,
+                                             long long chunk) {
+  const int row = threadIdx.x >> 2, part = threadIdx.x & 3;
+  const int mo = rt * 64 + row;
+  if (mo < Rows) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q)
+      *reinterpret_cast<uint4*>(y8 + ((chunk * NS + q) * Rows + mo) * 64 + part * 16) =
+          *reinterpret_cast<const uint4*>(&tile[q][row][part * 16]);
+  }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256)
+    oz_slice_y_kernel(int8_t* __restrict__ y8, int Rows, const double2* __restrict__ z, long long ldz,
+                      const int* __restrict__ ecol, const double* __restrict__ ew, const long long* __restrict__ ebeg,
+                      const int* __restrict__ cnt, const long long* __restrict__ bin_k0,
+                      const double* __restrict__ wr, const double* __restrict__ mu, double sign) {
+  __shared__ __align__(16) int8_t tile[NS][64][80];
+  const int b = blockIdx.y;
+  if (!(w_extent(wr, b, sign) > 0.0)) return;
+  const int n = cnt[b];
+  const int neb = (n + 31) / 32;
+  const int nrt = (Rows + 63) / 64;
+  const long long e0 = ebeg[b];
+  const long long kc = bin_k0[b];
+  const double* mub = mu + static_cast<long long>(b) * Rows;
+  const int mm = threadIdx.x & 63, g = threadIdx.x >> 6;
+  for (long long item = blockIdx.x; item < static_cast<long long>(neb) * nrt; item += gridDim.x) {
+    const int eb = static_cast<int>(item % neb), rt = static_cast<int>(item / neb);
+    const int m = rt * 64 + mm;
+    const double scale = (m < Rows) ? slice_unit<NS>() / mub[m] : 0.0;
+    double f[8];
+    double2 zv[8];
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+      const int e = eb * 32 + g * 8 + jj;
+      f[jj] = 0.0;
+      zv[jj] = make_double2(0.0, 0.0);
+      if (e < n && m < Rows) {
+        const long long ge = e0 + e;
+        const long long col = ecol ? ecol[ge] : e;
+        f[jj] = sqrt(fmax(sign * ew[ge], 0.0));
+        zv[jj] = z[m + col * ldz];
+      }
+    }
+    y_tile_pack<NS>(tile, mm, g, f, zv, scale);
+    __syncthreads();
+    y_tile_store<NS>(y8, tile, Rows, rt, kc + eb);
+    __syncthreads();
+  }
+}
+
+// chi0, every bin over the same columns 0..n-1 in order (bin b's weights at ew[b * n + e]): z is read
+// once per (32-column block, 64-row tile) item and sliced for every bin with a weight of this sign;
+// the 32 weights' square roots of a bin are formed once per item in shared memory.
+template <int NS>
+__global__ void __launch_bounds__(256)
+    oz_slice_y_dense_kernel(int8_t* __restrict__ y8, int Rows, const double2* __restrict__ z,
+                            long long ldz, int n, int nbins, const double* __restrict__ ew,
+                            const long long* __restrict__ bin_k0, const double* __restrict__ wr,
+                            const double* __restrict__ mu, double sign) {
+  __shared__ __align__(16) int8_t tile[NS][64][80];
+  __shared__ double sf[32];
+  const int neb = (n + 31) / 32;
+  const int nrt = (Rows + 63) / 64;
+  const int mm = threadIdx.x & 63, g = threadIdx.x >> 6;
+  for (long long item = blockIdx.x; item < static_cast<long long>(neb) * nrt; item += gridDim.x) {
+    const int eb = static_cast<int>(item % neb), rt = static_cast<int>(item / neb);
+    const int m = rt * 64 + mm;
+    double2 zv[8];
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+      const int e = eb * 32 + g * 8 + jj;
+      zv[jj] = (e < n && m < Rows) ? z[m + static_cast<long long>(e) * ldz] : make_double2(0.0, 0.0);
+    }
+    for (int b = 0; b < nbins; ++b) {
+      if (!(w_extent(wr, b, sign) > 0.0)) continue;                 // uniform over the block
+      if (threadIdx.x < 32) {
+        const int e = eb * 32 + threadIdx.x;
+        sf[threadIdx.x] = (e < n) ? sqrt(fmax(sign * ew[static_cast<long long>(b) * n + e], 0.0)) : 0.0;
+      }
+      __syncthreads();
+      double f[8];
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) f[jj] = sf[g * 8 + jj];
+      const double scale = (m < Rows) ? slice_unit<NS>() / mu[static_cast<long long>(b) * Rows + m] : 0.0;
+      y_tile_pack<NS>(tile, mm, g, f, zv, scale);
+      __syncthreads();
+      y_tile_store<NS>(y8, tile, Rows, rt, bin_k0[b] + eb);
+      __syncthreads();
+    }
+  }
+}
+
+// out[0] += sum |a - b|^2, out[1] += sum |b|^2 (one atomic pair per block)
+__global__ void oz_diff_norm_kernel(const double2* __restrict__ a, const double2* __restrict__ b, long long n,
+                                    double* __restrict__ out) {
+  __shared__ double sd[8], sb[8];
+  double d = 0.0, r = 0.0;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const double2 x = a[i], y = b[i];
+    d += (x.x - y.x) * (x.x - y.x) + (x.y - y.y) * (x.y - y.y);
+    r += y.x * y.x + y.y * y.y;
+  }
+  for (int o = 16; o; o >>= 1) {
+    d += __shfl_xor_sync(0xffffffffu, d, o);
+    r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  if ((threadIdx.x & 31) == 0) { sd[threadIdx.x >> 5] = d; sb[threadIdx.x >> 5] = r; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < static_cast<int>(blockDim.x >> 5); ++i) { d += sd[i]; r += sb[i]; }
+    atomicAdd(out, d);
+    atomicAdd(out + 1, r);
+  }
+}
+
+// =====================================================================================
+// host side
+
+static DevBuf g_a8, g_b8, g_mu, g_nu, g_tabs;          // Sigma_c
+static DevBuf g_y8, g_ymu, g_zmax, g_wr, g_bins;       // chi0
+
+template <int NS>
+static int launch_seg(const CUtensorMap& ma, const CUtensorMap& mb, const SegParams& p, dim3 grid, cudaStream_t s) {
+  static uint64_t attr = 0;                             // one bit per device
+  int rc = smem_limit_once(reinterpret_cast<const void*>(oz_seg_kernel<NS>), Cfg<NS>::SMEM, attr);
+  if (rc) return rc;
+  const int pi = prof_begin("sigc_seg_tc", s);
+  oz_seg_kernel<NS><<<grid, THREADS, Cfg<NS>::SMEM, s>>>(ma, mb, p);
+  prof_end(pi, s);
+  count_launch();
+  QSGW_LAUNCH_CHECK("oz_seg_kernel");
+  return QSGW_OK;
+}
+
+template <int NS>
+static int launch_herk(const CUtensorMap& ma, const CUtensorMap& mb, const HerkParams& p, dim3 grid,
+                       cudaStream_t s) {
+  static uint64_t attr = 0;
+  int rc = smem_limit_once(reinterpret_cast<const void*>(oz_herk_kernel<NS>), Cfg<NS>::SMEM, attr);
+  if (rc) return rc;
+  const int pi = prof_begin("chi0_tc", s);
+  oz_herk_kernel<NS><<<grid, THREADS, Cfg<NS>::SMEM, s>>>(ma, mb, p);
+  prof_end(pi, s);
+  count_launch();
+  QSGW_LAUNCH_CHECK("oz_herk_kernel");
+  return QSGW_OK;
+}
+
+static double post_scale(int ns) { return std::ldexp(1.0, -(12 + 7 * (ns - 1))); }
+
+}  // namespace oz
+
+using namespace oz;
+
+int rel_diff_fro(const double2* a, const double2* b, long long n, cudaStream_t s, double* rel) {
+  static DevBuf acc;
+  int rc = acc.ensure(2 * sizeof(double));
+  if (rc) return rc;
+  QSGW_CUDA(cudaMemsetAsync(acc.p, 0, 2 * sizeof(double), s));
+  const int g = static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 8LL * ctx().sm_count)));
+  oz_diff_norm_kernel<<<g, 256, 0, s>>>(a, b, n, acc.as<double>());
+  count_launch();
+  QSGW_LAUNCH_CHECK("oz_diff_norm_kernel");
+  double h[2] = {0.0, 0.0};
+  QSGW_CUDA(cudaMemcpyAsync(h, acc.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  QSGW_CUDA(cudaStreamSynchronize(s));
+  *rel = h[1] > 0.0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+  return QSGW_OK;
+}
+
+int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
+  QSGW_ARG(ns >= 2 && ns <= 4, "sigc split-i8: %d slices (2..4)", ns);
+  const int ngb = a.ngb;
+  const int T = (ngb + 63) / 64;
+  const int Kp = ((2 * ngb + K8 - 1) / K8) * K8;
+  // exact INT32 levels over one segment (K' = Kp): ns * 4096 * Kp < 2^31
+  QSGW_ARG(static_cast<long long>(ns) * 4096 * Kp < (1LL << 31), "sigc split-i8: ngb=%d too large", ngb);
+  const int nslot = a.nimag + a.nreal;
+  const int ntiles = static_cast<int>(a.tile_group.size());
+  QSGW_ARG(a.tile_cols.size() == static_cast<size_t>(ntiles) * BN, "sigc split-i8: %zu tile columns for %d tiles",
+           a.tile_cols.size(), ntiles);
+  const int nrows = ntiles * BN;
+  const size_t a_bytes = static_cast<size_t>(ns) * nslot * T * 128 * Kp;
+  const size_t b_bytes = static_cast<size_t>(ns) * nrows * Kp;
+  int rc = g_a8.ensure(a_bytes);
+  if (rc) return rc;
+  rc = g_b8.ensure(b_bytes);
+  if (rc) return rc;
+  rc = g_mu.ensure(static_cast<size_t>(nslot) * T * 64 * sizeof(double));
+  if (rc) return rc;
+  rc = g_nu.ensure(static_cast<size_t>(nrows) * sizeof(double));
+  if (rc) return rc;
+  // tables
+  rc = g_tabs.ensure((a.tile_cols.size() + a.tile_group.size() + a.group_seg_off.size() + a.group_nseg.size() +
+                      a.seg_slot.size() + 16) * sizeof(int) + a.segs.size() * sizeof(ZSeg) + 256);
+  if (rc) return rc;
+  unsigned char* tb = g_tabs.as<unsigned char>();
+  size_t off = 0;
+  int cprc = 0;
+  auto put = [&](const void* src, size_t n) -> const void* {
+    void* dst = tb + off;
+    if (!cprc && n) cprc = h2d(dst, src, n, s);
+    off += (n + 15) & ~size_t(15);
+    return dst;
+  };
+  const ZSeg* d_segs = reinterpret_cast<const ZSeg*>(put(a.segs.data(), a.segs.size() * sizeof(ZSeg)));
+  const int* d_cols = reinterpret_cast<const int*>(put(a.tile_cols.data(), a.tile_cols.size() * sizeof(int)));
+  const int* d_tg = reinterpret_cast<const int*>(put(a.tile_group.data(), a.tile_group.size() * sizeof(int)));
+  const int* d_gso = reinterpret_cast<const int*>(put(a.group_seg_off.data(), a.group_seg_off.size() * sizeof(int)));
+  const int* d_gns = reinterpret_cast<const int*>(put(a.group_nseg.data(), a.group_nseg.size() * sizeof(int)));
+  const int* d_slot = reinterpret_cast<const int*>(put(a.seg_slot.data(), a.seg_slot.size() * sizeof(int)));
+  if (cprc) return cprc;
+  double* mu = g_mu.as<double>();
+  double* nu = g_nu.as<double>();
+  // row scales of A' (= column scales of every W record) and column scales of B
+  oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nimag), 256, 0, s>>>(a.wi, a.ldw, a.ldw * a.ldw, ngb, ngb, nullptr,
+                                                                    T * 64, mu);
+  count_launch();
+  if (a.nreal > 0) {
+    oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nreal), 256, 0, s>>>(a.wr, a.ldw, a.ldw * a.ldw, ngb, ngb, nullptr,
+                                                                      T * 64, mu + static_cast<size_t>(a.nimag) * T * 64);
+    count_launch();
+  }
+  oz_colscale_kernel<<<dim3((nrows + 7) / 8, 1), 256, 0, s>>>(a.zmel, ngb, 0, ngb, 0, d_cols, nrows, nu);
+  count_launch();
+  QSGW_LAUNCH_CHECK("oz_colscale_kernel");
+  const int pslice = prof_begin("sigc_slice_i8", s);
+  int8_t* A8 = g_a8.as<int8_t>();
+  int8_t* B8 = g_b8.as<int8_t>();
+  const dim3 gk(static_cast<unsigned>((Kp / 2 + 127) / 128));
+  auto slice_w = [&](const double2* w, int n, int slot0) {
+    const dim3 g(gk.x, static_cast<unsigned>(n * T));
+    if (ns == 2) oz_slice_w_kernel<2><<<g, 256, 0, s>>>(A8, w, a.ldw, a.ldw * a.ldw, ngb, T, nslot, slot0, Kp, mu);
+    else if (ns == 3) oz_slice_w_kernel<3><<<g, 256, 0, s>>>(A8, w, a.ldw, a.ldw * a.ldw, ngb, T, nslot, slot0, Kp, mu);
+    else oz_slice_w_kernel<4><<<g, 256, 0, s>>>(A8, w, a.ldw, a.ldw * a.ldw, ngb, T, nslot, slot0, Kp, mu);
+    count_launch();
+  };
+  slice_w(a.wi, a.nimag, 0);
+  if (a.nreal > 0) slice_w(a.wr, a.nreal, a.nimag);
+  {
+    const dim3 g(gk.x, static_cast<unsigned>((nrows + 7) / 8));
+    if (ns == 2) oz_slice_z_kernel<2><<<g, 256, 0, s>>>(B8, a.zmel, ngb, ngb, d_cols, nrows, Kp, nu);
+    else if (ns == 3) oz_slice_z_kernel<3><<<g, 256, 0, s>>>(B8, a.zmel, ngb, ngb, d_cols, nrows, Kp, nu);
+    else oz_slice_z_kernel<4><<<g, 256, 0, s>>>(B8, a.zmel, ngb, ngb, d_cols, nrows, Kp, nu);
+    count_launch();
+  }
+  QSGW_LAUNCH_CHECK("Sigma_c int8 slices");
+  prof_end(pslice, s);
+  // maps: A' [Kp, 64, 2, ns * nslot * T] box {64, 64, 2, 1}; B [Kp, nrows, ns] box {64, 128, 1}
+  CUtensorMap ma, mb;
+  {
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(ns) * nslot * T};
+    const cuuint64_t str[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * 64,
+                               static_cast<cuuint64_t>(Kp) * 128};
+    const cuuint32_t box[4] = {K8, 64, 2, 1};
+    rc = make_tensor_map(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, A8, 4, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc) return rc;
+  }
+  {
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(nrows),
+                                static_cast<cuuint64_t>(ns)};
+    const cuuint64_t str[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * nrows};
+    const cuuint32_t box[3] = {K8, BN, 1};
+    rc = make_tensor_map(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, B8, 3, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc) return rc;
+  }
+  SegParams p{};
+  p.M = ngb;
+  p.ntm = T;
+  p.cps = Kp / K8;
+  p.nslot = nslot;
+  p.T = T;
+  p.nrows = nrows;
+  p.tile_group = d_tg; p.tile_cols = d_cols; p.group_seg_off = d_gso; p.group_nseg = d_gns;
+  p.seg_slot = d_slot; p.segs = d_segs;
+  p.mu_a = mu; p.nu_b = nu;
+  p.post = post_scale(ns);
+  p.C = a.out; p.ldc = ngb;
+  p.err = ctx().d_flags + 1;
+  const dim3 grid(static_cast<unsigned>(T * ntiles));
+  if (ns == 2) return launch_seg<2>(ma, mb, p, grid, s);
+  if (ns == 3) return launch_seg<3>(ma, mb, p, grid, s);
+  return launch_seg<4>(ma, mb, p, grid, s);
+}
+
+int chi0_split_i8(double2* C, long long ldc, long long c_bs, int M, int N, int row_b0, bool herm, const double2* z,
+                  long long ldz, long long ncols, const int* ecol_d, const double* ew_d, const OzChi0Bins& bins,
+                  int classes, int ns, cudaStream_t s, const char* tune_key) {
+  QSGW_ARG(ns >= 2 && ns <= 4, "chi0 split-i8: %d slices (2..4)", ns);
+  const int nbins = static_cast<int>(bins.cnt.size());
+  if (nbins == 0 || M <= 0 || N <= 0 || (classes & 3) == 0) return QSGW_OK;
+  QSGW_ARG(nbins <= 65535, "chi0 split-i8: %d bins exceed the grid limit", nbins);
+  const int Rows = std::max(M, row_b0 + N);
+  // bin layout in Y8: each bin padded to whole 64-byte chunks (32 entries)
+  std::vector<long long> k0(nbins);
+  std::vector<int> nch(nbins);
+  long long tot = 0;
+  int maxch = 0;
+  for (int b = 0; b < nbins; ++b) {
+    k0[b] = tot;
+    nch[b] = (bins.cnt[b] + 31) / 32;
+    tot += nch[b];
+    maxch = std::max(maxch, nch[b]);
+  }
+  const long long Ktot = tot * K8;
+  QSGW_ARG(tot < (1LL << 31), "chi0 split-i8: %lld K chunks exceed the TMA coordinate range", tot);
+  int rc = g_y8.ensure(static_cast<size_t>(ns) * Rows * Ktot);
+  if (rc) return rc;
+  rc = g_ymu.ensure(static_cast<size_t>(nbins) * Rows * sizeof(double));
+  if (rc) return rc;
+  rc = g_zmax.ensure(static_cast<size_t>(Rows) * sizeof(unsigned long long));
+  if (rc) return rc;
+  rc = g_wr.ensure(static_cast<size_t>(2 * nbins) * sizeof(double));
+  if (rc) return rc;
+  const size_t tb = static_cast<size_t>(nbins) * (2 * sizeof(long long) + 2 * sizeof(int));
+  rc = g_bins.ensure(tb + 64);
+  if (rc) return rc;
+  unsigned char* base = g_bins.as<unsigned char>();
+  long long* d_k0 = reinterpret_cast<long long*>(base);
+  long long* d_eb = d_k0 + nbins;
+  int* d_nch = reinterpret_cast<int*>(d_eb + nbins);
+  int* d_cnt = d_nch + nbins;
+  int* d_slab = nullptr;
+  {
+    // the slab table follows in a second small copy (keeps the four arrays 8-byte aligned)
+    static DevBuf g_slab;
+    rc = g_slab.ensure(static_cast<size_t>(nbins) * sizeof(int));
+    if (rc) return rc;
+    d_slab = g_slab.as<int>();
+    if ((rc = h2d(d_slab, bins.slab.data(), nbins * sizeof(int), s))) return rc;
+  }
+  if ((rc = h2d(d_k0, k0.data(), nbins * sizeof(long long), s))) return rc;
+  if ((rc = h2d(d_eb, bins.ebeg.data(), nbins * sizeof(long long), s))) return rc;
+  if ((rc = h2d(d_nch, nch.data(), nbins * sizeof(int), s))) return rc;
+  if ((rc = h2d(d_cnt, bins.cnt.data(), nbins * sizeof(int), s))) return rc;
+  unsigned long long* zmax = g_zmax.as<unsigned long long>();
+  QSGW_CUDA(cudaMemsetAsync(zmax, 0, static_cast<size_t>(Rows) * sizeof(unsigned long long), s));
+  {
+    const int g = static_cast<int>(std::max<long long>(1, std::min<long long>(ncols, 8LL * ctx().sm_count)));
+    oz_rowmax_kernel<<<g, 256, 0, s>>>(z, ldz, Rows, ncols, zmax);
+    count_launch();
+  }
+  QSGW_CUDA(cudaMemsetAsync(g_wr.p, 0, static_cast<size_t>(2 * nbins) * sizeof(double), s));
+  {
+    const int per = std::max(1, std::min(64, static_cast<int>((maxch * 32LL + 4095) / 4096)));
+    oz_wrange_kernel<<<dim3(static_cast<unsigned>(per), static_cast<unsigned>(nbins)), 256, 0, s>>>(
+        ew_d, d_eb, d_cnt, reinterpret_cast<unsigned long long*>(g_wr.p));
+    count_launch();
+  }
+  QSGW_LAUNCH_CHECK("chi0 int8 ranges");
+  int8_t* Y8 = g_y8.as<int8_t>();
+  double* mu = g_ymu.as<double>();
+  CUtensorMap ma, mb;
+  {
+    // [chunk][slice][row][64 B]: rows beyond Rows read as zero, boxes never cross a slice
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(K8), static_cast<cuuint64_t>(Rows),
+                                static_cast<cuuint64_t>(ns), static_cast<cuuint64_t>(tot)};
+    const cuuint64_t str[3] = {static_cast<cuuint64_t>(K8), static_cast<cuuint64_t>(K8) * Rows,
+                               static_cast<cuuint64_t>(K8) * Rows * ns};
+    const cuuint32_t boxa[4] = {K8, 64, 1, 1};
+    const cuuint32_t boxb[4] = {K8, BN, 1, 1};
+    rc = make_tensor_map(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, Y8, 4, dims, str, boxa, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc) return rc;
+    rc = make_tensor_map(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, Y8, 4, dims, str, boxb, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc) return rc;
+  }
+  const int ntm = (M + 63) / 64, ntn = (N + BN - 1) / BN;
+  long long units = 0;
+  for (int nt = 0; nt < ntn; ++nt)
+    for (int mt = 0; mt < ntm; ++mt)
+      if (!herm || mt * 64 + 63 >= nt * BN) ++units;
+  units *= nbins;
+  // split K so that one wave of CTAs covers whole (bin, K part) units: the tiles of a unit share its
+  // rows of Y8 through L2 only while they run together
+  const long long tiles_per_bin = units / nbins;
+  const int maxsplit = std::max(1, std::min(maxch / 4, 64));
+  int heur = static_cast<int>(std::max<long long>(1, (ctx().sm_count + tiles_per_bin / 2) / tiles_per_bin));
+  heur = std::min(heur, maxsplit);
+  // every bin over the same columns in order, weights at ew[b * n + e]: z is sliced in one pass
+  bool dense = ecol_d == nullptr;
+  for (int b = 0; b < nbins && dense; ++b) dense = bins.cnt[b] == bins.cnt[0] && bins.ebeg[b] == static_cast<long long>(b) * bins.cnt[0];
+  HerkParams p{};
+  p.M = M; p.N = N; p.ntm = ntm; p.herm = herm ? 1 : 0; p.row_b0 = row_b0; p.Rows = Rows;
+  p.bin_k0 = d_k0; p.bin_nch = d_nch; p.bin_slab = d_slab; p.wrange = g_wr.as<double>(); p.mu = mu;
+  p.post = post_scale(ns);
+  p.C = C; p.ldc = ldc; p.c_bs = c_bs;
+  p.err = ctx().d_flags + 1;
+  auto run_class = [&](double sign, int splitk) -> int {
+    const int nmu = nbins * Rows;
+    oz_mu_kernel<<<(nmu + 255) / 256, 256, 0, s>>>(zmax, g_wr.as<double>(), Rows, nbins, sign, mu);
+    count_launch();
+    const long long items = static_cast<long long>(maxch) * ((Rows + 63) / 64);   // (32-entry block, 64 rows)
+    const int pslice = prof_begin("chi0_slice_i8", s);
+    if (dense) {
+      const int n = bins.cnt[0];
+      const unsigned gd = static_cast<unsigned>(std::max<long long>(1, std::min<long long>(items, 16LL * ctx().sm_count)));
+      if (ns == 2) oz_slice_y_dense_kernel<2><<<gd, 256, 0, s>>>(Y8, Rows, z, ldz, n, nbins, ew_d, d_k0,
+                                                                 g_wr.as<double>(), mu, sign);
+      else if (ns == 3) oz_slice_y_dense_kernel<3><<<gd, 256, 0, s>>>(Y8, Rows, z, ldz, n, nbins, ew_d, d_k0,
+                                                                      g_wr.as<double>(), mu, sign);
+      else oz_slice_y_dense_kernel<4><<<gd, 256, 0, s>>>(Y8, Rows, z, ldz, n, nbins, ew_d, d_k0,
+                                                         g_wr.as<double>(), mu, sign);
+      count_launch();
+      QSGW_LAUNCH_CHECK("oz_slice_y_dense_kernel");
+      prof_end(pslice, s);
+      HerkParams q = p;
+      q.sign = sign;
+      const dim3 grid(static_cast<unsigned>(ntm * ntn), static_cast<unsigned>(nbins), static_cast<unsigned>(splitk));
+      if (ns == 2) return launch_herk<2>(ma, mb, q, grid, s);
+      if (ns == 3) return launch_herk<3>(ma, mb, q, grid, s);
+      return launch_herk<4>(ma, mb, q, grid, s);
+    }
+    const dim3 gy(static_cast<unsigned>(std::max<long long>(1, std::min<long long>(items, 4LL * ctx().sm_count))),
+                  static_cast<unsigned>(nbins));
+    if (ns == 2) oz_slice_y_kernel<2><<<gy, 256, 0, s>>>(Y8, Rows, z, ldz, ecol_d, ew_d, d_eb, d_cnt, d_k0,
+                                                         g_wr.as<double>(), mu, sign);
+    else if (ns == 3) oz_slice_y_kernel<3><<<gy, 256, 0, s>>>(Y8, Rows, z, ldz, ecol_d, ew_d, d_eb, d_cnt, d_k0,
+                                                              g_wr.as<double>(), mu, sign);
+    else oz_slice_y_kernel<4><<<gy, 256, 0, s>>>(Y8, Rows, z, ldz, ecol_d, ew_d, d_eb, d_cnt, d_k0,
+                                                 g_wr.as<double>(), mu, sign);
+    count_launch();
+    QSGW_LAUNCH_CHECK("oz_slice_y_kernel");
+    prof_end(pslice, s);
+    HerkParams q = p;
+    q.sign = sign;
+    const dim3 grid(static_cast<unsigned>(ntm * ntn), static_cast<unsigned>(nbins), static_cast<unsigned>(splitk));
+    if (ns == 2) return launch_herk<2>(ma, mb, q, grid, s);
+    if (ns == 3) return launch_herk<3>(ma, mb, q, grid, s);
+    return launch_herk<4>(ma, mb, q, grid, s);
+  };
+  auto run = [&](int splitk, bool clear) -> int {
+    if (clear) {
+      for (int b = 0; b < nbins; ++b) {
+        // only the slabs this call writes; the slab tables of the callers are distinct per bin
+        QSGW_CUDA(cudaMemsetAsync(C + static_cast<long long>(bins.slab[b]) * c_bs, 0,
+                                  static_cast<size_t>(ldc) * N * sizeof(double2), s));
+      }
+    }
+    int r = QSGW_OK;
+    if (classes & 1) r = run_class(-1.0, splitk);
+    if (!r && (classes & 2)) r = run_class(1.0, splitk);
+    return r;
+  };
+  std::vector<int> cands;
+  for (int c : {1, 2, 3, 4, 5, 6, 8})
+    if (c <= maxsplit) cands.push_back(c);
+  if (heur > 8) cands.push_back(heur);
+  char key[200];
+  std::snprintf(key, sizeof(key), "%s i8x%d M=%d N=%d bins=%d chunks~2^%.3f", tune_key ? tune_key : "-", ns, M, N, nbins,
+                std::round(8.0 * std::log2(static_cast<double>(std::max(1, maxch)))) / 8.0);
+  if (!tune_key) return run(heur, false);              // accumulating callers: no trials
+  int splitk = heur;
+  bool tried = false;
+  rc = tuned_choice(key, cands, heur, [&](int c) { return run(c, true); }, s, &splitk, &tried);
+  if (rc) return rc;
+  return run(splitk, tried);
+}
+
+}  // namespace qsgw

@@ -17,6 +17,8 @@
 #include <vector>
 #include "zgemm_f64.cuh"
 #include "split_f16.cuh"
+#include "ozaki_i8.cuh"
+#include "autotune.cuh"
 #include "hoststage.cuh"
 
 namespace qsgw {
@@ -211,6 +213,7 @@ static int pole_table_h(const qsgw_sxcf_args& a, std::vector<PoleEntry>& out) {
 
 static DevBuf g_sc_wg, g_sc_w3, g_sc_cz, g_sc_wi, g_sc_wr, g_sc_tabs, g_sc_recs, g_sc_tmp;
 static DevBuf g_sc_host_zs;
+static DevBuf g_sc_trial;                // Sigma_c of the slice-count trials
 // zmel, W(i omega), W(omega) records of the host-pointer calls: twelve slots (about 0.6 GB each
 // at ngb = 600), so the inputs of the next tasks keep the copy engine busy through a long kernel
 static HostRing g_sc_ring(12);
@@ -323,8 +326,10 @@ int sxcf_device(const qsgw_sxcf_args& a) {
   std::vector<int> order(ncol);
   for (long long c = 0; c < ncol; ++c) order[c] = static_cast<int>(c);
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
-  const bool split = ctx().prec_mode == QSGW_PREC_SPLIT_F16;
-  const int tilew = split ? sigc_split_tile_width() : ZG_BN;   // column tile of the split / FP64 kernel
+  const bool split = ctx().prec_mode != QSGW_PREC_FP64;
+  const bool i8 = ctx().prec_mode == QSGW_PREC_SPLIT_I8;
+  // column tile of the int8 / split-FP16 / FP64 kernel
+  const int tilew = i8 ? kOzTileN : (split ? sigc_split_tile_width() : ZG_BN);
   std::vector<ZSeg> segs;
   std::vector<int> gseg_off, gnseg, tile_group, tile_cols, seg_slot;
   int gidx = 0;
@@ -372,7 +377,48 @@ int sxcf_device(const qsgw_sxcf_args& a) {
     sa.group_seg_off = std::move(gseg_off); sa.group_nseg = std::move(gnseg);
     sa.seg_slot = std::move(seg_slot); sa.segs = std::move(segs);
     sa.out = cz;
-    rc = sigc_split_f16(sa, s);
+    if (i8) {
+      int ns = ctx().nslices;
+      if (ns == 0) {
+        // automatic slice count: the smallest whose Sigma_c diagonal (this call's contribution,
+        // the quantity the QP energies take) stays within the target of the 4-slice one
+        const long long kk = static_cast<long long>(ngb) * nm;
+        std::vector<double> ref, cur;
+        auto diag = [&](int n, std::vector<double>& d) -> int {
+          int r = sigc_split_i8(sa, n, s);
+          if (r) return r;
+          r = g_sc_trial.ensure(static_cast<size_t>(a.ntqxx) * a.ntqxx * sizeof(double2));
+          if (r) return r;
+          r = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,
+                        make_double2(0, 0), g_sc_trial.as<double2>(), a.ntqxx, 0, 1, s);
+          if (r) return r;
+          std::vector<double2> h(static_cast<size_t>(a.ntqxx) * a.ntqxx);
+          QSGW_CUDA(cudaMemcpyAsync(h.data(), g_sc_trial.p, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+          QSGW_CUDA(cudaStreamSynchronize(s));
+          d.resize(a.ntqxx);
+          for (int i = 0; i < a.ntqxx; ++i) d[i] = h[static_cast<size_t>(i) * (a.ntqxx + 1)].x;
+          return QSGW_OK;
+        };
+        auto err = [&](int n, double* e) -> int {
+          int r = ref.empty() ? diag(4, ref) : QSGW_OK;
+          if (r) return r;
+          r = diag(n, cur);
+          if (r) return r;
+          *e = 0.0;
+          for (int i = 0; i < a.ntqxx; ++i) *e = std::max(*e, std::fabs(cur[i] - ref[i]));
+          return QSGW_OK;
+        };
+        char key[200];
+        std::snprintf(key, sizeof(key), "sigc_i8 slices ngb=%d nm=%d ntq=%d niw=%d", ngb, nm, a.ntqxx, niw);
+        // the estimate comes from this call; later calls of the shape (other q, other bands) vary
+        // by a few times, so the choice keeps a factor 4 of margin
+        rc = tuned_slices(key, {2, 3}, 4, 0.25 * ctx().sigc_qp_tol, err, 4, &ns);
+        if (rc) return rc;
+      }
+      rc = sigc_split_i8(sa, ns, s);
+    } else {
+      rc = sigc_split_f16(sa, s);
+    }
     if (rc) return rc;
   } else {
     const size_t tb = segs.size() * sizeof(ZSeg) + (gseg_off.size() + gnseg.size() + tile_group.size() +

@@ -155,6 +155,16 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   d |= static_cast<uint64_t>(2) << 61;                 // SWIZZLE_128B
   return d;
 }
+// K-major, 64-byte swizzle: rows of 64 B in 8-row atoms (SBO = 512 B), layout type SWIZZLE_64B
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
+  d |= static_cast<uint64_t>(1) << 16;
+  d |= static_cast<uint64_t>(512 >> 4) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(4) << 61;
+  return d;
+}
 // kind::f16, A = B = F16, D = F32, both K-major, M = 128, N = NC
 constexpr uint32_t IDESC = (1u << 4) | (static_cast<uint32_t>(NC >> 3) << 17) | (static_cast<uint32_t>(BM2 >> 4) << 24);
 
@@ -212,6 +222,24 @@ __device__ __forceinline__ void tmem_ld32w(uint32_t taddr, uint32_t (&r)[32]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// 8-lane TMEM load: 32 lanes x 8 consecutive 32-bit columns
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+// Tiled tensor map over `base` (host side, split_f16.cu): dims / strides in elements / bytes as
+// cuTensorMapEncodeTiled takes them, no interleave, 256-byte L2 promotion, zero fill out of range.
+int make_tensor_map(CUtensorMap* map, CUtensorMapDataType dtype, void* base, int rank, const cuuint64_t* dims,
+                    const cuuint64_t* strides_bytes, const cuuint32_t* box, CUtensorMapSwizzle swz);
 
 // offset of the 16-byte chunk `c` of row `r` inside a 128B-swizzled tile
 __device__ __forceinline__ int sw128_off(int r, int c) { return r * 128 + ((c ^ (r & 7)) << 4); }

@@ -567,8 +567,8 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides_bytes,
-                    const cuuint32_t* box, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B) {
+int make_tensor_map(CUtensorMap* map, CUtensorMapDataType dtype, void* base, int rank, const cuuint64_t* dims,
+                    const cuuint64_t* strides_bytes, const cuuint32_t* box, CUtensorMapSwizzle swz) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled is not available from the driver");
@@ -579,7 +579,7 @@ static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* di
     return QSGW_ERR_ARG;
   }
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, rank, base, dims, strides_bytes, box, es,
+  CUresult r = fn(map, dtype, rank, base, dims, strides_bytes, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -587,6 +587,11 @@ static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* di
     return QSGW_ERR_CUDA;
   }
   return QSGW_OK;
+}
+
+static int make_map(CUtensorMap* map, void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides_bytes,
+                    const cuuint32_t* box, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B) {
+  return make_tensor_map(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, base, rank, dims, strides_bytes, box, swz);
 }
 
 static DevBuf g_a, g_s, g_mx, g_sc, g_tabs, g_w32;

@@ -38,16 +38,6 @@ struct WideCfg {
 // kind::f16, A = B = F16, D = F32, both K-major, M = 128, N = 256
 constexpr uint32_t IDESC_W = (1u << 4) | (static_cast<uint32_t>(NW >> 3) << 17) | (static_cast<uint32_t>(BM2 >> 4) << 24);
 
-// K-major, 64-byte swizzle: rows of 64 B in 8-row atoms (SBO = 512 B), layout type SWIZZLE_64B
-__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
-  d |= static_cast<uint64_t>(1) << 16;
-  d |= static_cast<uint64_t>(512 >> 4) << 32;
-  d |= static_cast<uint64_t>(1) << 46;
-  d |= static_cast<uint64_t>(4) << 61;
-  return d;
-}
 __device__ __forceinline__ void umma_f16_w(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"

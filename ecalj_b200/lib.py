@@ -27,6 +27,7 @@ STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_OOM", -4: "ERR_NOTINI
           -5: "ERR_NUMERIC", -6: "ERR_TIMEOUT", -7: "ERR_UNSUPPORTED"}
 PREC_FP64 = 0
 PREC_SPLIT_F16 = 1
+PREC_SPLIT_I8 = 2
 
 
 class QSGWError(RuntimeError):
@@ -78,6 +79,7 @@ _SIGS = {
     "qsgw_dpsion_matrix": [c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_dbl, c_vp],
     "qsgw_dpsion_chiq_d": [c_vp, c_int, c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp, c_dbl, c_dbl, c_vp, c_vp],
     "qsgw_get_precision": [c_ip, c_ip],
+    "qsgw_set_accuracy": [c_dbl, c_dbl],
     "qsgw_last_error": [ctypes.c_char_p, c_int],
     "qsgw_profile": [c_int],
     "qsgw_profile_get": [ctypes.c_char_p, c_dp, ctypes.POINTER(ctypes.c_longlong)],
@@ -248,6 +250,11 @@ def synchronize():
 
 def set_precision(mode, nslices=2):
     _chk(load().qsgw_set_precision(mode, nslices))
+
+
+def set_accuracy(sigc_qp_tol_ha=1e-3 / 27.211386245988, chi0_rel_tol=2e-5):
+    """Targets of the automatic int8 slice count (set_precision(PREC_SPLIT_I8, 0))."""
+    _chk(load().qsgw_set_accuracy(sigc_qp_tol_ha, chi0_rel_tol))
 
 
 def set_host_async(on):

@@ -360,7 +360,7 @@ def prediction_errors(sur, work, probe, wex, sig, pred, params):
 
 
 def study(N=600, nq_train=48, nq_test=16, nw=48, nb=64, schedule=((1e-3, 2000), (3e-4, 1500), (1e-4, 1000)),
-          tol_mev=1.0, seed=20263, nm=400, ntq=40, precision="split", log=None):
+          tol_mev=1.0, seed=20263, nm=400, ntq=40, precision="split", log=None, nslices=3):
     """Train on exact W_c of nq_train q points, then run the surrogate path on
     nq_test other q points and compare with the plain method (all frequencies
     exact).  Per test q: errors of the linear interpolation the heads start
@@ -371,8 +371,10 @@ def study(N=600, nq_train=48, nq_test=16, nw=48, nb=64, schedule=((1e-3, 2000), 
     log = log or (lambda m: None)
     if t.cuda.current_stream().cuda_stream == 0:
         lib.share_torch_stream()
-    prec = {"split": lib.PREC_SPLIT_F16, "fp64": lib.PREC_FP64}[precision]
-    lib.set_precision(prec)
+    # "split" / "split-f16": FP16 slices; "split-i8": nslices int8 slices (Ozaki); "fp64": plain
+    prec = {"split": (lib.PREC_SPLIT_F16, 2), "split-f16": (lib.PREC_SPLIT_F16, 2),
+            "split-i8": (lib.PREC_SPLIT_I8, nslices), "fp64": (lib.PREC_FP64, 1)}[precision]
+    lib.set_precision(*prec)
     work = Workload(N=N, nw=nw, seed=seed)
     anchors, targets, held = split_grid(nw)
     pred = [i for i in targets if i not in held]
@@ -395,7 +397,7 @@ def study(N=600, nq_train=48, nq_test=16, nw=48, nb=64, schedule=((1e-3, 2000), 
         probe = SigmaProbe(work, iq, ntq=ntq, nm=nm)
         lib.set_precision(lib.PREC_FP64)
         wex64, ms_plain64 = _ms(t, lambda: work.exact(iq, allslots, inp=inp))
-        lib.set_precision(prec)
+        lib.set_precision(*prec)
         wex, ms_plain = _ms(t, lambda: work.exact(iq, allslots, inp=inp))
         sig = probe.sigma(wex, range(nw))
         r = dict(iq=iq, ms_plain=ms_plain, ms_plain_fp64=ms_plain64, sig_mean_abs_ha=float(np.mean(np.abs(sig))))
@@ -407,7 +409,7 @@ def study(N=600, nq_train=48, nq_test=16, nw=48, nb=64, schedule=((1e-3, 2000), 
         r["qp_mev_final"] = qp_mev(probe.delta((wsur - wex)[ps], pred), sig)
         lib.set_precision(lib.PREC_FP64)
         sig64 = probe.sigma(wex64, range(nw))
-        lib.set_precision(prec)
+        lib.set_precision(*prec)
         r["qp_mev_final_vs_fp64"] = qp_mev(probe.sigma(wsur, range(nw)) - sig64, sig64)
         rows.append(r)
         log(f"q {iq}: W rel linear {r['linear']['w_rel']:.2e} lsq {r['lsq']['w_rel']:.2e} trained "

@@ -42,7 +42,8 @@ enum qsgw_status {
 
 enum qsgw_precision {
   QSGW_PREC_FP64 = 0,        /* complex FP64 on the FP64 tensor pipe (DMMA) */
-  QSGW_PREC_SPLIT_F16 = 1    /* split-FP16 slices on tcgen05, FP32 accumulate */
+  QSGW_PREC_SPLIT_F16 = 1,   /* split-FP16 slices on tcgen05, FP32 accumulate */
+  QSGW_PREC_SPLIT_I8 = 2     /* Ozaki int8 slices on tcgen05, exact INT32 accumulate */
 };
 
 /* ---- context (replaces m_gpu.f90:14-68 gpu_init / cuBLAS+cuSOLVER handles,
@@ -62,8 +63,24 @@ int qsgw_synchronize(void);
  * the device between synchronisations (one image per host array). */
 int qsgw_set_host_async(int on);
 /* Runtime precision switch; the reference's is the compile-time -D__MP
- * (m_kind.f90:3-11).  nslices: FP16 slices per operand for SPLIT_F16 (2). */
+ * (m_kind.f90:3-11).  nslices: FP16 slices per operand for SPLIT_F16 (2);
+ * int8 slices per operand for SPLIT_I8 (2, 3 or 4: about 14, 21 or 28 bits
+ * relative to the largest element of a row / column, products accumulated
+ * exactly).  Applies to the chi0 (qsgw_chi0_lorentz*, qsgw_x0gemm*), Sigma_c
+ * (qsgw_sxcf_correlation*) and zmel M->E (qsgw_zmel_m2e_d) contractions. */
 int qsgw_set_precision(int mode, int nslices);
+/* Targets of the automatic slice count (SPLIT_I8 with nslices = 0): on the
+ * first call of each problem shape the contraction runs at 4 slices and at 2
+ * and 3, and keeps the smallest count whose change against 4 slices stays
+ * within the target -- Sigma_c: largest |Re Sigma_c,nn| change of the call's
+ * contribution in Hartree (default 1 meV = 3.675e-5 Ha, the QP-energy gate),
+ * with a factor 4 of margin for the other calls of the shape; chi0: relative
+ * Frobenius norm (default 2e-5) -- else 4.  Choices and estimates are listed by
+ * qsgw_autotune_report.  Calls that accumulate into an output the caller
+ * holds (qsgw_chi0_lorentz_acc_d, qsgw_x0gemm*) take the choice already made
+ * for their shape, else 3 (chi0) / 4 (x0gemm) slices.  No counterpart in the
+ * reference (its precision is fixed at compile time).                     */
+int qsgw_set_accuracy(double sigc_qp_tol_ha, double chi0_rel_tol);
 int qsgw_get_precision(int *mode, int *nslices);
 /* Kernel of the split-precision Sigma_c contraction: 0 = one CTA per
  * 64 x 128 output tile, 1 = CTA pairs over 128-column tiles (tcgen05

@@ -63,10 +63,8 @@ HARTREE_MEV = 27211.386245988
 
 def _split_modes(qsgw):
     """(name, precision mode, slices, gate on the relative Frobenius error) of every split path."""
-    modes = [("split-f16", qsgw.PREC_SPLIT_F16, 2, 5e-5)]
-    if hasattr(qsgw, "PREC_SPLIT_I8"):
-        modes.append(("split-i8x3", qsgw.PREC_SPLIT_I8, 3, 5e-6))
-    return modes
+    return [("split-f16", qsgw.PREC_SPLIT_F16, 2, 5e-5), ("split-i8x3", qsgw.PREC_SPLIT_I8, 3, 3e-5),
+            ("split-i8x4", qsgw.PREC_SPLIT_I8, 4, 3e-7)]
 
 
 def test_chi0_n600_all_pairs_two_frequencies_vs_oracle(qsgw):
