@@ -37,7 +37,8 @@ METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err 
 # DRAM bytes (read + write) of one split-precision Sigma_c task launch
 # (N=600, 40 x 400 states, 25 imaginary slots + real-axis pole columns),
 # measured with ncu on that launch, per kernel of the path.
-SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": None}
+# split-i8: the 4-slice launch, the count the automatic choice makes on this workload.
+SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": 2.066e9}
 
 
 def load_peaks():
@@ -290,6 +291,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="heuristic launch parameters only")
     ap.add_argument("--nq", type=int, default=None, help="Sigma_c tasks (default: the configuration's 64)")
     ap.add_argument("--nk", type=int, default=None, help="k-points of the chi0 part (profiling only)")
+    ap.add_argument("--case", choices=["sigc", "chi0"], default=None,
+                    help="kernel case for ncu: three calls of one contraction of the workload (one Sigma_c "
+                         "task, or chi0 with --nk k points) in the chosen precision, no timing, no JSON line")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     log = (lambda m: print(f"[bench] {m}", file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
@@ -313,6 +317,9 @@ def main():
     modes = {"fp64": (lib.PREC_FP64, 1), "split-f16": (lib.PREC_SPLIT_F16, 2),
              "split-i8": (lib.PREC_SPLIT_I8, args.slices)}
     peaks, peak_src = load_peaks()
+    if args.case:
+        kernel_case(lib, torch, args, modes[prec], log)
+        return
 
     # ---- workload set-up (untimed)
     lib.set_precision(lib.PREC_FP64)
@@ -490,6 +497,35 @@ def main():
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
+
+
+def kernel_case(lib, torch, args, mode, log):
+    """Three calls of one contraction of the workload, for a profiler: the third
+    launch of the contraction's kernel is the one to capture (-s 2 -c 1)."""
+    lib.set_autotune(0, None)
+    if args.case == "chi0":
+        lib.set_precision(lib.PREC_FP64)
+        cfg = chi0_config(args.nk)
+        N, niw = cfg["N"], cfg["niw"]
+        zc = device_normal_c128(N * cfg["npair"], cfg["seed"], 1.0 / math.sqrt(N))
+        chi = torch.zeros(N * N * niw, dtype=torch.complex128, device="cuda")
+        lib.set_precision(*mode)
+        for _ in range(3):
+            lib.chi0_lorentz_d(chi, N, niw, cfg["freq_i"], cfg["nk"], cfg["nocc"], cfg["nun"], cfg["eocc_h"],
+                               cfg["eun_h"], zc)
+        log(f"chi0 case: N={N}, nk={cfg['nk']}, {cfg['npair']} pairs, {niw} iw")
+    else:
+        lib.set_precision(lib.PREC_FP64)
+        c = sigc_config()
+        c["nq"] = 1
+        s = build_sigc_inputs(lib, c, log)
+        for t in s["tasks"]:
+            t["zsec"] = torch.zeros(s["ntq"] * s["ntq"], dtype=torch.complex128, device="cuda")
+        lib.set_precision(*mode)
+        for _ in range(3):
+            run_sigc(lib, s)
+        log("Sigma_c case: one task of the workload")
+    lib.synchronize()
 
 
 def surrogate_summary(lib, log, nq_test=8, precision="split-i8", nslices=3):

@@ -4,7 +4,7 @@
 module m_qsgw_b200
   use, intrinsic :: iso_c_binding
   implicit none
-  integer(c_int), parameter :: QSGW_PREC_FP64 = 0, QSGW_PREC_SPLIT_F16 = 1
+  integer(c_int), parameter :: QSGW_PREC_FP64 = 0, QSGW_PREC_SPLIT_F16 = 1, QSGW_PREC_SPLIT_I8 = 2
   type, bind(C) :: qsgw_sxcf_args
     integer(c_int) :: ngb, nblochpmx, ns1, ns2, ns2r, ntqxx, ntq, niw, nw, nwxi, nwx, nctot, nekc, keepwv
     real(c_double) :: ef, esmr, wkkr, ua
@@ -41,6 +41,10 @@ module m_qsgw_b200
     integer(c_int) function qsgw_set_precision(mode, nslices) bind(C, name='qsgw_set_precision')
       import :: c_int
       integer(c_int), value :: mode, nslices
+    end function
+    integer(c_int) function qsgw_set_accuracy(sigc_qp_tol_ha, chi0_rel_tol) bind(C, name='qsgw_set_accuracy')
+      import :: c_int, c_double
+      real(c_double), value :: sigc_qp_tol_ha, chi0_rel_tol
     end function
     integer(c_int) function qsgw_set_host_async(on) bind(C, name='qsgw_set_host_async')
       import :: c_int
