@@ -568,12 +568,12 @@ __global__ void oz_colscale_kernel(const double2* __restrict__ src, long long ld
   if (lane == 0) out[static_cast<long long>(slot) * ncols_out + j] = pow2_at_least(m);
 }
 
-// Sigma_c A' slices from W: A(m, k) = conj(W_slot[k + m ld]) into
+// Sigma_c A' slices from W (K x M per slot): A(m, k) = conj(W_slot[k + m ld]) into
 // [q][slot_out0 + slot][t][half][64][Kp] int8; each thread four consecutive k of one row.
 // grid (ceil(Kp/2 / 128), nslot * T), block 256: warp w rows w, w + 8, ..
 template <int NS>
 __global__ void oz_slice_w_kernel(int8_t* __restrict__ out, const double2* __restrict__ w, long long ld,
-                                  long long slot_stride, int ngb, int T, int nslot_total, int slot_out0, int Kp,
+                                  long long slot_stride, int M, int K, int T, int nslot_total, int slot_out0, int Kp,
                                   const double* __restrict__ mu) {
   const int st = blockIdx.y;                           // slot * T + t of this launch
   const int t = st % T, slot = st / T;
@@ -588,7 +588,7 @@ __global__ void oz_slice_w_kernel(int8_t* __restrict__ out, const double2* __res
     for (int i = 0; i < 4; ++i) {
       const int k = k0 + i;
       double2 v = make_double2(0.0, 0.0);
-      if (m < ngb && k < ngb) v = w[static_cast<long long>(slot) * slot_stride + k + static_cast<long long>(m) * ld];
+      if (m < M && k < K) v = w[static_cast<long long>(slot) * slot_stride + k + static_cast<long long>(m) * ld];
       slice<NS>(v.x, inv, sr[i]);                      // Re a
       slice<NS>(-v.y, inv, si[i]);                     // Im a  (a = conj(W))
     }
@@ -881,8 +881,12 @@ int rel_diff_fro(const double2* a, const double2* b, long long n, cudaStream_t s
 
 int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
   QSGW_ARG(ns >= 2 && ns <= 4, "sigc split-i8: %d slices (2..4)", ns);
-  const int ngb = a.ngb;
-  const int T = (ngb + 63) / 64;
+  const int ngb = a.ngb;                              // K: rows of W and of the B columns
+  const int M = a.mrows > 0 ? a.mrows : ngb;          // output rows: columns of W
+  const long long ldz = a.ldz > 0 ? a.ldz : ngb;
+  const long long ldc = a.ldc > 0 ? a.ldc : M;
+  const long long wst = a.wstride > 0 ? a.wstride : a.ldw * a.ldw;   // one W record
+  const int T = (M + 63) / 64;
   const int Kp = ((2 * ngb + K8 - 1) / K8) * K8;
   // exact INT32 levels over one segment (K' = Kp): ns * 4096 * Kp < 2^31
   QSGW_ARG(static_cast<long long>(ns) * 4096 * Kp < (1LL << 31), "sigc split-i8: ngb=%d too large", ngb);
@@ -924,15 +928,15 @@ int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
   double* mu = g_mu.as<double>();
   double* nu = g_nu.as<double>();
   // row scales of A' (= column scales of every W record) and column scales of B
-  oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nimag), 256, 0, s>>>(a.wi, a.ldw, a.ldw * a.ldw, ngb, ngb, nullptr,
+  oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nimag), 256, 0, s>>>(a.wi, a.ldw, wst, ngb, M, nullptr,
                                                                     T * 64, mu);
   count_launch();
   if (a.nreal > 0) {
-    oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nreal), 256, 0, s>>>(a.wr, a.ldw, a.ldw * a.ldw, ngb, ngb, nullptr,
+    oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nreal), 256, 0, s>>>(a.wr, a.ldw, wst, ngb, M, nullptr,
                                                                       T * 64, mu + static_cast<size_t>(a.nimag) * T * 64);
     count_launch();
   }
-  oz_colscale_kernel<<<dim3((nrows + 7) / 8, 1), 256, 0, s>>>(a.zmel, ngb, 0, ngb, 0, d_cols, nrows, nu);
+  oz_colscale_kernel<<<dim3((nrows + 7) / 8, 1), 256, 0, s>>>(a.zmel, ldz, 0, ngb, 0, d_cols, nrows, nu);
   count_launch();
   QSGW_LAUNCH_CHECK("oz_colscale_kernel");
   const int pslice = prof_begin("sigc_slice_i8", s);
@@ -941,18 +945,19 @@ int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
   const dim3 gk(static_cast<unsigned>((Kp / 2 + 127) / 128));
   auto slice_w = [&](const double2* w, int n, int slot0) {
     const dim3 g(gk.x, static_cast<unsigned>(n * T));
-    if (ns == 2) oz_slice_w_kernel<2><<<g, 256, 0, s>>>(A8, w, a.ldw, a.ldw * a.ldw, ngb, T, nslot, slot0, Kp, mu);
-    else if (ns == 3) oz_slice_w_kernel<3><<<g, 256, 0, s>>>(A8, w, a.ldw, a.ldw * a.ldw, ngb, T, nslot, slot0, Kp, mu);
-    else oz_slice_w_kernel<4><<<g, 256, 0, s>>>(A8, w, a.ldw, a.ldw * a.ldw, ngb, T, nslot, slot0, Kp, mu);
+    const long long ss = wst;
+    if (ns == 2) oz_slice_w_kernel<2><<<g, 256, 0, s>>>(A8, w, a.ldw, ss, M, ngb, T, nslot, slot0, Kp, mu);
+    else if (ns == 3) oz_slice_w_kernel<3><<<g, 256, 0, s>>>(A8, w, a.ldw, ss, M, ngb, T, nslot, slot0, Kp, mu);
+    else oz_slice_w_kernel<4><<<g, 256, 0, s>>>(A8, w, a.ldw, ss, M, ngb, T, nslot, slot0, Kp, mu);
     count_launch();
   };
   slice_w(a.wi, a.nimag, 0);
   if (a.nreal > 0) slice_w(a.wr, a.nreal, a.nimag);
   {
     const dim3 g(gk.x, static_cast<unsigned>((nrows + 7) / 8));
-    if (ns == 2) oz_slice_z_kernel<2><<<g, 256, 0, s>>>(B8, a.zmel, ngb, ngb, d_cols, nrows, Kp, nu);
-    else if (ns == 3) oz_slice_z_kernel<3><<<g, 256, 0, s>>>(B8, a.zmel, ngb, ngb, d_cols, nrows, Kp, nu);
-    else oz_slice_z_kernel<4><<<g, 256, 0, s>>>(B8, a.zmel, ngb, ngb, d_cols, nrows, Kp, nu);
+    if (ns == 2) oz_slice_z_kernel<2><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, Kp, nu);
+    else if (ns == 3) oz_slice_z_kernel<3><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, Kp, nu);
+    else oz_slice_z_kernel<4><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, Kp, nu);
     count_launch();
   }
   QSGW_LAUNCH_CHECK("Sigma_c int8 slices");
@@ -976,7 +981,7 @@ int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
     if (rc) return rc;
   }
   SegParams p{};
-  p.M = ngb;
+  p.M = M;
   p.ntm = T;
   p.cps = Kp / K8;
   p.nslot = nslot;
@@ -986,12 +991,40 @@ int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
   p.seg_slot = d_slot; p.segs = d_segs;
   p.mu_a = mu; p.nu_b = nu;
   p.post = post_scale(ns);
-  p.C = a.out; p.ldc = ngb;
+  p.C = a.out; p.ldc = ldc;
   p.err = ctx().d_flags + 1;
   const dim3 grid(static_cast<unsigned>(T * ntiles));
   if (ns == 2) return launch_seg<2>(ma, mb, p, grid, s);
   if (ns == 3) return launch_seg<3>(ma, mb, p, grid, s);
   return launch_seg<4>(ma, mb, p, grid, s);
+}
+
+int zgemm_ch_i8(double2* C, long long ldc, int M, int N, int K, const double2* W, long long ldw, const double2* B,
+                long long ldb, int ns, cudaStream_t s) {
+  if (M <= 0 || N <= 0) return QSGW_OK;
+  static DevBuf g_one;
+  int rc = g_one.ensure(sizeof(double));
+  if (rc) return rc;
+  const double one = 1.0;
+  if ((rc = h2d(g_one.p, &one, sizeof(double), s))) return rc;
+  SigcSplitArgs a;
+  a.ngb = K; a.mrows = M; a.ldz = ldb; a.ldc = ldc;
+  a.ldw = ldw;
+  a.wi = W; a.nimag = 1;
+  a.wr = nullptr; a.nreal = 0;
+  a.zmel = B; a.ncol = N;
+  a.wgt = nullptr; a.nwgt = 0; a.w3 = nullptr; a.nw3 = 0;
+  const int ntiles = (N + BN - 1) / BN;
+  for (int t = 0; t < ntiles; ++t) {
+    a.tile_group.push_back(0);
+    for (int j = 0; j < BN; ++j) a.tile_cols.push_back(t * BN + j < N ? t * BN + j : -1);
+  }
+  a.group_seg_off.push_back(0);
+  a.group_nseg.push_back(1);
+  a.seg_slot.push_back(0);
+  a.segs.push_back(ZSeg{W, g_one.as<double>(), 0, 0});        // unit weight for every column
+  a.out = C;
+  return sigc_split_i8(a, ns, s);
 }
 
 int chi0_split_i8(double2* C, long long ldc, long long c_bs, int M, int N, int row_b0, bool herm, const double2* z,

@@ -28,6 +28,11 @@ int chi0_split_i8(double2* C, long long ldc, long long c_bs, int M, int N, int r
                   const double2* z, long long ldz, long long ncols, const int* ecol_d, const double* ew_d,
                   const OzChi0Bins& bins, int classes, int ns, cudaStream_t s, const char* tune_key);
 
+// C = W^H B (C: M x N, ldc; W: K x M, ldw; B: K x N, ldb) on the int8 path with ns slices,
+// C overwritten: the Sigma_c kernel with one segment of unit weight.
+int zgemm_ch_i8(double2* C, long long ldc, int M, int N, int K, const double2* W, long long ldw, const double2* B,
+                long long ldb, int ns, cudaStream_t s);
+
 // ||a - b||_F / ||b||_F of two complex device arrays of n elements (synchronises s)
 int rel_diff_fro(const double2* a, const double2* b, long long n, cudaStream_t s, double* rel);
 

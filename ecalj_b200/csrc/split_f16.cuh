@@ -24,6 +24,11 @@ struct SigcSplitArgs {
   std::vector<int> tile_cols, tile_group, group_seg_off, group_nseg, seg_slot;  // sigc_split_tile_width() columns
   std::vector<ZSeg> segs;
   double2* out;                        // (ngb, ncol), overwritten
+  // int8 path only: a non-square product C = W^H B with W (ngb x mrows), B (ngb x ncol, leading
+  // dimension ldz), C (mrows x ncol, leading dimension ldc); 0 = ngb for each
+  int mrows = 0;
+  long long ldz = 0, ldc = 0;
+  long long wstride = 0;               // elements between W records; 0 = ldw * ldw
 };
 int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s);
 // columns per tile of the selected split Sigma_c kernel (the tables are cut to it)

@@ -11,6 +11,7 @@
 // consecutive threads write consecutive product-basis rows of zmelt.
 #include <vector>
 #include "zgemm_f64.cuh"
+#include "ozaki_i8.cuh"
 
 namespace qsgw {
 
@@ -259,6 +260,12 @@ extern "C" int qsgw_zmel_m2e_d(double* zmel_d, const double* zmelt_d, int ngb, i
   if (is_m_basis) {                                                // copy (m_zmel.f90:549-554)
     QSGW_ARG(nbb == ngb, "zmel_m2e: M basis keeps nbb == ngb");
     QSGW_CUDA(cudaMemcpyAsync(zmel_d, zmelt_d, static_cast<size_t>(ngb) * ncol * 16, cudaMemcpyDeviceToDevice, s));
+  } else if (ctx().prec_mode == QSGW_PREC_SPLIT_I8) {              // the same product on the int8 path
+    QSGW_ARG(ncol < (1LL << 31), "zmel_m2e: %lld columns", ncol);
+    rc = zgemm_ch_i8(reinterpret_cast<double2*>(zmel_d), nbb, nbb, static_cast<int>(ncol), ngb,
+                     reinterpret_cast<const double2*>(m2e_d), ngb, reinterpret_cast<const double2*>(zmelt_d), ngb,
+                     ctx().nslices > 0 ? ctx().nslices : 4, s);
+    if (rc) return rc;
   } else {                                                         // zmel = m2e^H zmelt (:559-560)
     rc = zgemm_f64(2, 0, nbb, static_cast<int>(ncol), ngb, make_double2(1, 0), reinterpret_cast<const double2*>(m2e_d),
                    ngb, 0, reinterpret_cast<const double2*>(zmelt_d), ngb, 0, make_double2(0, 0),

@@ -193,3 +193,28 @@ def test_automatic_slice_count_meets_the_targets(i8):
     print(f"automatic chi0 slices: {rep[key]}, report {rep}")
     ref = _chi0_oracle(p)
     assert rel_fro(i8.from_device(chi, (N, N, niw)), ref) < 4e-5
+
+
+@pytest.mark.parametrize("ns", [3, 4])
+@pytest.mark.parametrize("conj", [0, 1])
+def test_zmel_m2e_i8_matches_emulation(i8, ns, conj):
+    """zmel = m2e^H zmelt (m_zmel.f90:559-560), then conj (:590-594), on the
+    int8 path: a non-square product (nbb = 130 E-basis rows from ngb = 150)."""
+    rng = np.random.default_rng(40 + ns)
+    ngb, nbb, nmtot, nqtot = 150, 130, 7, 23
+    m2e = _rc(rng, ngb, nbb)
+    zmelt = _rc(rng, ngb, nmtot, nqtot)
+    ref = (m2e.conj().T @ zmelt.reshape(ngb, -1, order='F')).reshape(nbb, nmtot, nqtot, order='F')
+    emu = ozaki_emul.complex_product(m2e.conj().T, zmelt.reshape(ngb, -1, order='F'), ns)
+    emu = emu.reshape(nbb, nmtot, nqtot, order='F')
+    if conj:
+        ref, emu = ref.conj(), emu.conj()
+    i8.set_precision(i8.PREC_SPLIT_I8, ns)
+    out = i8.to_device(np.zeros((nbb, nmtot, nqtot), complex, order='F'))
+    i8.zmel_m2e_d(out, i8.to_device(zmelt), ngb, nbb, nmtot, nqtot, i8.to_device(m2e), 0, conj)
+    i8.synchronize()
+    got = i8.from_device(out, (nbb, nmtot, nqtot))
+    e_emu, e_ref = rel_fro(got, emu), rel_fro(got, ref)
+    print(f"zmel m2e i8x{ns} conj={conj}: vs emulation {e_emu:.2e}, vs FP64 {e_ref:.2e}")
+    assert e_emu < EXACT
+    assert e_ref < GATE[ns]

@@ -23,6 +23,18 @@ def test_tetra_chain_vs_oracle(qsgw):
     _chain(qsgw, degenerate=False)
 
 
+@pytest.mark.parametrize("ns,tol", [(3, 3e-5), (4, 3e-7)])
+def test_tetra_chain_int8(qsgw, ns, tol):
+    """The same chain with x0gemm on the int8 Ozaki path (the reference's own
+    chi0 boundary: the pair/bin lists of the tetrahedron weights, accumulated
+    per k into rcxq), against the oracle chain with the same weights."""
+    try:
+        qsgw.set_precision(qsgw.PREC_SPLIT_I8, ns)
+        _chain(qsgw, degenerate=False, tol=tol)
+    finally:
+        qsgw.set_precision(qsgw.PREC_FP64, 1)
+
+
 def test_tetra_chain_degenerate_bands(qsgw):
     """Bands that touch at some k: the host copy of the GPU weights is
     symmetrised (qsgw_tetwt_symmetrize) before the lists are built, as
@@ -30,7 +42,8 @@ def test_tetra_chain_degenerate_bands(qsgw):
     _chain(qsgw, degenerate=True)
 
 
-def _chain(qsgw, degenerate):
+def _chain(qsgw, degenerate, tol=None):
+    """tol: the gate of a split-precision x0gemm (None: the FP64 gates)."""
     import torch
     idt, qbzw, ek, ekq = synth.tetra_mesh(3)
     if degenerate:
@@ -79,6 +92,9 @@ def _chain(qsgw, degenerate):
 
     ri, rr = oracle_chain(w)                                     # the GPU's weights
     print(f"tetra chain, same weights: imag {rel_fro(gi, ri):.2e} real {rel_fro(gr, rr):.2e}")
+    if tol is not None:
+        assert rel_fro(gi, ri) < tol and rel_fro(gr, rr) < tol
+        return
     assert rel_fro(gi, ri) < 1e-11
     assert rel_fro(gr, rr) < 1e-11
     wref, _ = tw.tetwt_hist(idt, qbzw, ek, ekq, ef, frhis, nocc, nunocc)
