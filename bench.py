@@ -287,6 +287,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the W_c frequency-interpolator study")
+    ap.add_argument("--no-c4", action="store_true", help="skip the N=1500 all-in study (configuration c4)")
+    ap.add_argument("--c4-k", type=int, default=16, help="k points of the 512 timed in the c4 study")
     ap.add_argument("--no-graph", action="store_true", help="time eager calls instead of CUDA-graph replays")
     ap.add_argument("--no-autotune", action="store_true", help="heuristic launch parameters only")
     ap.add_argument("--nq", type=int, default=None, help="Sigma_c tasks (default: the configuration's 64)")
@@ -469,6 +471,11 @@ def main():
         lib.set_autotune(0, None)          # no tuning trials inside the study's timed calls
         sur = surrogate_summary(lib, log, precision=prec if split else "fp64", nslices=args.slices)
         lib.set_precision(*modes[prec])
+    c4 = None
+    if split and not args.no_c4:
+        lib.set_autotune(0, None)
+        c4 = c4_study(lib, torch, log, modes, prec, args.c4_k)
+        lib.set_precision(*modes[prec])
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline()
@@ -490,6 +497,7 @@ def main():
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks, "kernel_ms": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]},
                 "fp64_peak_tflops": round(fp64_peak, 3), "int8_peak": i8_peak, "compare": compare, "surrogate": sur,
+                "c4": c4,
                 "autotune": lib.autotune_report()}
         if compare and cpu and cpu.get("value"):
             # both FP64: this library's plain GPU path over the CPU restatement (same flop count)
@@ -526,6 +534,118 @@ def kernel_case(lib, torch, args, mode, log):
             run_sigc(lib, s)
         log("Sigma_c case: one task of the workload")
     lib.synchronize()
+
+
+def c4_study(lib, torch, log, modes, prec, nk_timed=16):
+    """Configuration c4, all in, at N = 1500 (nk = 512, nocc = 40, nunocc U{300..1200}, 32 iw):
+    chi0 streamed k by k through qsgw_chi0_lorentz_acc_d (zmel of each k generated on the device,
+    720 MB per k) on the first nk_timed of the 512 k with the weights of the whole mesh, the time
+    extrapolated linearly in k; W = (1 - v chi0)^-1 v on all 33 slots (iw = 0 and the 32 points);
+    one Sigma_c task of 400 x 40 states on that W.  The split path (its chi0 -> W -> Sigma_c chain)
+    against the FP64 path (its own chain): times, speed-up and the QP error of the whole chain.
+    The oracle checks chi0 of k = 0 on 2 seeded frequencies."""
+    from ecalj_b200 import synth, sched
+    from oracle import x0
+    c = synth.CONFIGS["chi0_n1500_streamed"]
+    N, nk, niw = c["N"], c["nk"], c["niw"]
+    rng = np.random.default_rng(c["seed"])
+    nocc, nun, eocc, eun = synth.chi0_spectrum(rng, nk, c["nocc"], c["nun"])
+    mesh = synth.imag_mesh(niw)
+    freqs = np.concatenate([[0.0], mesh["freq_i"]])
+    nf = niw + 1
+    ks = list(range(nk_timed))
+    npair_k = [int(nocc[k] * nun[k]) for k in ks]
+    p_timed, p_all = sum(npair_k), int(np.sum(nocc * nun))
+    zs = [device_normal_c128(N * npair_k[k], c["seed"] * 7919 + k, 1.0 / math.sqrt(N)) for k in ks]
+    vsq, q = synth.coulomb(N, c["seed"] + 1)
+    m2e = lib.to_device(q)
+    trng = np.random.default_rng(c["seed"] + 3)
+    ntq, nm = 40, 400
+    omega = np.sort(trng.uniform(-1.0, 1.0, ntq))
+    ekc = np.sort(trng.uniform(-1.0, 4.0, nm))
+    zmel = device_normal_c128(N * nm * ntq, c["seed"] * 31 + 1, 1.0 / math.sqrt(N))
+    fr = synth.freq_r_mesh(50)
+    ef, esmr, wkkr = 0.0, 0.01, 1.0 / 64
+    nwxi, nwx, ntmax = sched.get_nwx(omega, ekc, fr, ef, esmr)
+    ns2r = min(nm, ntmax)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    out = {}
+    for name in (prec, "fp64"):
+        lib.set_precision(*modes[name])
+        chi = torch.zeros(N * N * nf, dtype=torch.complex128, device="cuda")
+        # untimed first call: scratch allocation (the accumulating calls run no trials)
+        lib.chi0_lorentz_acc_d(chi, N, nf, freqs, nk, nocc[:1], nun[:1], eocc[0] * 0.5, eun[0] * 0.5, zs[0])
+        chi.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        for k in ks:
+            lib.chi0_lorentz_acc_d(chi, N, nf, freqs, nk, nocc[k:k + 1], nun[k:k + 1], eocc[k] * 0.5, eun[k] * 0.5,
+                                   zs[k])
+        e1.record()
+        torch.cuda.synchronize()
+        t_chi = e0.elapsed_time(e1)
+        wi = torch.zeros(N * N * nf, dtype=torch.complex128, device="cuda")
+        e0, e1 = ev(), ev()
+        e0.record()
+        lib.wvi_llw(chi, 2, vsq, m2e, True, True, 2, zw=wi, device=True, ngb=N, niw=nf)
+        e1.record()
+        torch.cuda.synchronize()
+        t_w = e0.elapsed_time(e1)
+        g = torch.tensor(1.0 / (1.0 + (fr / 0.5) ** 2), dtype=torch.float64, device="cuda")
+        wr = (wi[:N * N].view(1, N * N) * g.view(-1, 1)).reshape(-1).contiguous()
+        zsec = torch.zeros(ntq * ntq, dtype=torch.complex128, device="cuda")
+        sargs = (1, nm, ns2r, nwxi, nwx, ntq, wi, wr, omega, ekc, 0, ef, esmr, wkkr, mesh["ua"], mesh["x"],
+                 mesh["wx"], mesh["expa"], fr)
+        lib.sxcf_correlation(zsec, zmel, *sargs, device=True, ngb=N, ntq=ntq)   # untimed: slice trials, scratch
+        zsec.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record()
+        lib.sxcf_correlation(zsec, zmel, *sargs, device=True, ngb=N, ntq=ntq)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = dict(chi=chi, wi=wi, zsec=zsec.view(ntq, ntq), t_chi=t_chi, t_w=t_w,
+                         t_sig=e0.elapsed_time(e1))
+        del wr
+        log(f"c4 {name}: chi0 {t_chi:.1f} ms on {nk_timed} k, W {t_w:.1f} ms, Sigma_c {out[name]['t_sig']:.1f} ms")
+    a, b = out[prec], out["fp64"]
+    rel = lambda x, y: float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
+    qp = float(torch.max(torch.abs(torch.real(a["zsec"].diagonal() - b["zsec"].diagonal())))) * 27211.386245988
+    fl_chi = 8.0 * N * N * p_timed * nf
+    scale = p_all / p_timed
+    tot = {n: out[n]["t_chi"] * scale + out[n]["t_w"] + out[n]["t_sig"] for n in out}
+    # the oracle on a seeded subset: chi0 of k = 0 on 2 of the frequencies
+    sel = np.sort(np.random.default_rng(c["seed"] + 9).choice(nf, 2, replace=False))
+    z0 = zs[0].cpu().numpy().reshape(N, int(nocc[0]), int(nun[0]), order="F")
+    ref = x0.chi0_direct([z0], x0.lorentz_pair_tables([eocc[0] * 0.5], [eun[0] * 0.5], 2, freqs[sel], nk), N, 2)[:, :, 1:]
+    oracle_err = {}
+    for name in (prec, "fp64"):
+        lib.set_precision(*modes[name])
+        ch = torch.zeros(N * N * 2, dtype=torch.complex128, device="cuda")
+        lib.chi0_lorentz_acc_d(ch, N, 2, freqs[sel], nk, nocc[:1], nun[:1], eocc[0] * 0.5, eun[0] * 0.5, zs[0])
+        lib.synchronize()
+        got = ch.cpu().numpy().reshape(N, N, 2, order="F")
+        oracle_err[name] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    res = {"workload": f"N=1500, nk=512 (chi0 timed on {nk_timed} k streamed, {p_timed} of {p_all} pairs, "
+                       "extrapolated linearly), nocc=40, nunocc U{300..1200}, 32 iw + w=0; W on 33 slots; "
+                       "one Sigma_c task of 400 x 40 states, 50-point real mesh",
+           "precision": prec,
+           "chi0_ms_timed": {n: round(out[n]["t_chi"], 2) for n in out},
+           "chi0_gflops_timed": {n: round(fl_chi / (out[n]["t_chi"] * 1e-3) / 1e9, 1) for n in out},
+           "chi0_s_per_q_extrapolated": {n: round(out[n]["t_chi"] * scale * 1e-3, 3) for n in out},
+           "w_ms": {n: round(out[n]["t_w"], 2) for n in out},
+           "sigc_ms": {n: round(out[n]["t_sig"], 2) for n in out},
+           "total_s_per_q_extrapolated": {n: round(tot[n] * 1e-3, 3) for n in out},
+           "speedup_vs_fp64": round(tot["fp64"] / tot[prec], 3),
+           "chi0_rel_err_vs_fp64": rel(a["chi"], b["chi"]), "w_rel_err_vs_fp64": rel(a["wi"], b["wi"]),
+           "sigc_rel_err_vs_fp64_chain": rel(a["zsec"], b["zsec"]),
+           "qp_err_mev_max_chain": qp, "qp_gate_1mev_met": qp <= 1.0,
+           "oracle_chi0_k0_2iw_rel_err": oracle_err, "oracle_frequencies": [int(i) for i in sel],
+           "slices": chosen_slices(lib, modes[prec][1]) if prec == "split-i8" else None}
+    del out, zs
+    torch.cuda.empty_cache()
+    return res
 
 
 def surrogate_summary(lib, log, nq_test=8, precision="split-i8", nslices=3):
