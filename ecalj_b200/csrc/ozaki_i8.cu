@@ -86,6 +86,49 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t d
       " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n"
       ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC_I8), "r"(accumulate));
 }
+// The same MMA with the A operand kept in the tensor core's collector buffer: FILL loads it and
+// keeps it, USE reads the kept copy (same A descriptor), LAST reads it and releases the buffer.
+enum { A_FILL = 0, A_USE = 1, A_LAST = 2 };
+template <int MODE>
+__device__ __forceinline__ void umma_i8_ca(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  if (MODE == A_FILL)
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8.collector::a::fill [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC_I8), "r"(accumulate));
+  else if (MODE == A_USE)
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8.collector::a::use [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC_I8), "r"(accumulate));
+  else
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8.collector::a::lastuse [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC_I8), "r"(accumulate));
+}
+
+// The slice products of one K step: for each A slice pa (one shared-memory read through the
+// collector buffer), the B slices qb with pa + qb < NS into the accumulator of level pa + qb.
+// The first product into each level (pa == 0) starts it when `start` is set.
+template <int NS>
+__device__ __forceinline__ void slice_products(uint32_t tmem, uint64_t da0, uint64_t db0, uint32_t a_step,
+                                               uint32_t b_step, bool start) {
+#pragma unroll
+  for (int pa = 0; pa < NS; ++pa) {
+    const uint64_t da = da0 + pa * a_step;
+#pragma unroll
+    for (int qb = 0; qb < NS - pa; ++qb) {
+      const uint64_t db = db0 + qb * b_step;
+      const uint32_t d = tmem + static_cast<uint32_t>((pa + qb) * kOzTileN);
+      const uint32_t acc = (start && pa == 0) ? 0u : 1u;
+      if (NS - pa == 1) umma_i8(d, da, db, acc);
+      else if (qb == 0) umma_i8_ca<A_FILL>(d, da, db, acc);
+      else if (qb == NS - pa - 1) umma_i8_ca<A_LAST>(d, da, db, acc);
+      else umma_i8_ca<A_USE>(d, da, db, acc);
+    }
+  }
+}
 
 // 32 lanes x 4 consecutive 32-bit TMEM columns
 __device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
@@ -244,18 +287,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (!mbar_wait(&full[st], ph, abort_flag)) break;
         tc_fence_after();
 #pragma unroll
-        for (int kk = 0; kk < K8 / 32; ++kk) {       // 32 int8 = 32 B along K = 2 descriptor units
-#pragma unroll
-          for (int lv = 0; lv < NS; ++lv) {
-#pragma unroll
-            for (int pa = 0; pa <= lv; ++pa) {
-              const int qb = lv - pa;
-              const uint64_t da = dA0 + static_cast<uint32_t>(((st * NS + pa) * SLA8) >> 4) + 2 * kk;
-              const uint64_t db = dB0 + static_cast<uint32_t>(((st * NS + qb) * SLB8) >> 4) + 2 * kk;
-              umma_i8(tmem + static_cast<uint32_t>(lv * BN), da, db, (first && kk == 0 && pa == 0) ? 0u : 1u);
-            }
-          }
-        }
+        for (int kk = 0; kk < K8 / 32; ++kk)          // 32 int8 = 32 B along K = 2 descriptor units
+          slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((st * NS * SLA8) >> 4) + 2 * kk,
+                             dB0 + static_cast<uint32_t>((st * NS * SLB8) >> 4) + 2 * kk, SLA8 >> 4, SLB8 >> 4,
+                             first && kk == 0);
         umma_commit(&empty[st]);
         if (last) umma_commit(accfull);
         if (++st == NST) { st = 0; ph ^= 1; }
@@ -435,18 +470,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (!mbar_wait(&cfull[st], ph, abort_flag)) break;
       tc_fence_after();
 #pragma unroll
-      for (int kk = 0; kk < K8 / 32; ++kk) {
-#pragma unroll
-        for (int lv = 0; lv < NS; ++lv) {
-#pragma unroll
-          for (int pa = 0; pa <= lv; ++pa) {
-            const int qb = lv - pa;
-            const uint64_t da = dA0 + static_cast<uint32_t>(((st * NS + pa) * SLA8) >> 4) + 2 * kk;
-            const uint64_t db = dB0 + static_cast<uint32_t>(((st * NS + qb) * SLB8) >> 4) + 2 * kk;
-            umma_i8(tmem + static_cast<uint32_t>(lv * BN), da, db, (first && kk == 0 && pa == 0) ? 0u : 1u);
-          }
-        }
-      }
+      for (int kk = 0; kk < K8 / 32; ++kk)
+        slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((st * NS * SLA8) >> 4) + 2 * kk,
+                           dB0 + static_cast<uint32_t>((st * NS * SLB8) >> 4) + 2 * kk, SLA8 >> 4, SLB8 >> 4,
+                           first && kk == 0);
       umma_commit(&empty[st]);
       if (last) umma_commit(accfull);
       if (++st == NST) { st = 0; ph ^= 1; }
