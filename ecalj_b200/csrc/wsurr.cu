@@ -42,10 +42,15 @@ struct State {
   double* lsq = nullptr;       // normal equations of the heads: G[NTMAX][NIN*NIN], then H[NTMAX][NIN]
   int step = 0;
   int cap = 0;                 // batch capacity of the buffers below
-  float* h1 = nullptr;         // activations (batch x NH)
+  __nv_bfloat16* w2t = nullptr;  // W2 transposed [n][k] (BF16), the forward GEMM's B operand
+  __nv_bfloat16* h1 = nullptr;   // layer-1 activations (batch x NH, BF16: the layer-2 GEMM's operand)
+  __nv_bfloat16* h1t = nullptr;  // the same transposed (NH x cap), the weight-gradient GEMM's operand
   float* h2 = nullptr;
   float* g1 = nullptr;         // dL/dpre1
-  float* g2 = nullptr;         // dL/dpre2
+  float* g2 = nullptr;         // dL/dpre2 (FP32, for db2)
+  __nv_bfloat16* g2b = nullptr;  // dL/dpre2 in BF16 (batch x NH) and transposed (NH x cap)
+  __nv_bfloat16* g2t = nullptr;
+  float* head = nullptr;       // linear-head term of every row
   float* out = nullptr;
   float* xb = nullptr;         // gathered mini-batch
   float* yb = nullptr;
@@ -79,18 +84,17 @@ __global__ void to_bf16_kernel(const float* __restrict__ p, __nv_bfloat16* __res
   if (i < NPARAM) w[i] = __float2bfloat16_rn(p[i]);
 }
 
-// Forward pass: one block = 32 samples, thread = hidden unit.  h1/h2 keep the
-// activations for the backward pass (null for inference).  With wt and sumw
-// (training) the sum of the sample weights is added to *sumw.
-__global__ void __launch_bounds__(256) forward_kernel(const float* __restrict__ x, const int* __restrict__ tix,
-                                                      int batch, const __nv_bfloat16* __restrict__ w,
-                                                      const float* __restrict__ master, float* __restrict__ h1,
-                                                      float* __restrict__ h2, float* __restrict__ out,
-                                                      const float* __restrict__ wt, float* __restrict__ sumw) {
+// Forward pass, layer 1 and the linear head: one block = 32 samples, thread = hidden unit.
+// h1 = relu(x W1 + b1) in BF16 (row-major, and transposed into h1t when training, rows
+// beyond the batch up to the 32-row block zero); head[r] = C[t_r] . x_r (FP32 master
+// parameters).  With wt and sumw (training) the sum of the sample weights is added to *sumw.
+__global__ void __launch_bounds__(256) forward_l1_kernel(const float* __restrict__ x, const int* __restrict__ tix,
+                                                         int batch, const __nv_bfloat16* __restrict__ w,
+                                                         const float* __restrict__ master,
+                                                         __nv_bfloat16* __restrict__ h1, __nv_bfloat16* __restrict__ h1t,
+                                                         long long ldt, float* __restrict__ head,
+                                                         const float* __restrict__ wt, float* __restrict__ sumw) {
   __shared__ float sx[32][NIN];
-  __shared__ float s1[32][NH + 1];
-  __shared__ float shead[32];
-  __shared__ float smask[32];
   const int s0 = blockIdx.x * 32;
   const int tid = threadIdx.x;
   for (int e = tid; e < 32 * NIN; e += blockDim.x) {
@@ -98,58 +102,156 @@ __global__ void __launch_bounds__(256) forward_kernel(const float* __restrict__ 
     sx[r][c] = (s0 + r < batch) ? x[static_cast<long long>(s0 + r) * NIN + c] : 0.f;
   }
   __syncthreads();
-  if (tid < 32) {
-    // linear head C[t] . x (FP32 master parameters)
+  if (tid < 32 && s0 + tid < batch) {
     float a = 0.f;
-    const int t = (s0 + tid < batch) ? tix[s0 + tid] : -1;
+    const int t = tix[s0 + tid];
     if (t >= 0 && t < NTMAX) {                         // rows with a bad head index get no head term
       const float* c = master + OFF_C + t * NIN;
 #pragma unroll
       for (int i = 0; i < NIN; ++i) a += c[i] * sx[tid][i];
     }
-    smask[tid] = (t < NMLP) ? 1.f : 0.f;               // linear-only rows take no MLP term
-    if (wt && sumw && s0 + tid < batch) atomicAdd(sumw, wt[s0 + tid]);
-    shead[tid] = a;
+    head[s0 + tid] = a;
+    if (wt && sumw) atomicAdd(sumw, wt[s0 + tid]);
   }
   float wcol[NIN];
 #pragma unroll
   for (int i = 0; i < NIN; ++i) wcol[i] = bf(w[OFF_W1 + i * NH + tid]);
   const float b1 = bf(w[OFF_B1 + tid]);
   for (int r = 0; r < 32; ++r) {
+    const bool in = s0 + r < batch;
     float a = b1;
 #pragma unroll
     for (int i = 0; i < NIN; ++i) a += sx[r][i] * wcol[i];
-    a = fmaxf(a, 0.f);
-    s1[r][tid] = a;
-    if (h1 && s0 + r < batch) h1[static_cast<long long>(s0 + r) * NH + tid] = a;
+    const __nv_bfloat16 v = __float2bfloat16_rn(in ? fmaxf(a, 0.f) : 0.f);
+    if (in) h1[static_cast<long long>(s0 + r) * NH + tid] = v;
+    if (h1t) h1t[static_cast<long long>(tid) * ldt + s0 + r] = v;
   }
-  __syncthreads();
-  float acc[32];
-  const float b2 = bf(w[OFF_B2 + tid]);
+}
+
+// Forward pass, layer 3: out_r = m_r (h2_r . W3 + b3) + head_r, m_r = 0 on linear-only rows.
+// One warp per row.
+__global__ void forward_l3_kernel(const float* __restrict__ h2, const int* __restrict__ tix, int batch,
+                                  const __nv_bfloat16* __restrict__ w, const float* __restrict__ head,
+                                  float* __restrict__ out) {
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= batch) return;
+  float a = 0.f;
+  for (int k = lane; k < NH; k += 32) a += h2[static_cast<long long>(r) * NH + k] * bf(w[OFF_W3 + k]);
+  for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if (lane == 0) out[r] = (tix[r] < NMLP ? a + bf(w[OFF_B3]) : 0.f) + head[r];
+}
+
+// C[m][n] = sum_k A[m][k] Bt[n][k] on the tensor cores (mma.sync m16n8k16, BF16 operands, FP32
+// accumulation): A (M x K) and Bt (N x K) row-major BF16, K a multiple of 32 within each split,
+// N a multiple of 128.  Block tile 64 x 128 (8 warps of 32 x 32), K steps of 32 through shared
+// memory (80-byte rows: conflict-free ldmatrix).  Epilogues: layer 2 forward (bias, ReLU, FP32
+// h2), layer 2 backward (the unit's ReLU mask from h1, FP32 g1), weight gradient (FP32 atomics,
+// one K split per blockIdx.z).
+enum { EPI_FWD = 0, EPI_BWD = 1, EPI_WGRAD = 2 };
+struct MmaArgs {
+  const __nv_bfloat16* A;
+  long long lda;
+  const __nv_bfloat16* Bt;
+  long long ldb;
+  int M, N, K, ksplit;
+  float* C;
+  long long ldc;
+  const __nv_bfloat16* bias;   // EPI_FWD: b2
+  const __nv_bfloat16* mask;   // EPI_BWD: h1 (ld = ldc)
+};
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))));
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(256) mma_gemm_kernel(const MmaArgs p) {
+  __shared__ __align__(16) __nv_bfloat16 sa[64][40];
+  __shared__ __align__(16) __nv_bfloat16 sb[128][40];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 128;
+  const int kb = blockIdx.z * p.ksplit, ke = min(p.K, kb + p.ksplit);
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  float acc[2][4][4];
 #pragma unroll
-  for (int r = 0; r < 32; ++r) acc[r] = b2;
-  for (int k = 0; k < NH; ++k) {
-    const float wk = bf(w[OFF_W2 + k * NH + tid]);
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int r = 0; r < 32; ++r) acc[r] += s1[r][k] * wk;
-  }
-  __syncthreads();
-  const float w3 = bf(w[OFF_W3 + tid]);
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
-  for (int r = 0; r < 32; ++r) {
-    const float a = fmaxf(acc[r], 0.f);
-    if (h2 && s0 + r < batch) h2[static_cast<long long>(s0 + r) * NH + tid] = a;
-    s1[r][tid] = a * w3;
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+  for (int k0 = kb; k0 < ke; k0 += 32) {
+    {
+      const int r = tid >> 2, c = (tid & 3) * 8;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (m0 + r < p.M) v = *reinterpret_cast<const uint4*>(p.A + static_cast<long long>(m0 + r) * p.lda + k0 + c);
+      *reinterpret_cast<uint4*>(&sa[r][c]) = v;
+    }
+#pragma unroll
+    for (int i = tid; i < 512; i += 256) {
+      const int r = i >> 2, c = (i & 3) * 8;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (n0 + r < p.N) v = *reinterpret_cast<const uint4*>(p.Bt + static_cast<long long>(n0 + r) * p.ldb + k0 + c);
+      *reinterpret_cast<uint4*>(&sb[r][c]) = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 32; kk += 16) {
+      uint32_t af[2][4], bq[2][4];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) ldsm_x4(af[mi], &sa[wm + mi * 16 + (lane & 15)][kk + (lane >> 4) * 8]);
+#pragma unroll
+      for (int nj = 0; nj < 2; ++nj)   // n8 tiles 2 nj and 2 nj + 1: {b0, b1} of each
+        ldsm_x4(bq[nj], &sb[wn + nj * 16 + ((lane >> 4) & 1) * 8 + (lane & 7)][kk + ((lane >> 3) & 1) * 8]);
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], af[mi], bq[ni >> 1][(ni & 1) * 2], bq[ni >> 1][(ni & 1) * 2 + 1]);
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  // out = sum_k h2 w3 + b3 + head (warp v reduces rows v, v+8, ...)
-  const int warp = tid >> 5, lane = tid & 31;
-  for (int r = warp; r < 32; r += 8) {
-    float a = 0.f;
-    for (int k = lane; k < NH; k += 32) a += s1[r][k];
-    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0 && s0 + r < batch) out[s0 + r] = smask[r] * (a + bf(w[OFF_B3])) + shead[r];
-  }
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int m = m0 + wm + mi * 16 + (lane >> 2) + (e >> 1) * 8;
+        const int n = n0 + wn + ni * 8 + (lane & 3) * 2 + (e & 1);
+        if (m >= p.M || n >= p.N) continue;
+        const float v = acc[mi][ni][e];
+        const long long o = static_cast<long long>(m) * p.ldc + n;
+        if (EPI == EPI_FWD) p.C[o] = fmaxf(v + bf(p.bias[n]), 0.f);
+        else if (EPI == EPI_BWD) p.C[o] = (bf(p.mask[o]) > 0.f) ? v : 0.f;
+        else atomicAdd(&p.C[o], v);
+      }
+}
+
+// w2t[n][k] = W2[k][n] (BF16), the forward GEMM's B operand
+__global__ void w2t_kernel(const __nv_bfloat16* __restrict__ w, __nv_bfloat16* __restrict__ w2t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NH * NH) return;
+  const int n = i / NH, k = i % NH;
+  w2t[i] = w[OFF_W2 + k * NH + n];
+}
+
+// db[j] += sum_r G[r][j] (FP32), rows split over blockIdx.y
+__global__ void colsum_kernel(const float* __restrict__ G, int batch, int rows_per_block, float* __restrict__ db) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= NH) return;
+  const int r0 = blockIdx.y * rows_per_block, r1 = min(batch, r0 + rows_per_block);
+  float a = 0.f;
+  for (int r = r0; r < r1; ++r) a += G[static_cast<long long>(r) * NH + j];
+  atomicAdd(&db[j], a);
 }
 
 // Backward of L = sum_r w_r (out_r - y_r)^2 / sum_r w_r (w_r = 1 without weights),
@@ -158,13 +260,13 @@ __global__ void __launch_bounds__(256) forward_kernel(const float* __restrict__ 
 __global__ void __launch_bounds__(256) backward_act_kernel(const float* __restrict__ x, const int* __restrict__ tix,
                                                            const float* __restrict__ y, const float* __restrict__ wt,
                                                            int batch, const __nv_bfloat16* __restrict__ w,
-                                                           const float* __restrict__ h1, const float* __restrict__ h2,
-                                                           const float* __restrict__ out, float* __restrict__ g1,
-                                                           float* __restrict__ g2, float* __restrict__ grad,
-                                                           float* __restrict__ red) {
+                                                           const float* __restrict__ h2,
+                                                           const float* __restrict__ out, float* __restrict__ g2,
+                                                           __nv_bfloat16* __restrict__ g2b,
+                                                           __nv_bfloat16* __restrict__ g2t, long long ldt,
+                                                           float* __restrict__ grad, float* __restrict__ red) {
   __shared__ float sd[32];      // dL/dout for the MLP part (0 on linear-only rows)
   __shared__ float sdh[32];     // dL/dout for the head
-  __shared__ float sg2[32][NH + 1];
   const int s0 = blockIdx.x * 32;
   const int tid = threadIdx.x;
   const float inv_sumw = wt ? 1.f / fmaxf(red[1], 1e-30f) : 1.f / batch;
@@ -194,31 +296,22 @@ __global__ void __launch_bounds__(256) backward_act_kernel(const float* __restri
   const float w3 = bf(w[OFF_W3 + tid]);
   float gw3 = 0.f;
   for (int r = 0; r < 32; ++r) {
-    const float a2 = (s0 + r < batch) ? h2[static_cast<long long>(s0 + r) * NH + tid] : 0.f;
+    const bool in = s0 + r < batch;
+    const float a2 = in ? h2[static_cast<long long>(s0 + r) * NH + tid] : 0.f;
     gw3 += a2 * sd[r];
     const float gv = (a2 > 0.f) ? sd[r] * w3 : 0.f;
-    sg2[r][tid] = gv;
-    if (s0 + r < batch) g2[static_cast<long long>(s0 + r) * NH + tid] = gv;
+    const __nv_bfloat16 gb = __float2bfloat16_rn(gv);
+    if (in) {
+      g2[static_cast<long long>(s0 + r) * NH + tid] = gv;
+      g2b[static_cast<long long>(s0 + r) * NH + tid] = gb;
+    }
+    g2t[static_cast<long long>(tid) * ldt + s0 + r] = gb;   // zero beyond the batch
   }
   atomicAdd(&grad[OFF_W3 + tid], gw3);
   if (tid == 0) {
     float gb3 = 0.f;
     for (int r = 0; r < 32; ++r) gb3 += sd[r];
     atomicAdd(&grad[OFF_B3], gb3);
-  }
-  __syncthreads();
-  float acc[32];
-#pragma unroll
-  for (int r = 0; r < 32; ++r) acc[r] = 0.f;
-  for (int jj = 0; jj < NH; ++jj) {
-    const float wkj = bf(w[OFF_W2 + tid * NH + jj]);
-#pragma unroll
-    for (int r = 0; r < 32; ++r) acc[r] += sg2[r][jj] * wkj;
-  }
-  for (int r = 0; r < 32; ++r) {
-    if (s0 + r >= batch) break;
-    const float a1 = h1[static_cast<long long>(s0 + r) * NH + tid];
-    g1[static_cast<long long>(s0 + r) * NH + tid] = (a1 > 0.f) ? acc[r] : 0.f;
   }
 }
 
@@ -484,12 +577,17 @@ static bool chol_solve(double* a, double* b, int n) {
 }
 
 static void free_batch() {
-  cudaFree(g.h1); cudaFree(g.h2); cudaFree(g.g1); cudaFree(g.g2); cudaFree(g.out);
+  cudaFree(g.h1); cudaFree(g.h1t); cudaFree(g.h2); cudaFree(g.g1); cudaFree(g.g2); cudaFree(g.g2b);
+  cudaFree(g.g2t); cudaFree(g.head); cudaFree(g.out);
   cudaFree(g.xb); cudaFree(g.yb); cudaFree(g.wb); cudaFree(g.tb);
-  g.h1 = g.h2 = g.g1 = g.g2 = g.out = g.xb = g.yb = g.wb = nullptr;
+  g.h2 = g.g1 = g.g2 = g.head = g.out = g.xb = g.yb = g.wb = nullptr;
+  g.h1 = g.h1t = g.g2b = g.g2t = nullptr;
   g.tb = nullptr;
   g.cap = 0;
 }
+
+// rows of the transposed activation buffers (the batch capacity rounded up to the 32-row blocks)
+static long long ldt() { return (static_cast<long long>(g.cap) + 31) / 32 * 32; }
 
 static int ensure_cap(int batch) {
   if (batch <= g.cap) return QSGW_OK;
@@ -498,10 +596,15 @@ static int ensure_cap(int batch) {
     free_batch();
   }
   const size_t b = static_cast<size_t>(batch);
-  QSGW_CUDA(cudaMalloc(&g.h1, b * NH * sizeof(float)));
+  const size_t b32 = (b + 31) / 32 * 32;
+  QSGW_CUDA(cudaMalloc(&g.h1, b * NH * sizeof(__nv_bfloat16)));
+  QSGW_CUDA(cudaMalloc(&g.h1t, b32 * NH * sizeof(__nv_bfloat16)));
   QSGW_CUDA(cudaMalloc(&g.h2, b * NH * sizeof(float)));
   QSGW_CUDA(cudaMalloc(&g.g1, b * NH * sizeof(float)));
   QSGW_CUDA(cudaMalloc(&g.g2, b * NH * sizeof(float)));
+  QSGW_CUDA(cudaMalloc(&g.g2b, b * NH * sizeof(__nv_bfloat16)));
+  QSGW_CUDA(cudaMalloc(&g.g2t, b32 * NH * sizeof(__nv_bfloat16)));
+  QSGW_CUDA(cudaMalloc(&g.head, b * sizeof(float)));
   QSGW_CUDA(cudaMalloc(&g.out, b * sizeof(float)));
   QSGW_CUDA(cudaMalloc(&g.xb, b * NIN * sizeof(float)));
   QSGW_CUDA(cudaMalloc(&g.yb, b * sizeof(float)));
@@ -515,21 +618,55 @@ static int grid_for(long long n) {
   return static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, 32LL * ctx().sm_count)));
 }
 
+// the 256 x 256 layer on the tensor cores: C = A Bt^T with one of the epilogues
+template <int EPI>
+static void mma_gemm(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* Bt, long long ldb, int M, int K,
+                     int ksplit, float* C, const __nv_bfloat16* bias, const __nv_bfloat16* mask, cudaStream_t s) {
+  MmaArgs p{A, lda, Bt, ldb, M, NH, K, ksplit, C, NH, bias, mask};
+  const dim3 grid(static_cast<unsigned>((M + 63) / 64), NH / 128, static_cast<unsigned>((K + ksplit - 1) / ksplit));
+  mma_gemm_kernel<EPI><<<grid, 256, 0, s>>>(p);
+  count_launch();
+}
+
+// forward pass of `batch` rows into g.out (training: also the transposed h1 for the weight gradient)
+static void forward_pass(const float* x, const int* tix, int batch, bool train, const float* wt, cudaStream_t s) {
+  const int nb = (batch + 31) / 32;
+  forward_l1_kernel<<<nb, NH, 0, s>>>(x, tix, batch, g.w16, g.master, g.h1, train ? g.h1t : nullptr, ldt(), g.head,
+                                      wt, train ? g.red + 1 : nullptr);
+  mma_gemm<EPI_FWD>(g.h1, NH, g.w2t, NH, batch, NH, NH, g.h2, g.w16 + OFF_B2, nullptr, s);
+  forward_l3_kernel<<<(batch + 7) / 8, 256, 0, s>>>(g.h2, tix, batch, g.w16, g.head, g.out);
+  count_launch(2);
+}
+
 // forward + backward on (x, tix, y, wt) rows already on the device; gradient in g.grad, loss terms in g.red
 static int grad_pass(const float* x, const int* tix, const float* y, const float* wt, int batch, cudaStream_t s) {
   QSGW_CUDA(cudaMemsetAsync(g.grad, 0, NPARAM * sizeof(float), s));
   QSGW_CUDA(cudaMemsetAsync(g.red, 0, 2 * sizeof(float), s));
   const int nb = (batch + 31) / 32;
-  forward_kernel<<<nb, NH, 0, s>>>(x, tix, batch, g.w16, g.master, g.h1, g.h2, g.out, wt, g.red + 1);
-  backward_act_kernel<<<nb, NH, 0, s>>>(x, tix, y, wt, batch, g.w16, g.h1, g.h2, g.out, g.g1, g.g2, g.grad, g.red);
-  const int rpb = 4096;
+  forward_pass(x, tix, batch, true, wt, s);
+  backward_act_kernel<<<nb, NH, 0, s>>>(x, tix, y, wt, batch, g.w16, g.h2, g.out, g.g2, g.g2b, g.g2t, ldt(), g.grad,
+                                        g.red);
+  count_launch();
+  // g1 = relu'(h1) (g2 W2^T): Bt = W2 itself ([k][j], k the output unit)
+  mma_gemm<EPI_BWD>(g.g2b, NH, g.w16 + OFF_W2, NH, batch, NH, NH, g.g1, nullptr, g.h1, s);
+  // dW2 = h1^T g2 over the batch (rows split in ranges of 1024)
+  const int kpad = nb * 32;
+  mma_gemm<EPI_WGRAD>(g.h1t, ldt(), g.g2t, ldt(), NH, kpad, 1024, g.grad + OFF_W2, nullptr, nullptr, s);
+  const int rpb = 1024;
   const int nz = (batch + rpb - 1) / rpb;
-  wgrad_kernel<<<dim3(NH / 32, NH / 32, nz), 256, 0, s>>>(g.h1, NH, g.g2, batch, rpb, g.grad + OFF_W2,
-                                                          g.grad + OFF_B2);
-  wgrad_kernel<<<dim3(1, NH / 32, nz), 256, 0, s>>>(x, NIN, g.g1, batch, rpb, g.grad + OFF_W1, g.grad + OFF_B1);
-  count_launch(4);
+  colsum_kernel<<<dim3(1, nz), NH, 0, s>>>(g.g2, batch, rpb, g.grad + OFF_B2);
+  wgrad_kernel<<<dim3(1, NH / 32, (batch + 4095) / 4096), 256, 0, s>>>(x, NIN, g.g1, batch, 4096, g.grad + OFF_W1,
+                                                                      g.grad + OFF_B1);
+  count_launch(2);
   QSGW_LAUNCH_CHECK("wsurr gradient");
   return QSGW_OK;
+}
+
+// the BF16 weights and the transposed W2 from the FP32 master parameters
+static void refresh_bf16(cudaStream_t s) {
+  to_bf16_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(g.master, g.w16);
+  w2t_kernel<<<(NH * NH + 255) / 256, 256, 0, s>>>(g.w16, g.w2t);
+  count_launch(2);
 }
 
 static int adam_step(float lr, cudaStream_t s) {
@@ -538,7 +675,8 @@ static int adam_step(float lr, cudaStream_t s) {
   const float c1 = 1.f - std::pow(b1, static_cast<float>(g.step));
   const float c2 = 1.f - std::pow(b2, static_cast<float>(g.step));
   adam_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(g.master, g.grad, g.m1, g.m2, g.w16, lr, b1, b2, c1, c2, 1e-8f);
-  count_launch();
+  w2t_kernel<<<(NH * NH + 255) / 256, 256, 0, s>>>(g.w16, g.w2t);
+  count_launch(2);
   QSGW_LAUNCH_CHECK("wsurr adam");
   return QSGW_OK;
 }
@@ -578,6 +716,7 @@ extern "C" int qsgw_wsurr_init(unsigned long long seed) {
   if (!g.ready) {
     QSGW_CUDA(cudaMalloc(&g.master, NPARAM * sizeof(float)));
     QSGW_CUDA(cudaMalloc(&g.w16, NPARAM * sizeof(__nv_bfloat16)));
+    QSGW_CUDA(cudaMalloc(&g.w2t, NH * NH * sizeof(__nv_bfloat16)));
     QSGW_CUDA(cudaMalloc(&g.grad, NPARAM * sizeof(float)));
     QSGW_CUDA(cudaMalloc(&g.m1, NPARAM * sizeof(float)));
     QSGW_CUDA(cudaMalloc(&g.m2, NPARAM * sizeof(float)));
@@ -588,8 +727,8 @@ extern "C" int qsgw_wsurr_init(unsigned long long seed) {
   QSGW_CUDA(cudaMemsetAsync(g.lsq, 0, NTMAX * (NIN * NIN + NIN) * sizeof(double), ctx().stream));
   cudaStream_t s = ctx().stream;
   init_params_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(g.master, seed);
-  to_bf16_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(g.master, g.w16);
-  count_launch(2);
+  count_launch();
+  refresh_bf16(s);
   QSGW_CUDA(cudaMemsetAsync(g.m1, 0, NPARAM * sizeof(float), s));
   QSGW_CUDA(cudaMemsetAsync(g.m2, 0, NPARAM * sizeof(float), s));
   g.step = 0;
@@ -606,8 +745,7 @@ extern "C" int qsgw_wsurr_params(float* host, int set) {
   cudaStream_t s = ctx().stream;
   if (set) {
     QSGW_CUDA(cudaMemcpyAsync(g.master, host, NPARAM * sizeof(float), cudaMemcpyHostToDevice, s));
-    to_bf16_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(g.master, g.w16);
-    count_launch();
+    refresh_bf16(s);
     QSGW_LAUNCH_CHECK("wsurr params");
   } else {
     QSGW_CUDA(cudaMemcpyAsync(host, g.master, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -689,13 +827,14 @@ extern "C" int qsgw_wsurr_forward_d(const float* x_d, const int* tix_d, float* y
   QSGW_ARG(g.ready && x_d && tix_d && y_d && batch >= 0, "wsurr_forward: bad arguments");
   if (batch == 0) return QSGW_OK;
   cudaStream_t s = ctx().stream;
-  // inference keeps no activations; chunks bound the launch size
-  const int chunk = 1 << 22;
+  // chunks of at most 2^16 rows through the activation buffers
+  rc = ensure_cap(std::max(g.cap, std::min(batch, 1 << 16)));
+  if (rc) return rc;
+  const int chunk = g.cap;
   for (int b0 = 0; b0 < batch; b0 += chunk) {
     const int nb = std::min(chunk, batch - b0);
-    forward_kernel<<<(nb + 31) / 32, NH, 0, s>>>(x_d + static_cast<long long>(b0) * NIN, tix_d + b0, nb, g.w16,
-                                                 g.master, nullptr, nullptr, y_d + b0, nullptr, nullptr);
-    count_launch();
+    forward_pass(x_d + static_cast<long long>(b0) * NIN, tix_d + b0, nb, false, nullptr, s);
+    QSGW_CUDA(cudaMemcpyAsync(y_d + b0, g.out, nb * sizeof(float), cudaMemcpyDeviceToDevice, s));
   }
   QSGW_LAUNCH_CHECK("wsurr forward");
   return QSGW_OK;
@@ -848,8 +987,7 @@ extern "C" int qsgw_wsurr_lsq_solve(double ridge, int* rows_solved) {
     ++solved;
   }
   QSGW_CUDA(cudaMemcpyAsync(g.master, p.data(), NPARAM * sizeof(float), cudaMemcpyHostToDevice, s));
-  to_bf16_kernel<<<(NPARAM + 255) / 256, 256, 0, s>>>(g.master, g.w16);
-  count_launch();
+  refresh_bf16(s);
   QSGW_CUDA(cudaMemsetAsync(g.lsq, 0, eq.size() * sizeof(double), s));
   QSGW_CUDA(cudaStreamSynchronize(s));
   QSGW_LAUNCH_CHECK("wsurr lsq_solve");

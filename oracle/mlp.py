@@ -15,6 +15,10 @@ The MLP weights enter as their BF16 roundings (the library computes with a
 BF16 copy of its FP32 master parameters); the linear head C stays FP32.
 Gradients are taken with respect to the master parameters through the
 rounded weights (the straight-through rule the library's Adam step uses).
+The 256 x 256 layer runs on BF16 tensor-core products, so with rounding on
+its operands are rounded too: the layer-1 activations h1 in the forward
+pass and in the weight gradient, the layer-2 gradient g2 in the products
+that give g1 and dW2 (db2 sums the unrounded g2).
 """
 import numpy as np
 
@@ -57,7 +61,8 @@ def forward(p, x, tix, rounded=True):
     x = np.asarray(x, dtype=np.float64)
     a1 = x @ W1 + b1
     h1 = np.maximum(a1, 0.0)
-    a2 = h1 @ W2 + b2
+    h1r = bf16_round(h1.astype(np.float32)).astype(np.float64) if rounded else h1
+    a2 = h1r @ W2 + b2
     h2 = np.maximum(a2, 0.0)
     head = np.einsum('ri,ri->r', C[tix], x)
     y = (np.asarray(tix) < NMLP) * (h2 @ W3 + b3) + head
@@ -79,9 +84,14 @@ def loss_and_grad(p, x, tix, ystar, w=None, rounded=True):
     g[OFF_W3:OFF_B3] = h2.T @ d
     g[OFF_B3] = d.sum()
     g2 = np.outer(d, W3) * (h2 > 0)
-    g[OFF_W2:OFF_B2] = (h1.T @ g2).ravel()
+    if rounded:                                # the tensor-core products' BF16 operands
+        h1r = bf16_round(h1.astype(np.float32)).astype(np.float64)
+        g2r = bf16_round(g2.astype(np.float32)).astype(np.float64)
+    else:
+        h1r, g2r = h1, g2
+    g[OFF_W2:OFF_B2] = (h1r.T @ g2r).ravel()
     g[OFF_B2:OFF_W3] = g2.sum(0)
-    g1 = (g2 @ W2.T) * (h1 > 0)
+    g1 = (g2r @ W2.T) * (h1 > 0)
     g[OFF_W1:OFF_B1] = (x.T @ g1).ravel()
     g[OFF_B1:OFF_W2] = g1.sum(0)
     gc = np.zeros((NTMAX, NIN))

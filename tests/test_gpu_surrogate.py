@@ -33,8 +33,13 @@ def test_forward_and_gradient_match_oracle(qsgw):
     # FP32 / float64 difference of 1e-7 could flip a unit on or off
     W1, b1, W2, b2 = mlp.unpack(p)[:4]
     a1 = x @ W1 + b1
-    a2 = np.maximum(a1, 0.0) @ W2 + b2
-    x = x[(np.abs(a1).min(1) > 1e-4) & (np.abs(a2).min(1) > 1e-4)][:1000]
+    h1 = np.maximum(a1, 0.0)
+    a2 = mlp.bf16_round(h1.astype(np.float32)).astype(np.float64) @ W2 + b2
+    # ... and whose layer-1 activations are clear of a BF16 rounding tie (the tensor-core layer
+    # takes them rounded to BF16; the GPU's FP32 and the oracle's float64 must round alike)
+    m, e = np.frexp(h1)
+    tie = np.abs(m * 2.0 ** 8 - np.floor(m * 2.0 ** 8) - 0.5) < 1e-3   # BF16: 8 significant bits
+    x = x[(np.abs(a1).min(1) > 1e-4) & (np.abs(a2).min(1) > 1e-4) & ~(tie & (h1 > 0)).any(1)][:1000]
     B = len(x)                                      # not a multiple of the 32-row block
     assert B == 1000
     tix = rng.integers(0, 80, B).astype(np.int32)   # both head banks (rows >= 64: no MLP term)
@@ -171,8 +176,11 @@ def trained(qsgw):
 
 def test_trained_network_gains_over_linear_interpolation(trained):
     """What training buys, at the predicted frequencies of held-out q points:
-    the network against the linear interpolation in x its heads start from
-    (the method without learning) and against its least-squares heads alone."""
+    the learned model (least-squares heads + MLP) against the linear
+    interpolation in x its heads start from (the method without learning):
+    at least 10x lower W and QP errors.  Against its least-squares heads alone
+    the MLP adds nothing measurable in W (about 0.2 %), so it is held only to
+    not worsening them."""
     for r in trained["rows"]:
         lin, lsq, tr = r["linear"], r["lsq"], r["trained"]
         assert tr["w_rel"] < 0.1 * lin["w_rel"], r
