@@ -201,13 +201,21 @@ def sigc_flops(lib, s):
 
 
 def run_sigc(lib, s, host=None):
+    """Every Sigma_c task of the step: device arrays through one qsgw_sxcf_correlation_batch_d call,
+    host arrays (the end-to-end run) through qsgw_sxcf_correlation task by task."""
     m = s["mesh"]
+
+    def kw(t, src):
+        return dict(zsec=src["zsec"], zmel=src["zmel"], ns1=1, ns2=s["nm"], ns2r=t["ns2r"], nwxi=t["nwxi"],
+                    nwx=t["nwx"], ntqxx=s["ntq"], wc_imag=src["wi"], wc_real=src["wr"], omega=t["omega"],
+                    ekc=t["ekc"], nctot=0, ef=t["ef"], esmr=t["esmr"], wkkr=s["wkkr"], ua=m["ua"], freqx=m["x"],
+                    wwx=m["wx"], expa=m["expa"], freq_r=s["fr"], nblochpmx=s["N"], ngb=s["N"], ntq=s["ntq"])
+
+    if host is None:
+        lib.sxcf_correlation_batch_d([kw(t, t) for t in s["tasks"]])
+        return
     for i, t in enumerate(s["tasks"]):
-        src = host["tasks"][i] if host else t
-        lib.sxcf_correlation(src["zsec"], src["zmel"], 1, s["nm"], t["ns2r"], t["nwxi"], t["nwx"], s["ntq"],
-                             src["wi"], src["wr"], t["omega"], t["ekc"], 0, t["ef"], t["esmr"], s["wkkr"],
-                             m["ua"], m["x"], m["wx"], m["expa"], s["fr"], nblochpmx=s["N"],
-                             device=host is None, ngb=s["N"], ntq=s["ntq"])
+        lib.sxcf_correlation(**kw(t, host["tasks"][i]))
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -453,11 +461,16 @@ def main():
     else:
         peak = fp64_peak
         peak_note = "cuBLAS ZGEMM (complex128, 4096^3) measured in this run; MEASURED_PEAKS.json has no FP64 figure"
+    # Sigma_c tasks per launch of the dominant kernel (the int8 path batches the step's tasks)
+    tasks_per_launch = len(s["tasks"]) * args.steps / max(k_n, 1)
+    traffic = SIGC_TC_TRAFFIC.get(prec)
     roof = {"bound": "tensor", "achieved": round(achieved, 3) if achieved else None, "peak": round(peak, 3),
             "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if achieved else None,
-            "traffic": SIGC_TC_TRAFFIC.get(prec),
-            "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one Sigma_c task launch "
-                               "(same shape) from ncu" if SIGC_TC_TRAFFIC.get(prec) else "not captured"),
+            "traffic": traffic * tasks_per_launch if traffic else None,
+            "traffic_source": (f"dram__bytes_read.sum + dram__bytes_write.sum of the kernel on one Sigma_c task "
+                               f"of the same shape from ncu ({traffic:.4g} B), times the {tasks_per_launch:g} "
+                               f"tasks a launch runs" if traffic else "not captured"),
+            "tasks_per_launch": tasks_per_launch,
             "kernel": dom_tag, "launch_ms": round(per_launch_ms, 4), "peak_source": peak_note,
             "algorithmic_flops_per_launch": dom_flops * args.steps / max(k_n, 1)}
 

@@ -103,6 +103,13 @@ int tuned_choice(const std::string& key, const std::vector<int>& cands, int heur
   return QSGW_OK;
 }
 
+bool tuned_lookup(const std::string& key, int* v) {
+  auto it = g_cache.find(key);
+  if (it == g_cache.end()) return false;
+  *v = it->second;
+  return true;
+}
+
 int tuned_slices(const std::string& key, const std::vector<int>& cands, int top, double tol,
                  const std::function<int(int, double*)>& err, int fallback, int* chosen) {
   *chosen = fallback;

@@ -23,6 +23,9 @@ int tuned_choice(const std::string& key, const std::vector<int>& cands, int heur
 int tuned_slices(const std::string& key, const std::vector<int>& cands, int top, double tol,
                  const std::function<int(int, double*)>& err, int fallback, int* chosen);
 
+// The cached choice for `key` into *v, if there is one (no trials).
+bool tuned_lookup(const std::string& key, int* v);
+
 // While one of these lives, tuned_choice runs no trials (for calls that add into
 // an output the caller already holds, which a trial would clear).
 struct TuneSuspend {

@@ -204,7 +204,7 @@ struct SegParams {
   const double* mu_a;         // [slot][T * 64] row scales
   const double* nu_b;         // [nrows] column scales
   double post;                // 2^-(12 + 7 (NS - 1))
-  double2* C;
+  double2* const* tile_out;   // [tile] output of the tile's task: column col at tile_out[t] + col ldc
   long long ldc;
   int* err;
 };
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::OFF_MISC + 8);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int mt = blockIdx.x % p.ntm, nt = blockIdx.x / p.ntm;
+  const int mt = blockIdx.x % p.ntm, nt = blockIdx.x / p.ntm;   // the row tiles of a column tile adjacent
   const int group = p.tile_group[nt];
   const int nseg = p.group_nseg[group];
   const int seg0 = p.group_seg_off[group];
@@ -348,11 +348,12 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (ok && !*abort_flag) {
         const int m = mt * 64 + mloc;
         const int part = row >= 64 ? 1 : 0;
+        double2* const C = p.tile_out[nt];
         if (m < p.M) {
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = p.tile_cols[rtile + j];
-            if (col >= 0) reinterpret_cast<double*>(p.C + m + static_cast<long long>(col) * p.ldc)[part] = acc[j];
+            if (col >= 0) reinterpret_cast<double*>(C + m + static_cast<long long>(col) * p.ldc)[part] = acc[j];
           }
         }
       }
@@ -633,11 +634,13 @@ __global__ void oz_slice_w_kernel(int8_t* __restrict__ out, const double2* __res
   }
 }
 
-// Sigma_c B slices: row r = zmel column cols[r] (-1: zero row), [Re b, Im b] per k, into [q][nrows][Kp].
+// Sigma_c B slices: row r = zmel column cols[r] (-1: zero row), [Re b, Im b] per k, into
+// [q][rs][Kp] (slice q of row r at (q rs + r) Kp; rs >= nrows).
 // grid (ceil(Kp/2 / 128), ceil(nrows / 8)), block 256: one row per warp
 template <int NS>
 __global__ void oz_slice_z_kernel(int8_t* __restrict__ out, const double2* __restrict__ z, long long ld, int K,
-                                  const int* __restrict__ cols, int nrows, int Kp, const double* __restrict__ nu) {
+                                  const int* __restrict__ cols, int nrows, long long rs, int Kp,
+                                  const double* __restrict__ nu) {
   const int r = blockIdx.y * 8 + (threadIdx.x >> 5);
   const int k0 = (blockIdx.x * 32 + (threadIdx.x & 31)) * 4;
   if (r >= nrows || k0 >= Kp / 2) return;
@@ -657,7 +660,7 @@ __global__ void oz_slice_z_kernel(int8_t* __restrict__ out, const double2* __res
     uint2 h;
     h.x = pack4(sr[0][q], si[0][q], sr[1][q], si[1][q]);
     h.y = pack4(sr[2][q], si[2][q], sr[3][q], si[3][q]);
-    *reinterpret_cast<uint2*>(out + (static_cast<long long>(q) * nrows + r) * Kp + 2 * k0) = h;
+    *reinterpret_cast<uint2*>(out + (static_cast<long long>(q) * rs + r) * Kp + 2 * k0) = h;
   }
 }
 
@@ -906,35 +909,135 @@ int rel_diff_fro(const double2* a, const double2* b, long long n, cudaStream_t s
   return QSGW_OK;
 }
 
-int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
+static DevBuf g_cols;                                   // Sigma_c column map of every tile of a batch
+
+size_t OzSigcBatch::bytes_per(int ns, int ngb, int mrows, long long nslot, long long ntiles) {
+  const long long T = (mrows + 63) / 64;
+  const long long Kp = ((2LL * ngb + K8 - 1) / K8) * K8;
+  return static_cast<size_t>(ns) * (nslot * T * 128 + ntiles * BN) * Kp + (nslot * T * 64 + ntiles * BN) * 8 +
+         ntiles * BN * 4;
+}
+
+int OzSigcBatch::reserve(int ns, int ngb, int mrows, long long ldc, long long nslot, long long ntiles) {
   QSGW_ARG(ns >= 2 && ns <= 4, "sigc split-i8: %d slices (2..4)", ns);
+  QSGW_ARG(ngb >= 1 && mrows >= 1 && nslot >= 1 && ntiles >= 1,
+           "sigc split-i8: ngb=%d rows=%d slots=%lld tiles=%lld", ngb, mrows, nslot, ntiles);
+  const int T = (mrows + 63) / 64;
+  const int Kp = ((2 * ngb + K8 - 1) / K8) * K8;
+  // exact INT32 levels over one segment (K' = Kp): ns * 4096 * Kp < 2^31; int tile coordinates
+  QSGW_ARG(static_cast<long long>(ns) * 4096 * Kp < (1LL << 31), "sigc split-i8: ngb=%d too large", ngb);
+  QSGW_ARG(ns * nslot * T < (1LL << 31) && ntiles * BN < (1LL << 31),
+           "sigc split-i8: batch of %lld slots, %lld tiles too large", nslot, ntiles);
+  ns_ = ns; ngb_ = ngb; M_ = mrows; ldc_ = ldc; T_ = T; Kp_ = Kp;
+  cap_slot_ = nslot; cap_tiles_ = ntiles;
+  nslot_ = 0; ntiles_ = 0;
+  tile_group_.clear(); group_seg_off_.clear(); group_nseg_.clear(); seg_slot_.clear();
+  segs_.clear(); tile_out_.clear();
+  int rc = g_a8.ensure(static_cast<size_t>(ns) * nslot * T * 128 * Kp);
+  if (rc) return rc;
+  if ((rc = g_b8.ensure(static_cast<size_t>(ns) * ntiles * BN * Kp))) return rc;
+  if ((rc = g_mu.ensure(static_cast<size_t>(nslot) * T * 64 * sizeof(double)))) return rc;
+  if ((rc = g_nu.ensure(static_cast<size_t>(ntiles) * BN * sizeof(double)))) return rc;
+  return g_cols.ensure(static_cast<size_t>(ntiles) * BN * sizeof(int));
+}
+
+int OzSigcBatch::add(const SigcSplitArgs& a, cudaStream_t s) {
   const int ngb = a.ngb;                              // K: rows of W and of the B columns
   const int M = a.mrows > 0 ? a.mrows : ngb;          // output rows: columns of W
   const long long ldz = a.ldz > 0 ? a.ldz : ngb;
   const long long ldc = a.ldc > 0 ? a.ldc : M;
   const long long wst = a.wstride > 0 ? a.wstride : a.ldw * a.ldw;   // one W record
-  const int T = (M + 63) / 64;
-  const int Kp = ((2 * ngb + K8 - 1) / K8) * K8;
-  // exact INT32 levels over one segment (K' = Kp): ns * 4096 * Kp < 2^31
-  QSGW_ARG(static_cast<long long>(ns) * 4096 * Kp < (1LL << 31), "sigc split-i8: ngb=%d too large", ngb);
+  QSGW_ARG(cap_slot_ > 0, "sigc split-i8 batch: add before reserve");
+  QSGW_ARG(ngb == ngb_ && M == M_ && ldc == ldc_,
+           "sigc split-i8 batch: task ngb=%d rows=%d ldc=%lld in a batch of ngb=%d rows=%d ldc=%lld", ngb, M, ldc,
+           ngb_, M_, ldc_);
   const int nslot = a.nimag + a.nreal;
   const int ntiles = static_cast<int>(a.tile_group.size());
   QSGW_ARG(a.tile_cols.size() == static_cast<size_t>(ntiles) * BN, "sigc split-i8: %zu tile columns for %d tiles",
            a.tile_cols.size(), ntiles);
+  QSGW_ARG(a.group_seg_off.size() == a.group_nseg.size() && a.seg_slot.size() == a.segs.size(),
+           "sigc split-i8: inconsistent segment tables");
+  QSGW_ARG(nslot_ + nslot <= cap_slot_ && ntiles_ + ntiles <= cap_tiles_,
+           "sigc split-i8 batch: %lld + %d slots, %lld + %d tiles over the reserved %lld, %lld", nslot_, nslot,
+           ntiles_, ntiles, cap_slot_, cap_tiles_);
+  for (int sl : a.seg_slot) QSGW_ARG(sl >= 0 && sl < nslot, "sigc split-i8: segment slot %d of %d", sl, nslot);
+  for (int g : a.tile_group)
+    QSGW_ARG(g >= 0 && g < static_cast<int>(a.group_nseg.size()), "sigc split-i8: tile group %d", g);
+  for (size_t g = 0; g < a.group_nseg.size(); ++g)
+    QSGW_ARG(a.group_seg_off[g] >= 0 && a.group_nseg[g] >= 0 &&
+                 a.group_seg_off[g] + a.group_nseg[g] <= static_cast<int>(a.segs.size()),
+             "sigc split-i8: group %zu segments %d + %d of %zu", g, a.group_seg_off[g], a.group_nseg[g],
+             a.segs.size());
+  const int T = T_, Kp = Kp_, ns = ns_;
+  const long long slot0 = nslot_, row0 = ntiles_ * BN;
   const int nrows = ntiles * BN;
-  const size_t a_bytes = static_cast<size_t>(ns) * nslot * T * 128 * Kp;
-  const size_t b_bytes = static_cast<size_t>(ns) * nrows * Kp;
-  int rc = g_a8.ensure(a_bytes);
+  // the task's column map: the slicing below reads it now, the contraction at launch()
+  int* d_cols = g_cols.as<int>() + row0;
+  int rc = h2d(d_cols, a.tile_cols.data(), a.tile_cols.size() * sizeof(int), s);
   if (rc) return rc;
-  rc = g_b8.ensure(b_bytes);
-  if (rc) return rc;
-  rc = g_mu.ensure(static_cast<size_t>(nslot) * T * 64 * sizeof(double));
-  if (rc) return rc;
-  rc = g_nu.ensure(static_cast<size_t>(nrows) * sizeof(double));
-  if (rc) return rc;
-  // tables
-  rc = g_tabs.ensure((a.tile_cols.size() + a.tile_group.size() + a.group_seg_off.size() + a.group_nseg.size() +
-                      a.seg_slot.size() + 16) * sizeof(int) + a.segs.size() * sizeof(ZSeg) + 256);
+  double* mu = g_mu.as<double>();
+  double* nu = g_nu.as<double>() + row0;
+  // row scales of A' (= column scales of every W record) and column scales of B
+  oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nimag), 256, 0, s>>>(a.wi, a.ldw, wst, ngb, M, nullptr, T * 64,
+                                                                    mu + slot0 * T * 64);
+  count_launch();
+  if (a.nreal > 0) {
+    oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nreal), 256, 0, s>>>(a.wr, a.ldw, wst, ngb, M, nullptr, T * 64,
+                                                                      mu + (slot0 + a.nimag) * T * 64);
+    count_launch();
+  }
+  oz_colscale_kernel<<<dim3((nrows + 7) / 8, 1), 256, 0, s>>>(a.zmel, ldz, 0, ngb, 0, d_cols, nrows, nu);
+  count_launch();
+  QSGW_LAUNCH_CHECK("oz_colscale_kernel");
+  const int pslice = prof_begin("sigc_slice_i8", s);
+  int8_t* A8 = g_a8.as<int8_t>();
+  int8_t* B8 = g_b8.as<int8_t>() + row0 * Kp;
+  const int nst = static_cast<int>(cap_slot_);
+  const long long rs = cap_tiles_ * BN;
+  const dim3 gk(static_cast<unsigned>((Kp / 2 + 127) / 128));
+  auto slice_w = [&](const double2* w, int n, int gslot0) {
+    const dim3 g(gk.x, static_cast<unsigned>(n * T));
+    if (ns == 2) oz_slice_w_kernel<2><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, nst, gslot0, Kp, mu);
+    else if (ns == 3) oz_slice_w_kernel<3><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, nst, gslot0, Kp, mu);
+    else oz_slice_w_kernel<4><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, nst, gslot0, Kp, mu);
+    count_launch();
+  };
+  slice_w(a.wi, a.nimag, static_cast<int>(slot0));
+  if (a.nreal > 0) slice_w(a.wr, a.nreal, static_cast<int>(slot0) + a.nimag);
+  {
+    const dim3 g(gk.x, static_cast<unsigned>((nrows + 7) / 8));
+    if (ns == 2) oz_slice_z_kernel<2><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, rs, Kp, nu);
+    else if (ns == 3) oz_slice_z_kernel<3><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, rs, Kp, nu);
+    else oz_slice_z_kernel<4><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, rs, Kp, nu);
+    count_launch();
+  }
+  QSGW_LAUNCH_CHECK("Sigma_c int8 slices");
+  prof_end(pslice, s);
+  // host tables of the contraction, in the batch's numbering
+  const int g0 = static_cast<int>(group_nseg_.size());
+  const int sg0 = static_cast<int>(segs_.size());
+  for (size_t g = 0; g < a.group_nseg.size(); ++g) {
+    group_seg_off_.push_back(sg0 + a.group_seg_off[g]);
+    group_nseg_.push_back(a.group_nseg[g]);
+  }
+  for (size_t i = 0; i < a.segs.size(); ++i) {
+    segs_.push_back(a.segs[i]);
+    seg_slot_.push_back(static_cast<int>(slot0) + a.seg_slot[i]);
+  }
+  for (int t = 0; t < ntiles; ++t) {
+    tile_group_.push_back(g0 + a.tile_group[t]);
+    tile_out_.push_back(a.out);
+  }
+  nslot_ += nslot;
+  ntiles_ += ntiles;
+  return QSGW_OK;
+}
+
+int OzSigcBatch::launch(cudaStream_t s) {
+  if (ntiles_ == 0) return QSGW_OK;
+  const int T = T_, Kp = Kp_, ns = ns_;
+  int rc = g_tabs.ensure((tile_group_.size() + group_seg_off_.size() + group_nseg_.size() + seg_slot_.size() + 16) *
+                             sizeof(int) + segs_.size() * sizeof(ZSeg) + tile_out_.size() * sizeof(double2*) + 256);
   if (rc) return rc;
   unsigned char* tb = g_tabs.as<unsigned char>();
   size_t off = 0;
@@ -945,58 +1048,23 @@ int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
     off += (n + 15) & ~size_t(15);
     return dst;
   };
-  const ZSeg* d_segs = reinterpret_cast<const ZSeg*>(put(a.segs.data(), a.segs.size() * sizeof(ZSeg)));
-  const int* d_cols = reinterpret_cast<const int*>(put(a.tile_cols.data(), a.tile_cols.size() * sizeof(int)));
-  const int* d_tg = reinterpret_cast<const int*>(put(a.tile_group.data(), a.tile_group.size() * sizeof(int)));
-  const int* d_gso = reinterpret_cast<const int*>(put(a.group_seg_off.data(), a.group_seg_off.size() * sizeof(int)));
-  const int* d_gns = reinterpret_cast<const int*>(put(a.group_nseg.data(), a.group_nseg.size() * sizeof(int)));
-  const int* d_slot = reinterpret_cast<const int*>(put(a.seg_slot.data(), a.seg_slot.size() * sizeof(int)));
+  SegParams p{};
+  p.segs = reinterpret_cast<const ZSeg*>(put(segs_.data(), segs_.size() * sizeof(ZSeg)));
+  p.tile_out = reinterpret_cast<double2* const*>(put(tile_out_.data(), tile_out_.size() * sizeof(double2*)));
+  p.tile_group = reinterpret_cast<const int*>(put(tile_group_.data(), tile_group_.size() * sizeof(int)));
+  p.group_seg_off = reinterpret_cast<const int*>(put(group_seg_off_.data(), group_seg_off_.size() * sizeof(int)));
+  p.group_nseg = reinterpret_cast<const int*>(put(group_nseg_.data(), group_nseg_.size() * sizeof(int)));
+  p.seg_slot = reinterpret_cast<const int*>(put(seg_slot_.data(), seg_slot_.size() * sizeof(int)));
   if (cprc) return cprc;
-  double* mu = g_mu.as<double>();
-  double* nu = g_nu.as<double>();
-  // row scales of A' (= column scales of every W record) and column scales of B
-  oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nimag), 256, 0, s>>>(a.wi, a.ldw, wst, ngb, M, nullptr,
-                                                                    T * 64, mu);
-  count_launch();
-  if (a.nreal > 0) {
-    oz_colscale_kernel<<<dim3((T * 64 + 7) / 8, a.nreal), 256, 0, s>>>(a.wr, a.ldw, wst, ngb, M, nullptr,
-                                                                      T * 64, mu + static_cast<size_t>(a.nimag) * T * 64);
-    count_launch();
-  }
-  oz_colscale_kernel<<<dim3((nrows + 7) / 8, 1), 256, 0, s>>>(a.zmel, ldz, 0, ngb, 0, d_cols, nrows, nu);
-  count_launch();
-  QSGW_LAUNCH_CHECK("oz_colscale_kernel");
-  const int pslice = prof_begin("sigc_slice_i8", s);
-  int8_t* A8 = g_a8.as<int8_t>();
-  int8_t* B8 = g_b8.as<int8_t>();
-  const dim3 gk(static_cast<unsigned>((Kp / 2 + 127) / 128));
-  auto slice_w = [&](const double2* w, int n, int slot0) {
-    const dim3 g(gk.x, static_cast<unsigned>(n * T));
-    const long long ss = wst;
-    if (ns == 2) oz_slice_w_kernel<2><<<g, 256, 0, s>>>(A8, w, a.ldw, ss, M, ngb, T, nslot, slot0, Kp, mu);
-    else if (ns == 3) oz_slice_w_kernel<3><<<g, 256, 0, s>>>(A8, w, a.ldw, ss, M, ngb, T, nslot, slot0, Kp, mu);
-    else oz_slice_w_kernel<4><<<g, 256, 0, s>>>(A8, w, a.ldw, ss, M, ngb, T, nslot, slot0, Kp, mu);
-    count_launch();
-  };
-  slice_w(a.wi, a.nimag, 0);
-  if (a.nreal > 0) slice_w(a.wr, a.nreal, a.nimag);
-  {
-    const dim3 g(gk.x, static_cast<unsigned>((nrows + 7) / 8));
-    if (ns == 2) oz_slice_z_kernel<2><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, Kp, nu);
-    else if (ns == 3) oz_slice_z_kernel<3><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, Kp, nu);
-    else oz_slice_z_kernel<4><<<g, 256, 0, s>>>(B8, a.zmel, ldz, ngb, d_cols, nrows, Kp, nu);
-    count_launch();
-  }
-  QSGW_LAUNCH_CHECK("Sigma_c int8 slices");
-  prof_end(pslice, s);
-  // maps: A' [Kp, 64, 2, ns * nslot * T] box {64, 64, 2, 1}; B [Kp, nrows, ns] box {64, 128, 1}
+  const long long nrows = cap_tiles_ * BN;
+  // maps: A' [Kp, 64, 2, ns * cap_slot * T] box {64, 64, 2, 1}; B [Kp, cap_rows, ns] box {64, 128, 1}
   CUtensorMap ma, mb;
   {
-    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(ns) * nslot * T};
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), 64, 2, static_cast<cuuint64_t>(ns) * cap_slot_ * T};
     const cuuint64_t str[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * 64,
                                static_cast<cuuint64_t>(Kp) * 128};
     const cuuint32_t box[4] = {K8, 64, 2, 1};
-    rc = make_tensor_map(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, A8, 4, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
+    rc = make_tensor_map(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, g_a8.p, 4, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc) return rc;
   }
   {
@@ -1004,26 +1072,36 @@ int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
                                 static_cast<cuuint64_t>(ns)};
     const cuuint64_t str[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * nrows};
     const cuuint32_t box[3] = {K8, BN, 1};
-    rc = make_tensor_map(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, B8, 3, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
+    rc = make_tensor_map(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, g_b8.p, 3, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc) return rc;
   }
-  SegParams p{};
-  p.M = M;
+  p.M = M_;
   p.ntm = T;
   p.cps = Kp / K8;
-  p.nslot = nslot;
+  p.nslot = static_cast<int>(cap_slot_);
   p.T = T;
-  p.nrows = nrows;
-  p.tile_group = d_tg; p.tile_cols = d_cols; p.group_seg_off = d_gso; p.group_nseg = d_gns;
-  p.seg_slot = d_slot; p.segs = d_segs;
-  p.mu_a = mu; p.nu_b = nu;
+  p.nrows = static_cast<int>(nrows);
+  p.tile_cols = g_cols.as<int>();
+  p.mu_a = g_mu.as<double>(); p.nu_b = g_nu.as<double>();
   p.post = post_scale(ns);
-  p.C = a.out; p.ldc = ldc;
+  p.ldc = ldc_;
   p.err = ctx().d_flags + 1;
-  const dim3 grid(static_cast<unsigned>(T * ntiles));
+  const dim3 grid(static_cast<unsigned>(static_cast<long long>(T) * ntiles_));
+  nslot_ = 0; ntiles_ = 0; cap_slot_ = 0; cap_tiles_ = 0;      // the next batch starts with reserve()
   if (ns == 2) return launch_seg<2>(ma, mb, p, grid, s);
   if (ns == 3) return launch_seg<3>(ma, mb, p, grid, s);
   return launch_seg<4>(ma, mb, p, grid, s);
+}
+
+int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
+  const int M = a.mrows > 0 ? a.mrows : a.ngb;
+  const long long ldc = a.ldc > 0 ? a.ldc : M;
+  if (a.tile_group.empty()) return QSGW_OK;
+  OzSigcBatch b;
+  int rc = b.reserve(ns, a.ngb, M, ldc, a.nimag + a.nreal, static_cast<long long>(a.tile_group.size()));
+  if (rc) return rc;
+  if ((rc = b.add(a, s))) return rc;
+  return b.launch(s);
 }
 
 int zgemm_ch_i8(double2* C, long long ldc, int M, int N, int K, const double2* W, long long ldw, const double2* B,

@@ -14,6 +14,30 @@ constexpr int kOzTileN = 128;
 // columns per tile) with ns int8 slices per operand (2..4).
 int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s);
 
+// Several such contractions of one shape (equal ngb, row count and ldc; each task with its own W
+// records, zmel, weights and output) in ONE launch of the int8 kernel.  reserve() sizes the slice
+// buffers for the whole batch (slots = sum of nimag + nreal, tiles = sum of the tile counts);
+// add() slices one task into them on stream s -- its W records and zmel may be overwritten by
+// work enqueued after add(), its weight tables (the ZSeg scales) and output must stay valid until
+// launch(); launch() runs the tiles of every added task, task after task, and ends the batch.
+// The outputs are those of one sigc_split_i8 call per task, bit for bit.  One batch at a time
+// (the slice buffers are the library's).
+class OzSigcBatch {
+ public:
+  int reserve(int ns, int ngb, int mrows, long long ldc, long long nslot, long long ntiles);
+  int add(const SigcSplitArgs& a, cudaStream_t s);
+  int launch(cudaStream_t s);
+  // device bytes of the slice buffers for nslot slots and ntiles tiles
+  static size_t bytes_per(int ns, int ngb, int mrows, long long nslot, long long ntiles);
+
+ private:
+  int ns_ = 0, ngb_ = 0, M_ = 0, T_ = 0, Kp_ = 0;
+  long long ldc_ = 0, cap_slot_ = 0, cap_tiles_ = 0, nslot_ = 0, ntiles_ = 0;
+  std::vector<int> tile_group_, group_seg_off_, group_nseg_, seg_slot_;
+  std::vector<ZSeg> segs_;
+  std::vector<double2*> tile_out_;
+};
+
 // Binned chi0 rank-k update:
 //   C(:, :, slab[b]) += sum_{e in bin b} w_e conj(z_col(e)(0:M)) z_col(e)(row_b0 : row_b0+N)^T
 // with bin b's entries e in [ebeg[b], ebeg[b] + cnt[b]); col(e) = ecol_d[e], or e - ebeg[b]

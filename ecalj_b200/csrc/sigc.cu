@@ -13,6 +13,7 @@
 #include <cmath>
 #include <map>
 #include <set>
+#include <string>
 #include <algorithm>
 #include <vector>
 #include "zgemm_f64.cuh"
@@ -236,12 +237,85 @@ static int sxcf_check(const qsgw_sxcf_args* a) {
   return QSGW_OK;
 }
 
-int sxcf_device(const qsgw_sxcf_args& a) {
+// ---- one task, split into the steps a batch of tasks interleaves
+// host plan: pole entries, the real-axis records they read, and the column tiles.  Columns are
+// sorted by their pole bin ixs (0 = no pole) and cut into tiles of the kernel's column width; a
+// tile's segments are the niw+1 imaginary slots and the union of its columns' real-axis bins.
+// scale_bin[r][col] = the column's pole weight on record r (zero when the column has no pole
+// there), so mixing bins in a tile adds no padding columns.
+struct SxcfPlan {
+  int nm = 0;
+  long long ncol = 0;
+  std::vector<int> recs;                 // real-axis bins used, in record order
+  std::vector<double> scale_bin;         // [nrec][ncol]
+  std::vector<int> tile_cols, tile_group, gseg_off, gnseg, seg_slot;   // slot niw+1+r = record r
+};
+
+static int sxcf_plan(const qsgw_sxcf_args& a, int tilew, SxcfPlan& pl) {
+  const int niw = a.niw;
+  pl.nm = a.ns2 - a.ns1 + 1;
+  pl.ncol = static_cast<long long>(pl.nm) * a.ntqxx;
+  const long long ncol = pl.ncol;
+  std::vector<PoleEntry> poles;
+  int rc = pole_table_h(a, poles);
+  if (rc) return rc;
+  // bins needed by the pole entries, restricted to [nwxi, nwx] (:557)
+  std::map<int, int> bin_slot;
+  for (const auto& e : poles)
+    for (int i = 0; i < 3; ++i) {
+      const int b = e.ixs - 1 + i;
+      if (b >= a.nwxi && b <= a.nwx && !bin_slot.count(b)) bin_slot.emplace(b, 0);
+    }
+  pl.recs.clear();
+  for (auto& kv : bin_slot) { kv.second = static_cast<int>(pl.recs.size()); pl.recs.push_back(kv.first); }
+  const int nrec = static_cast<int>(pl.recs.size());
+  std::vector<int> key(ncol, 0);
+  for (const auto& e : poles) key[e.col] = e.ixs;
+  pl.scale_bin.assign(static_cast<size_t>(std::max(nrec, 1)) * ncol, 0.0);
+  for (const auto& e : poles)
+    for (int i = 0; i < 3; ++i) {
+      auto it = bin_slot.find(e.ixs - 1 + i);
+      if (it != bin_slot.end()) pl.scale_bin[static_cast<size_t>(it->second) * ncol + e.col] = e.w3[i];
+    }
+  std::vector<int> order(ncol);
+  for (long long c = 0; c < ncol; ++c) order[c] = static_cast<int>(c);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
+  pl.tile_cols.clear(); pl.tile_group.clear(); pl.gseg_off.clear(); pl.gnseg.clear(); pl.seg_slot.clear();
+  int gidx = 0;
+  for (long long t0 = 0; t0 < ncol; t0 += tilew) {
+    const long long t1 = std::min<long long>(ncol, t0 + tilew);
+    pl.gseg_off.push_back(static_cast<int>(pl.seg_slot.size()));
+    for (int sgi = 0; sgi <= niw; ++sgi) pl.seg_slot.push_back(sgi);
+    std::set<int> rset;                          // records used by the tile's columns
+    for (long long j = t0; j < t1; ++j) {
+      const int k = key[order[j]];
+      if (k <= 0) continue;
+      for (int i = 0; i < 3; ++i) {
+        auto it = bin_slot.find(k - 1 + i);
+        if (it != bin_slot.end()) rset.insert(it->second);
+      }
+    }
+    for (int r : rset) pl.seg_slot.push_back(niw + 1 + r);
+    pl.gnseg.push_back(static_cast<int>(pl.seg_slot.size()) - pl.gseg_off.back());
+    pl.tile_group.push_back(gidx++);
+    for (int j = 0; j < tilew; ++j) pl.tile_cols.push_back(t0 + j < t1 ? order[t0 + j] : -1);
+  }
+  return QSGW_OK;
+}
+
+// Per-task device buffers: the imaginary-axis weights, the pole weights and czmelwc live until the
+// contraction and the final product have run; the W operands (unpacked / hermitised records) only
+// until the contraction has read them (the int8 batch slices them at once).
+struct SxcfBufs {
+  DevBuf *wg, *w3, *cz, *wi, *wr;
+};
+
+// device side of the plan: wgtim (:432-458), the W operands, the pole weights; fills sa (the
+// segments point into the task's buffers) with out = czmelwc
+static int sxcf_bind(const qsgw_sxcf_args& a, SxcfPlan& pl, const SxcfBufs& b, SigcSplitArgs& sa) {
   cudaStream_t s = ctx().stream;
-  if (a.ns1 > a.ns2 || a.ntqxx == 0) return QSGW_OK;   // :418
-  const int ngb = a.ngb, niw = a.niw, nm = a.ns2 - a.ns1 + 1;
-  const long long ncol = static_cast<long long>(nm) * a.ntqxx;
-  const double2* zmel = reinterpret_cast<const double2*>(a.zmel);
+  const int ngb = a.ngb, niw = a.niw;
+  const long long ncol = pl.ncol;
   // ---- 1. imaginary-axis weights on the GPU
   int rc = g_sc_tabs.ensure((4 * niw + a.ntq + a.nekc + 8) * sizeof(double));
   if (rc) return rc;
@@ -252,177 +326,157 @@ int sxcf_device(const qsgw_sxcf_args& a) {
   if ((rc = h2d(d_ex, a.expa, niw * sizeof(double), s))) return rc;
   if ((rc = h2d(d_om, a.omega, a.ntq * sizeof(double), s))) return rc;
   if ((rc = h2d(d_ekc, a.ekc, a.nekc * sizeof(double), s))) return rc;
-  rc = g_sc_wg.ensure(ncol * (niw + 1) * sizeof(double));
-  if (rc) return rc;
+  if ((rc = b.wg->ensure(ncol * (niw + 1) * sizeof(double)))) return rc;
   wgtim_kernel<<<static_cast<int>((ncol + 127) / 128), 128, 0, s>>>(
-      g_sc_wg.as<double>(), niw, a.ns1, nm, a.ntqxx, a.nctot, d_om, d_ekc, a.esmr, a.wkkr, a.ua, d_x, d_wt, d_ex);
+      b.wg->as<double>(), niw, a.ns1, pl.nm, a.ntqxx, a.nctot, d_om, d_ekc, a.esmr, a.wkkr, a.ua, d_x, d_wt, d_ex);
   count_launch();
   QSGW_LAUNCH_CHECK("wgtim_kernel");
-  // ---- 2. pole entries (host)
-  std::vector<PoleEntry> poles;
-  rc = pole_table_h(a, poles);
-  if (rc) return rc;
   // ---- W operands
   const long long ldw = a.keepwv ? ngb : a.nblochpmx;
   const long long wsz = ldw * ldw;
   const double2* wi = reinterpret_cast<const double2*>(a.wc_imag);
   const double2* wr_src = reinterpret_cast<const double2*>(a.wc_real);
   if (a.keepwv) {
-    rc = g_sc_wi.ensure(wsz * (niw + 1) * sizeof(double2));
-    if (rc) return rc;
-    unpack_upper_kernel<<<grid_for(wsz * (niw + 1)), 256, 0, s>>>(g_sc_wi.as<double2>(), wi, ngb, niw + 1);
+    if ((rc = b.wi->ensure(wsz * (niw + 1) * sizeof(double2)))) return rc;
+    unpack_upper_kernel<<<grid_for(wsz * (niw + 1)), 256, 0, s>>>(b.wi->as<double2>(), wi, ngb, niw + 1);
     count_launch();
     QSGW_LAUNCH_CHECK("unpack_upper_kernel");
-    wi = g_sc_wi.as<double2>();
+    wi = b.wi->as<double2>();
   }
-  // bins needed by the pole entries, restricted to [nwxi, nwx] (:557)
-  std::map<int, int> bin_slot;
-  for (const auto& e : poles)
-    for (int i = 0; i < 3; ++i) {
-      const int b = e.ixs - 1 + i;
-      if (b >= a.nwxi && b <= a.nwx && !bin_slot.count(b)) bin_slot.emplace(b, 0);
-    }
-  std::vector<int> recs;
-  for (auto& kv : bin_slot) { kv.second = static_cast<int>(recs.size()); recs.push_back(kv.first); }
-  const int nrec = static_cast<int>(recs.size());
+  const int nrec = static_cast<int>(pl.recs.size());
   const double2* wr = nullptr;
   if (nrec > 0) {
-    rc = g_sc_wr.ensure(wsz * nrec * sizeof(double2));
-    if (rc) return rc;
-    rc = g_sc_recs.ensure(nrec * sizeof(int));
-    if (rc) return rc;
+    if ((rc = b.wr->ensure(wsz * nrec * sizeof(double2)))) return rc;
     if (a.keepwv) {
       // packed records are already (W+W^H)/2; unpack only the used ones
       const long long np = static_cast<long long>(ngb) * (ngb + 1) / 2;
       for (int q = 0; q < nrec; ++q) {
-        unpack_upper_kernel<<<grid_for(wsz), 256, 0, s>>>(g_sc_wr.as<double2>() + q * wsz, wr_src + recs[q] * np, ngb, 1);
+        unpack_upper_kernel<<<grid_for(wsz), 256, 0, s>>>(b.wr->as<double2>() + q * wsz, wr_src + pl.recs[q] * np,
+                                                          ngb, 1);
         count_launch();
         QSGW_LAUNCH_CHECK("unpack_upper_kernel");
       }
     } else {
-      if ((rc = h2d(g_sc_recs.p, recs.data(), nrec * sizeof(int), s))) return rc;
+      if ((rc = g_sc_recs.ensure(nrec * sizeof(int)))) return rc;
+      if ((rc = h2d(g_sc_recs.p, pl.recs.data(), nrec * sizeof(int), s))) return rc;
       hermitize_kernel<<<dim3((ngb + 31) / 32, (ngb + 31) / 32, nrec), dim3(32, 8), 0, s>>>(
-          g_sc_wr.as<double2>(), wr_src, g_sc_recs.as<int>(), ngb, ldw, nrec);
+          b.wr->as<double2>(), wr_src, g_sc_recs.as<int>(), ngb, ldw, nrec);
       count_launch();
       QSGW_LAUNCH_CHECK("hermitize_kernel");
     }
-    wr = g_sc_wr.as<double2>();
+    wr = b.wr->as<double2>();
   }
-  // ---- column tiles: columns sorted by their pole bin ixs (0 = no pole), cut into tiles of
-  // the kernel's column width; a tile's segments are the niw+1 imaginary slots and the union of
-  // its columns' real-axis bins.  scale_bin[r][col] = the column's pole weight on record r (zero
-  // when the column has no pole there), so mixing bins in a tile adds no padding columns.
-  std::vector<int> key(ncol, 0);
-  for (const auto& e : poles) key[e.col] = e.ixs;
-  std::vector<double> scale_bin(static_cast<size_t>(std::max(nrec, 1)) * ncol, 0.0);
-  for (const auto& e : poles)
-    for (int i = 0; i < 3; ++i) {
-      auto it = bin_slot.find(e.ixs - 1 + i);
-      if (it != bin_slot.end()) scale_bin[static_cast<size_t>(it->second) * ncol + e.col] = e.w3[i];
-    }
-  rc = g_sc_w3.ensure(scale_bin.size() * sizeof(double));
+  if ((rc = b.w3->ensure(pl.scale_bin.size() * sizeof(double)))) return rc;
+  if ((rc = h2d(b.w3->p, pl.scale_bin.data(), pl.scale_bin.size() * sizeof(double), s))) return rc;
+  if ((rc = b.cz->ensure(static_cast<size_t>(ngb) * ncol * sizeof(double2)))) return rc;
+  sa = SigcSplitArgs();
+  sa.ngb = ngb; sa.ldw = ldw;
+  sa.wi = wi; sa.nimag = niw + 1;
+  sa.wr = wr; sa.nreal = nrec;
+  sa.zmel = reinterpret_cast<const double2*>(a.zmel); sa.ncol = ncol;
+  sa.wgt = b.wg->as<double>(); sa.nwgt = ncol * (niw + 1);
+  sa.w3 = b.w3->as<double>(); sa.nw3 = nrec == 0 ? 0 : static_cast<long long>(nrec) * ncol;
+  sa.tile_cols = pl.tile_cols; sa.tile_group = pl.tile_group;
+  sa.group_seg_off = pl.gseg_off; sa.group_nseg = pl.gnseg; sa.seg_slot = pl.seg_slot;
+  sa.segs.resize(pl.seg_slot.size());
+  for (size_t i = 0; i < pl.seg_slot.size(); ++i) {
+    const int sl = pl.seg_slot[i];
+    sa.segs[i] = sl <= niw ? ZSeg{wi + sl * wsz, sa.wgt + sl, niw + 1, 0}
+                           : ZSeg{wr + (sl - niw - 1) * wsz, sa.w3 + static_cast<long long>(sl - niw - 1) * ncol, 1, 0};
+  }
+  sa.out = b.cz->as<double2>();
+  return QSGW_OK;
+}
+
+// ---- 4. zsec += czmelwc^H zmel (:599) and the Im clamp (:601-607)
+static int sxcf_finish(const qsgw_sxcf_args& a, const double2* cz) {
+  cudaStream_t s = ctx().stream;
+  const long long kk = static_cast<long long>(a.ngb) * (a.ns2 - a.ns1 + 1);
+  const double2* zmel = reinterpret_cast<const double2*>(a.zmel);
+  int rc = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,
+                     make_double2(1, 0), reinterpret_cast<double2*>(a.zsec), a.ntq, 0, 1, s);
   if (rc) return rc;
-  if ((rc = h2d(g_sc_w3.p, scale_bin.data(), scale_bin.size() * sizeof(double), s))) return rc;
-  std::vector<int> order(ncol);
-  for (long long c = 0; c < ncol; ++c) order[c] = static_cast<int>(c);
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
+  clamp_diag_kernel<<<(a.ntqxx + 127) / 128, 128, 0, s>>>(reinterpret_cast<double2*>(a.zsec), a.ntqxx, a.ntq);
+  count_launch();
+  QSGW_LAUNCH_CHECK("clamp_diag_kernel");
+  return QSGW_OK;
+}
+
+static std::string sigc_slice_key(const qsgw_sxcf_args& a) {
+  char key[200];
+  std::snprintf(key, sizeof(key), "sigc_i8 slices ngb=%d nm=%d ntq=%d niw=%d", a.ngb, a.ns2 - a.ns1 + 1, a.ntqxx,
+                a.niw);
+  return key;
+}
+
+// slice count of the int8 contraction of task a (sa bound): the fixed count, or the smallest whose
+// Sigma_c diagonal (this call's contribution, the quantity the QP energies take) stays within the
+// target of the 4-slice one
+static int sxcf_i8_slices(const qsgw_sxcf_args& a, const SigcSplitArgs& sa, int* ns_out) {
+  cudaStream_t s = ctx().stream;
+  int ns = ctx().nslices;
+  if (ns == 0) {
+    const long long kk = static_cast<long long>(a.ngb) * (a.ns2 - a.ns1 + 1);
+    const double2* zmel = reinterpret_cast<const double2*>(a.zmel);
+    std::vector<double> ref, cur;
+    auto diag = [&](int n, std::vector<double>& d) -> int {
+      int r = sigc_split_i8(sa, n, s);
+      if (r) return r;
+      r = g_sc_trial.ensure(static_cast<size_t>(a.ntqxx) * a.ntqxx * sizeof(double2));
+      if (r) return r;
+      r = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), sa.out, kk, 0, zmel, kk, 0,
+                    make_double2(0, 0), g_sc_trial.as<double2>(), a.ntqxx, 0, 1, s);
+      if (r) return r;
+      std::vector<double2> h(static_cast<size_t>(a.ntqxx) * a.ntqxx);
+      QSGW_CUDA(cudaMemcpyAsync(h.data(), g_sc_trial.p, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+      QSGW_CUDA(cudaStreamSynchronize(s));
+      d.resize(a.ntqxx);
+      for (int i = 0; i < a.ntqxx; ++i) d[i] = h[static_cast<size_t>(i) * (a.ntqxx + 1)].x;
+      return QSGW_OK;
+    };
+    auto err = [&](int n, double* e) -> int {
+      int r = ref.empty() ? diag(4, ref) : QSGW_OK;
+      if (r) return r;
+      r = diag(n, cur);
+      if (r) return r;
+      *e = 0.0;
+      for (int i = 0; i < a.ntqxx; ++i) *e = std::max(*e, std::fabs(cur[i] - ref[i]));
+      return QSGW_OK;
+    };
+    // the estimate comes from this call; later calls of the shape (other q, other bands) vary
+    // by a few times, so the choice keeps a factor 4 of margin
+    int rc = tuned_slices(sigc_slice_key(a), {2, 3}, 4, 0.25 * ctx().sigc_qp_tol, err, 4, &ns);
+    if (rc) return rc;
+  }
+  *ns_out = ns;
+  return QSGW_OK;
+}
+
+int sxcf_device(const qsgw_sxcf_args& a) {
+  cudaStream_t s = ctx().stream;
+  if (a.ns1 > a.ns2 || a.ntqxx == 0) return QSGW_OK;   // :418
   const bool split = ctx().prec_mode != QSGW_PREC_FP64;
   const bool i8 = ctx().prec_mode == QSGW_PREC_SPLIT_I8;
   // column tile of the int8 / split-FP16 / FP64 kernel
   const int tilew = i8 ? kOzTileN : (split ? sigc_split_tile_width() : ZG_BN);
-  std::vector<ZSeg> segs;
-  std::vector<int> gseg_off, gnseg, tile_group, tile_cols, seg_slot;
-  int gidx = 0;
-  for (long long t0 = 0; t0 < ncol; t0 += tilew) {
-    const long long t1 = std::min<long long>(ncol, t0 + tilew);
-    gseg_off.push_back(static_cast<int>(segs.size()));
-    for (int sgi = 0; sgi <= niw; ++sgi) {
-      ZSeg z{wi + sgi * wsz, g_sc_wg.as<double>() + sgi, niw + 1, 0};
-      segs.push_back(z);
-      seg_slot.push_back(sgi);
-    }
-    std::set<int> rset;                          // records used by the tile's columns
-    for (long long j = t0; j < t1; ++j) {
-      const int k = key[order[j]];
-      if (k <= 0) continue;
-      for (int i = 0; i < 3; ++i) {
-        auto it = bin_slot.find(k - 1 + i);
-        if (it != bin_slot.end()) rset.insert(it->second);
-      }
-    }
-    for (int r : rset) {
-      ZSeg z{wr + r * wsz, g_sc_w3.as<double>() + static_cast<long long>(r) * ncol, 1, 0};
-      segs.push_back(z);
-      seg_slot.push_back(niw + 1 + r);
-    }
-    gnseg.push_back(static_cast<int>(segs.size()) - gseg_off.back());
-    tile_group.push_back(gidx);
-    for (int j = 0; j < tilew; ++j) tile_cols.push_back(t0 + j < t1 ? order[t0 + j] : -1);
-    ++gidx;
-  }
-  const int ntiles = static_cast<int>(tile_group.size());
-  rc = g_sc_cz.ensure(static_cast<size_t>(ngb) * ncol * sizeof(double2));
+  SxcfPlan pl;
+  int rc = sxcf_plan(a, tilew, pl);
   if (rc) return rc;
-  double2* cz = g_sc_cz.as<double2>();
-  if (split) {
+  SigcSplitArgs sa;
+  rc = sxcf_bind(a, pl, SxcfBufs{&g_sc_wg, &g_sc_w3, &g_sc_cz, &g_sc_wi, &g_sc_wr}, sa);
+  if (rc) return rc;
+  if (i8) {
+    // ---- 3. imaginary axis + poles: int8 slices on tcgen05
+    int ns = 0;
+    if ((rc = sxcf_i8_slices(a, sa, &ns))) return rc;
+    rc = sigc_split_i8(sa, ns, s);
+  } else if (split) {
     // ---- 3'. the same contraction in split FP16 on tcgen05
-    SigcSplitArgs sa;
-    sa.ngb = ngb; sa.ldw = ldw;
-    sa.wi = wi; sa.nimag = niw + 1;
-    sa.wr = wr; sa.nreal = nrec;
-    sa.zmel = zmel; sa.ncol = ncol;
-    sa.wgt = g_sc_wg.as<double>(); sa.nwgt = ncol * (niw + 1);
-    sa.w3 = g_sc_w3.as<double>(); sa.nw3 = (poles.empty() || nrec == 0) ? 0 : static_cast<long long>(nrec) * ncol;
-    sa.tile_cols = std::move(tile_cols); sa.tile_group = std::move(tile_group);
-    sa.group_seg_off = std::move(gseg_off); sa.group_nseg = std::move(gnseg);
-    sa.seg_slot = std::move(seg_slot); sa.segs = std::move(segs);
-    sa.out = cz;
-    if (i8) {
-      int ns = ctx().nslices;
-      if (ns == 0) {
-        // automatic slice count: the smallest whose Sigma_c diagonal (this call's contribution,
-        // the quantity the QP energies take) stays within the target of the 4-slice one
-        const long long kk = static_cast<long long>(ngb) * nm;
-        std::vector<double> ref, cur;
-        auto diag = [&](int n, std::vector<double>& d) -> int {
-          int r = sigc_split_i8(sa, n, s);
-          if (r) return r;
-          r = g_sc_trial.ensure(static_cast<size_t>(a.ntqxx) * a.ntqxx * sizeof(double2));
-          if (r) return r;
-          r = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,
-                        make_double2(0, 0), g_sc_trial.as<double2>(), a.ntqxx, 0, 1, s);
-          if (r) return r;
-          std::vector<double2> h(static_cast<size_t>(a.ntqxx) * a.ntqxx);
-          QSGW_CUDA(cudaMemcpyAsync(h.data(), g_sc_trial.p, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
-          QSGW_CUDA(cudaStreamSynchronize(s));
-          d.resize(a.ntqxx);
-          for (int i = 0; i < a.ntqxx; ++i) d[i] = h[static_cast<size_t>(i) * (a.ntqxx + 1)].x;
-          return QSGW_OK;
-        };
-        auto err = [&](int n, double* e) -> int {
-          int r = ref.empty() ? diag(4, ref) : QSGW_OK;
-          if (r) return r;
-          r = diag(n, cur);
-          if (r) return r;
-          *e = 0.0;
-          for (int i = 0; i < a.ntqxx; ++i) *e = std::max(*e, std::fabs(cur[i] - ref[i]));
-          return QSGW_OK;
-        };
-        char key[200];
-        std::snprintf(key, sizeof(key), "sigc_i8 slices ngb=%d nm=%d ntq=%d niw=%d", ngb, nm, a.ntqxx, niw);
-        // the estimate comes from this call; later calls of the shape (other q, other bands) vary
-        // by a few times, so the choice keeps a factor 4 of margin
-        rc = tuned_slices(key, {2, 3}, 4, 0.25 * ctx().sigc_qp_tol, err, 4, &ns);
-        if (rc) return rc;
-      }
-      rc = sigc_split_i8(sa, ns, s);
-    } else {
-      rc = sigc_split_f16(sa, s);
-    }
-    if (rc) return rc;
+    rc = sigc_split_f16(sa, s);
   } else {
-    const size_t tb = segs.size() * sizeof(ZSeg) + (gseg_off.size() + gnseg.size() + tile_group.size() +
-                                                    tile_cols.size()) * sizeof(int);
+    const size_t tb = sa.segs.size() * sizeof(ZSeg) +
+                      (sa.group_seg_off.size() + sa.group_nseg.size() + sa.tile_group.size() + sa.tile_cols.size()) *
+                          sizeof(int);
     rc = g_sc_tmp.ensure(tb + 16 * 5);
     if (rc) return rc;
     unsigned char* tbase = g_sc_tmp.as<unsigned char>();
@@ -435,28 +489,97 @@ int sxcf_device(const qsgw_sxcf_args& a) {
       return dst;
     };
     ZParams p{};
-    p.segs = reinterpret_cast<const ZSeg*>(put(segs.data(), segs.size() * sizeof(ZSeg)));
-    p.group_seg_off = reinterpret_cast<const int*>(put(gseg_off.data(), gseg_off.size() * sizeof(int)));
-    p.group_nseg = reinterpret_cast<const int*>(put(gnseg.data(), gnseg.size() * sizeof(int)));
-    p.tile_group = reinterpret_cast<const int*>(put(tile_group.data(), tile_group.size() * sizeof(int)));
-    p.tile_cols = reinterpret_cast<const int*>(put(tile_cols.data(), tile_cols.size() * sizeof(int)));
+    p.segs = reinterpret_cast<const ZSeg*>(put(sa.segs.data(), sa.segs.size() * sizeof(ZSeg)));
+    p.group_seg_off = reinterpret_cast<const int*>(put(sa.group_seg_off.data(), sa.group_seg_off.size() * sizeof(int)));
+    p.group_nseg = reinterpret_cast<const int*>(put(sa.group_nseg.data(), sa.group_nseg.size() * sizeof(int)));
+    p.tile_group = reinterpret_cast<const int*>(put(sa.tile_group.data(), sa.tile_group.size() * sizeof(int)));
+    p.tile_cols = reinterpret_cast<const int*>(put(sa.tile_cols.data(), sa.tile_cols.size() * sizeof(int)));
     if (cprc) return cprc;
     // ---- 3. imaginary axis + poles in one launch
-    p.M = ngb; p.K = ngb;
-    p.a_rs = ldw; p.a_ks = 1; p.a_conj = 1;             // Wc^H (:492 opA = m_op_C)
-    p.B = zmel; p.b_rs = ngb; p.b_ks = 1; p.b_conj = 0;
-    p.C = cz; p.ldc = ngb; p.beta_zero = 1;
-    rc = zgemm_seg_launch(p, ntiles, s);
-    if (rc) return rc;
+    p.M = a.ngb; p.K = a.ngb;
+    p.a_rs = sa.ldw; p.a_ks = 1; p.a_conj = 1;          // Wc^H (:492 opA = m_op_C)
+    p.B = sa.zmel; p.b_rs = a.ngb; p.b_ks = 1; p.b_conj = 0;
+    p.C = sa.out; p.ldc = a.ngb; p.beta_zero = 1;
+    rc = zgemm_seg_launch(p, static_cast<int>(sa.tile_group.size()), s);
   }
-  // ---- 4. zsec += czmelwc^H zmel (:599) and the Im clamp (:601-607)
-  const long long kk = static_cast<long long>(ngb) * nm;
-  rc = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,
-                 make_double2(1, 0), reinterpret_cast<double2*>(a.zsec), a.ntq, 0, 1, s);
   if (rc) return rc;
-  clamp_diag_kernel<<<(a.ntqxx + 127) / 128, 128, 0, s>>>(reinterpret_cast<double2*>(a.zsec), a.ntqxx, a.ntq);
-  count_launch();
-  QSGW_LAUNCH_CHECK("clamp_diag_kernel");
+  return sxcf_finish(a, sa.out);
+}
+
+// Tasks of one shape in SPLIT_I8 share the launches of the int8 contraction: the tasks of a group
+// are planned on the host, then each is bound and sliced into the batch buffers (its W operands
+// are read once, so the next task's records can reuse the same scratch), then one launch runs every
+// tile of the group, then the final products run task by task.  Groups are cut where the shape or
+// the slice count changes or the group's scratch passes kSigcBatchBytes.
+static constexpr size_t kSigcBatchBytes = size_t(8) << 30;
+static std::vector<DevBuf> g_sb_wg, g_sb_w3, g_sb_cz;   // per task of a group
+
+int sxcf_batch_device(const qsgw_sxcf_args* t, int n) {
+  if (ctx().prec_mode != QSGW_PREC_SPLIT_I8) {
+    for (int i = 0; i < n; ++i) {
+      const int rc = sxcf_device(t[i]);
+      if (rc) return rc;
+    }
+    return QSGW_OK;
+  }
+  cudaStream_t s = ctx().stream;
+  int i = 0;
+  while (i < n) {
+    const qsgw_sxcf_args& a0 = t[i];
+    if (a0.ns1 > a0.ns2 || a0.ntqxx == 0) { ++i; continue; }   // :418
+    int ns = ctx().nslices;
+    if (ns == 0 && !tuned_lookup(sigc_slice_key(a0), &ns)) {
+      // the first task of a shape chooses the slice count on its own data
+      const int rc = sxcf_device(a0);
+      if (rc) return rc;
+      ++i;
+      continue;
+    }
+    // the group: following tasks of the same ngb and slice count within the scratch budget
+    std::vector<int> members;
+    std::vector<SxcfPlan> plans;
+    long long nslot = 0, ntiles = 0;
+    size_t bytes = 0;
+    for (int j = i; j < n; ++j) {
+      const qsgw_sxcf_args& a = t[j];
+      if (a.ns1 > a.ns2 || a.ntqxx == 0) {
+        if (members.empty()) continue;
+        break;
+      }
+      int nsj = ctx().nslices;
+      if (a.ngb != a0.ngb || (nsj == 0 && (!tuned_lookup(sigc_slice_key(a), &nsj) || nsj != ns))) break;
+      SxcfPlan pl;
+      int rc = sxcf_plan(a, kOzTileN, pl);
+      if (rc) return rc;
+      const long long sl = a.niw + 1 + static_cast<long long>(pl.recs.size());
+      const long long nt = static_cast<long long>(pl.tile_group.size());
+      const size_t add = OzSigcBatch::bytes_per(ns, a.ngb, a.ngb, sl, nt) +
+                         static_cast<size_t>(a.ngb) * pl.ncol * sizeof(double2);
+      if (!members.empty() && bytes + add > kSigcBatchBytes) break;
+      members.push_back(j);
+      plans.push_back(std::move(pl));
+      nslot += sl;
+      ntiles += nt;
+      bytes += add;
+    }
+    const int ng = static_cast<int>(members.size());
+    if (static_cast<int>(g_sb_wg.size()) < ng) {
+      g_sb_wg.resize(ng); g_sb_w3.resize(ng); g_sb_cz.resize(ng);
+    }
+    OzSigcBatch batch;
+    int rc = batch.reserve(ns, a0.ngb, a0.ngb, a0.ngb, nslot, ntiles);
+    if (rc) return rc;
+    for (int g = 0; g < ng; ++g) {
+      SigcSplitArgs sa;
+      rc = sxcf_bind(t[members[g]], plans[g], SxcfBufs{&g_sb_wg[g], &g_sb_w3[g], &g_sb_cz[g], &g_sc_wi, &g_sc_wr}, sa);
+      if (rc) return rc;
+      if ((rc = batch.add(sa, s))) return rc;
+    }
+    if ((rc = batch.launch(s))) return rc;
+    for (int g = 0; g < ng; ++g)
+      if ((rc = sxcf_finish(t[members[g]], g_sb_cz[g].as<double2>()))) return rc;
+    i = members.back() + 1;
+  }
   return QSGW_OK;
 }
 
@@ -475,6 +598,21 @@ extern "C" int qsgw_sxcf_correlation_d(const qsgw_sxcf_args* args) {
                (reinterpret_cast<uintptr_t>(args->zsec) & 15) == 0,
            "sxcf: complex arrays must be 16-byte aligned");
   return sxcf_device(*args);
+}
+
+extern "C" int qsgw_sxcf_correlation_batch_d(const qsgw_sxcf_args* tasks, int ntask) {
+  int rc = require_init();
+  if (rc) return rc;
+  QSGW_ARG(ntask >= 0 && (tasks || ntask == 0), "sxcf batch: %d tasks at %p", ntask, static_cast<const void*>(tasks));
+  for (int i = 0; i < ntask; ++i) {
+    rc = sxcf_check(&tasks[i]);
+    if (rc) return rc;
+    const qsgw_sxcf_args* a = &tasks[i];
+    QSGW_ARG((reinterpret_cast<uintptr_t>(a->zmel) & 15) == 0 && (reinterpret_cast<uintptr_t>(a->wc_imag) & 15) == 0 &&
+                 (reinterpret_cast<uintptr_t>(a->wc_real) & 15) == 0 && (reinterpret_cast<uintptr_t>(a->zsec) & 15) == 0,
+             "sxcf batch: task %d: complex arrays must be 16-byte aligned", i);
+  }
+  return sxcf_batch_device(tasks, ntask);
 }
 
 extern "C" int qsgw_sxcf_correlation(const qsgw_sxcf_args* args) {

@@ -97,6 +97,7 @@ _SIGS = {
     "qsgw_wvi_llw_d": [c_vp, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_int, c_vp, c_int],
     "qsgw_sxcf_correlation": [ctypes.POINTER(SxcfArgs)],
     "qsgw_sxcf_correlation_d": [ctypes.POINTER(SxcfArgs)],
+    "qsgw_sxcf_correlation_batch_d": [ctypes.POINTER(SxcfArgs), c_int],
     "qsgw_sxcf_wgtim_d": [c_vp, c_int, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_dbl, c_dbl,
                           c_dbl, c_vp, c_vp, c_vp],
     "qsgw_sxcf_exchange_d": [c_vp, c_int, c_vp, c_int, c_int, c_int, c_int, c_vp, c_vp, c_int, c_int, c_dbl,
@@ -418,10 +419,10 @@ def wvi_llw(zxqi, nspin, vcousq, m2e, is_x0_m_basis, is_wc_m_basis, iq, nblochpm
 
 
 # ---------------------------------------------------------------- Sigma_c
-def sxcf_correlation(zsec, zmel, ns1, ns2, ns2r, nwxi, nwx, ntqxx, wc_imag, wc_real,
-                     omega, ekc, nctot, ef, esmr, wkkr, ua, freqx, wwx, expa, freq_r,
-                     keepwv=False, nblochpmx=None, device=False, ngb=None, ntq=None):
-    """get_correlation_block (m_sxcf_gemm.f90:407-612) for one task; zsec updated in place."""
+def _sxcf_args(zsec, zmel, ns1, ns2, ns2r, nwxi, nwx, ntqxx, wc_imag, wc_real,
+               omega, ekc, nctot, ef, esmr, wkkr, ua, freqx, wwx, expa, freq_r,
+               keepwv=False, nblochpmx=None, device=False, ngb=None, ntq=None):
+    """(SxcfArgs, arrays to keep alive, zsec) of one task."""
     tabs = dict(omega=_f64(omega), ekc=_f64(ekc), freqx=_f64(freqx), wwx=_f64(wwx),
                 expa=_f64(expa), freq_r=_f64(freq_r))
     if device:
@@ -437,9 +438,30 @@ def sxcf_correlation(zsec, zmel, ns1, ns2, ns2r, nwxi, nwx, ntqxx, wc_imag, wc_r
                  omega=_p(tabs['omega']), ekc=_p(tabs['ekc']), freqx=_p(tabs['freqx']),
                  wwx=_p(tabs['wwx']), expa=_p(tabs['expa']), freq_r=_p(tabs['freq_r']),
                  zmel=_p(zmel), wc_imag=_p(wc_imag), wc_real=_p(wc_real), zsec=_p(zsec))
+    return a, (tabs, zmel, wc_imag, wc_real), zsec
+
+
+def sxcf_correlation(zsec, zmel, ns1, ns2, ns2r, nwxi, nwx, ntqxx, wc_imag, wc_real,
+                     omega, ekc, nctot, ef, esmr, wkkr, ua, freqx, wwx, expa, freq_r,
+                     keepwv=False, nblochpmx=None, device=False, ngb=None, ntq=None):
+    """get_correlation_block (m_sxcf_gemm.f90:407-612) for one task; zsec updated in place."""
+    a, keep, zsec = _sxcf_args(zsec, zmel, ns1, ns2, ns2r, nwxi, nwx, ntqxx, wc_imag, wc_real, omega, ekc, nctot,
+                               ef, esmr, wkkr, ua, freqx, wwx, expa, freq_r, keepwv, nblochpmx, device, ngb, ntq)
     f = load().qsgw_sxcf_correlation_d if device else load().qsgw_sxcf_correlation
     _chk(f(ctypes.byref(a)))
     return zsec
+
+
+def sxcf_correlation_batch_d(tasks):
+    """qsgw_sxcf_correlation_batch_d: ``tasks`` is a list of keyword dicts of
+    sxcf_correlation (device arrays, ngb and ntq given); the same result as
+    calling sxcf_correlation(..., device=True) on each in order."""
+    built = [_sxcf_args(**dict(t, device=True)) for t in tasks]
+    arr = (SxcfArgs * len(built))()
+    for i, (a, _, _) in enumerate(built):
+        arr[i] = a
+    _chk(load().qsgw_sxcf_correlation_batch_d(arr, len(built)))
+    return [z for _, _, z in built]
 
 
 def sxcf_wgtim_d(out, niw, ns1, ns2, ntqxx, nctot, omega, ekc, esmr, wkkr, ua, freqx, wwx, expa):

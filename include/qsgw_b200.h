@@ -262,6 +262,16 @@ typedef struct qsgw_sxcf_args {
 int qsgw_sxcf_correlation(const qsgw_sxcf_args *args);
 /* zmel, wc_imag, wc_real, zsec are device pointers; the tables stay host. */
 int qsgw_sxcf_correlation_d(const qsgw_sxcf_args *args);
+/* ntask tasks (device pointers, as qsgw_sxcf_correlation_d): the same result
+ * as calling qsgw_sxcf_correlation_d on tasks[0], tasks[1], ... in order
+ * (tasks may share zsec; it accumulates in that order).  It replaces the
+ * loop over (irot, ip, isp, icount) of sxcf_scz_correlation
+ * (m_sxcf_gemm.f90:369-384).  With QSGW_PREC_SPLIT_I8, consecutive tasks of
+ * equal ngb and slice count share one launch of the int8 contraction (up to
+ * 8 GiB of slice scratch per launch; the first task of a shape whose slice
+ * count is automatic runs alone to choose it); every other precision runs
+ * the tasks one by one. */
+int qsgw_sxcf_correlation_batch_d(const qsgw_sxcf_args *tasks, int ntask);
 
 /* Imaginary-axis weights wgtim(0:niw, ns1:ns2, ntqxx), FP64 on the GPU
  * (m_sxcf_gemm.f90:432-458, npm = 1).  wgtim_d: device (niw+1, nm, ntqxx). */
