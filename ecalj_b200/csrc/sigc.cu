@@ -452,9 +452,9 @@ static int sxcf_i8_slices(const qsgw_sxcf_args& a, const SigcSplitArgs& sa, int*
   return QSGW_OK;
 }
 
-int sxcf_device(const qsgw_sxcf_args& a) {
+// steps 1-3 of one non-empty task: czmelwc into sa.out
+static int sxcf_contract(const qsgw_sxcf_args& a, SigcSplitArgs& sa) {
   cudaStream_t s = ctx().stream;
-  if (a.ns1 > a.ns2 || a.ntqxx == 0) return QSGW_OK;   // :418
   const bool split = ctx().prec_mode != QSGW_PREC_FP64;
   const bool i8 = ctx().prec_mode == QSGW_PREC_SPLIT_I8;
   // column tile of the int8 / split-FP16 / FP64 kernel
@@ -462,7 +462,6 @@ int sxcf_device(const qsgw_sxcf_args& a) {
   SxcfPlan pl;
   int rc = sxcf_plan(a, tilew, pl);
   if (rc) return rc;
-  SigcSplitArgs sa;
   rc = sxcf_bind(a, pl, SxcfBufs{&g_sc_wg, &g_sc_w3, &g_sc_cz, &g_sc_wi, &g_sc_wr}, sa);
   if (rc) return rc;
   if (i8) {
@@ -502,7 +501,27 @@ int sxcf_device(const qsgw_sxcf_args& a) {
     p.C = sa.out; p.ldc = a.ngb; p.beta_zero = 1;
     rc = zgemm_seg_launch(p, static_cast<int>(sa.tile_group.size()), s);
   }
-  if (rc) return rc;
+  return rc;
+}
+
+int sxcf_device(const qsgw_sxcf_args& a) {
+  if (a.ns1 > a.ns2 || a.ntqxx == 0) return QSGW_OK;   // :418
+  SigcSplitArgs sa;
+  int rc;
+  if (ctx().prec_mode == QSGW_PREC_SPLIT_F16 && !sigc_kind_fixed()) {
+    // the split-FP16 kernel (64 x 128 tiles, CTA pairs, 64 x 256 tiles): timed once per shape
+    // on this call's data when tuning is on, else the 64 x 256 one
+    char key[200];
+    std::snprintf(key, sizeof(key), "sigc_f16 kernel ngb=%d nm=%d ntq=%d niw=%d", a.ngb, a.ns2 - a.ns1 + 1,
+                  a.ntqxx, a.niw);
+    int kind = 2;
+    bool tried = false;
+    rc = tuned_choice(key, {0, 1, 2}, 2, [&](int k) { sigc_kind_use(k); return sxcf_contract(a, sa); },
+                      ctx().stream, &kind, &tried);
+    if (rc) return rc;
+    sigc_kind_use(kind);
+  }
+  if ((rc = sxcf_contract(a, sa))) return rc;
   return sxcf_finish(a, sa.out);
 }
 

@@ -606,12 +606,15 @@ static int launch_mode(const CUtensorMap& ma, const CUtensorMap& ms, const Param
 }
 
 // Sigma_c kernel: 0 = one CTA per 64 x 128 tile, 1 = CTA pairs over 128-column tiles, 2 = one
-// CTA per 64 x 256 tile (default, the fastest on B200); QSGW_SIGC_KERNEL=<n> sets it at load time
+// CTA per 64 x 256 tile (default, the fastest on B200).  QSGW_SIGC_KERNEL=<n> at load time or
+// qsgw_set_sigc_kernel fixes it; otherwise the autotuner may pick it per shape (sigc_kind_use).
 static int g_sigc_kind = -1;
+static bool g_sigc_fixed = false;
 static int sigc_kind() {
   if (g_sigc_kind < 0) {
     const char* e = std::getenv("QSGW_SIGC_KERNEL");
-    g_sigc_kind = (e && (e[0] == '0' || e[0] == '1' || e[0] == '2') && e[1] == '\0') ? e[0] - '0' : 2;
+    g_sigc_fixed = e && (e[0] == '0' || e[0] == '1' || e[0] == '2') && e[1] == '\0';
+    g_sigc_kind = g_sigc_fixed ? e[0] - '0' : 2;
   }
   return g_sigc_kind;
 }
@@ -851,6 +854,14 @@ int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s) {
 }
 
 int sigc_split_tile_width() { return sigc_kind() == 2 ? NW : NC; }
+bool sigc_kind_fixed() {
+  sigc_kind();
+  return g_sigc_fixed;
+}
+void sigc_kind_use(int kind) {
+  sigc_kind();
+  g_sigc_kind = kind;
+}
 
 }  // namespace qsgw
 
@@ -859,6 +870,8 @@ extern "C" int qsgw_set_sigc_kernel(int kind) {
     qsgw::set_error("qsgw_set_sigc_kernel: %d (0 = 64 x 128 tiles, 1 = CTA pairs, 2 = 64 x 256 tiles)", kind);
     return QSGW_ERR_ARG;
   }
+  qsgw::tc::sigc_kind();
   qsgw::tc::g_sigc_kind = kind;
+  qsgw::tc::g_sigc_fixed = true;
   return QSGW_OK;
 }

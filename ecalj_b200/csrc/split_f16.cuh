@@ -33,5 +33,10 @@ struct SigcSplitArgs {
 int sigc_split_f16(const SigcSplitArgs& a, cudaStream_t s);
 // columns per tile of the selected split Sigma_c kernel (the tables are cut to it)
 int sigc_split_tile_width();
+// The split-FP16 Sigma_c kernel kind (0, 1, 2 as qsgw_set_sigc_kernel): whether the caller fixed
+// it (qsgw_set_sigc_kernel or QSGW_SIGC_KERNEL), and the kind the following calls use (the
+// autotuner's choice for their shape otherwise).
+bool sigc_kind_fixed();
+void sigc_kind_use(int kind);
 
 }  // namespace qsgw
