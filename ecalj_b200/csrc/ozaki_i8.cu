@@ -86,6 +86,25 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t d
       " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n"
       ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC_I8), "r"(accumulate));
 }
+// The MMA above preceded by a non-blocking test (mbarrier.test_wait, acquire) of phase `parity` of
+// the barrier at shared address `bar`, whose answer (1 = complete) is read only after the MMA has
+// been issued.  The issuing thread blocks in every MMA issue until the tensor core takes it, so a
+// wait between two K chunks leaves the tensor core idle; the test's latency is spent inside the
+// MMA issue instead.
+__device__ __forceinline__ uint32_t umma_i8_then_test(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate,
+                                                      uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p, q;\n"
+      " mbarrier.test_wait.parity.shared::cta.b64 q, [%5], %6;\n"
+      " setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%1], %2, %3, %7, p;\n"
+      " selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(ok)
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(accumulate), "r"(bar), "r"(parity), "r"(IDESC_I8)
+      : "memory");
+  return ok;
+}
 // The same MMA with the A operand kept in the tensor core's collector buffer: FILL loads it and
 // keeps it, USE reads the kept copy (same A descriptor), LAST reads it and releases the buffer.
 enum { A_FILL = 0, A_USE = 1, A_LAST = 2 };
@@ -110,10 +129,14 @@ __device__ __forceinline__ void umma_i8_ca(uint32_t tmem_d, uint64_t da, uint64_
 
 // The slice products of one K step: for each A slice pa (one shared-memory read through the
 // collector buffer), the B slices qb with pa + qb < NS into the accumulator of level pa + qb.
-// The first product into each level (pa == 0) starts it when `start` is set.
+// The first product into each level (pa == 0) starts it when `start` is set.  With test_bar != 0
+// the last product (pa = NS - 1, no collector) also tests phase test_parity of that barrier
+// (umma_i8_then_test); the answer is returned (0 otherwise).
 template <int NS>
-__device__ __forceinline__ void slice_products(uint32_t tmem, uint64_t da0, uint64_t db0, uint32_t a_step,
-                                               uint32_t b_step, bool start) {
+__device__ __forceinline__ uint32_t slice_products(uint32_t tmem, uint64_t da0, uint64_t db0, uint32_t a_step,
+                                                   uint32_t b_step, bool start, uint32_t test_bar = 0,
+                                                   uint32_t test_parity = 0) {
+  uint32_t ready = 0;
 #pragma unroll
   for (int pa = 0; pa < NS; ++pa) {
     const uint64_t da = da0 + pa * a_step;
@@ -122,12 +145,16 @@ __device__ __forceinline__ void slice_products(uint32_t tmem, uint64_t da0, uint
       const uint64_t db = db0 + qb * b_step;
       const uint32_t d = tmem + static_cast<uint32_t>((pa + qb) * kOzTileN);
       const uint32_t acc = (start && pa == 0) ? 0u : 1u;
-      if (NS - pa == 1) umma_i8(d, da, db, acc);
+      if (NS - pa == 1) {
+        if (test_bar) ready = umma_i8_then_test(d, da, db, acc, test_bar, test_parity);
+        else umma_i8(d, da, db, acc);
+      }
       else if (qb == 0) umma_i8_ca<A_FILL>(d, da, db, acc);
       else if (qb == NS - pa - 1) umma_i8_ca<A_LAST>(d, da, db, acc);
       else umma_i8_ca<A_USE>(d, da, db, acc);
     }
   }
+  return ready;
 }
 
 // 32 lanes x 4 consecutive 32-bit TMEM columns
@@ -281,16 +308,20 @@ __global__ void __launch_bounds__(THREADS, 1)
       // ---------------- MMA issuer: NS level accumulators, one accumulation period per segment
       const uint64_t dA0 = sw64_desc(smem_u32(sA)), dB0 = sw64_desc(smem_u32(sB));
       int seg = 0, cin = 0, st = 0, ph = 0;
+      uint32_t ready = 0;                            // the chunk's stage was seen full by the last test
       for (int c = 0; c < nchunk && !*abort_flag; ++c) {
         const bool first = cin == 0, last = cin == p.cps - 1;
         if (first && seg >= 1 && !mbar_wait(accempty, (seg - 1) & 1, abort_flag)) break;
-        if (!mbar_wait(&full[st], ph, abort_flag)) break;
+        if (!ready && !mbar_wait(&full[st], ph, abort_flag)) break;
         tc_fence_after();
+        // the next chunk's stage is tested during this chunk's last MMA
+        const uint32_t nbar = c + 1 < nchunk ? smem_u32(&full[st + 1 == NST ? 0 : st + 1]) : 0u;
+        const uint32_t npar = st + 1 == NST ? (ph ^ 1) : ph;
 #pragma unroll
         for (int kk = 0; kk < K8 / 32; ++kk)          // 32 int8 = 32 B along K = 2 descriptor units
-          slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((st * NS * SLA8) >> 4) + 2 * kk,
-                             dB0 + static_cast<uint32_t>((st * NS * SLB8) >> 4) + 2 * kk, SLA8 >> 4, SLB8 >> 4,
-                             first && kk == 0);
+          ready = slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((st * NS * SLA8) >> 4) + 2 * kk,
+                                     dB0 + static_cast<uint32_t>((st * NS * SLB8) >> 4) + 2 * kk, SLA8 >> 4,
+                                     SLB8 >> 4, first && kk == 0, kk == K8 / 32 - 1 ? nbar : 0u, npar);
         umma_commit(&empty[st]);
         if (last) umma_commit(accfull);
         if (++st == NST) { st = 0; ph ^= 1; }
@@ -464,17 +495,20 @@ __global__ void __launch_bounds__(THREADS, 1)
     // ---------------- MMA issuer: periods of at most PER chunks (exact INT32 levels)
     const uint64_t dA0 = sw64_desc(smem_u32(sA)), dB0 = sw64_desc(smem_u32(sB));
     int st = 0, ph = 0, cin = 0, per = 0;
+    uint32_t ready = 0;                              // the chunk's stage was seen converted by the last test
     for (int c = 0; c < nchunk && !*abort_flag; ++c) {
       const bool first = cin == 0;
       const bool last = cin == PER - 1 || c == nchunk - 1;
       if (first && per >= 1 && !mbar_wait(accempty, (per - 1) & 1, abort_flag)) break;
-      if (!mbar_wait(&cfull[st], ph, abort_flag)) break;
+      if (!ready && !mbar_wait(&cfull[st], ph, abort_flag)) break;
       tc_fence_after();
+      const uint32_t nbar = c + 1 < nchunk ? smem_u32(&cfull[st + 1 == NST ? 0 : st + 1]) : 0u;
+      const uint32_t npar = st + 1 == NST ? (ph ^ 1) : ph;
 #pragma unroll
       for (int kk = 0; kk < K8 / 32; ++kk)
-        slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((st * NS * SLA8) >> 4) + 2 * kk,
-                           dB0 + static_cast<uint32_t>((st * NS * SLB8) >> 4) + 2 * kk, SLA8 >> 4, SLB8 >> 4,
-                           first && kk == 0);
+        ready = slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((st * NS * SLA8) >> 4) + 2 * kk,
+                                   dB0 + static_cast<uint32_t>((st * NS * SLB8) >> 4) + 2 * kk, SLA8 >> 4,
+                                   SLB8 >> 4, first && kk == 0, kk == K8 / 32 - 1 ? nbar : 0u, npar);
       umma_commit(&empty[st]);
       if (last) umma_commit(accfull);
       if (++st == NST) { st = 0; ph ^= 1; }
