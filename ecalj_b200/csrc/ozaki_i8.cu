@@ -54,6 +54,7 @@ constexpr int BN = kOzTileN;             // accumulator columns (UMMA N)
 constexpr int K8 = 64;                   // int8 K per chunk: one 64-byte swizzled row
 constexpr int THREADS = 576;
 constexpr int NDW = 16;                  // drain warps 2..17
+constexpr int NCONV = 12;                // chi0: the drain warps that also convert (warp mod 4 != 1)
 constexpr int SLA8 = BM * K8;         // 8 KB: one slice of the A' tile of a stage
 constexpr int SLB8 = BN * K8;         // 8 KB: one slice of the B tile of a stage
 constexpr int STAGE_BUDGET = 192 * 1024;
@@ -181,23 +182,25 @@ template <int NS>
 __host__ __device__ constexpr double slice_unit() { return static_cast<double>(1LL << (6 + 7 * (NS - 1))); }
 
 // NS slices of x / mu, given scale = slice_unit<NS>() / mu (a power of two, so x * scale is exact):
-// V = rint(x * scale) (|V| <= 64 * 128^(NS-1)) written in base 128 from the bottom with digits
-// d = sign(V) r, r = |V| mod 128 taken in [-63, 64]; the top digit holds the rest.  Every digit
-// lies in [-64, 64] (one int8), negation commutes with the slicing, and the digits rebuild
-// x to mu 2^-(7 NS).  One FP64 multiply and round, then integer work only.
+// V = rint(x * scale) (|V| <= 64 * 128^(NS-1) <= 2^27, an int32) written in base 128 from the
+// bottom with digits d = sign(V) r, r = |V| mod 128 taken in [-63, 64]; the top digit holds the
+// rest.  Every digit lies in [-64, 64] (one int8), negation commutes with the slicing, and the
+// digits rebuild x to mu 2^-(7 NS).  One FP64 multiply and round, then 32-bit integer work
+// (about seven operations a digit: these kernels are bound by it, not by HBM).
 template <int NS>
 __device__ __forceinline__ void slice(double x, double scale, int (&s)[NS]) {
-  long long v = __double2ll_rn(x * scale);
+  static_assert(6 + 7 * (NS - 1) <= 30, "V must fit an int32");
+  int v = __double2int_rn(x * scale);
 #pragma unroll
   for (int i = NS - 1; i >= 1; --i) {
-    const long long u = v < 0 ? -v : v;
-    int r = static_cast<int>(u & 127);
-    if (r > 64) r -= 128;
-    const int d = v < 0 ? -r : r;
+    const int sg = v >> 31;                  // 0 or -1
+    const int u = (v ^ sg) - sg;             // |v|
+    const int r = ((u + 63) & 127) - 63;     // |v| mod 128 in [-63, 64]
+    const int d = (r ^ sg) - sg;             // sign(v) r
     s[i] = d;
-    v = (v - d) >> 7;                      // exact: v - d is a multiple of 128
+    v = (v - d) >> 7;                        // exact: v - d is a multiple of 128
   }
-  s[0] = static_cast<int>(v);
+  s[0] = v;
 }
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
   return (static_cast<uint32_t>(a) & 0xFFu) | ((static_cast<uint32_t>(b) & 0xFFu) << 8) |
@@ -458,7 +461,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   const int nper = (nchunk + PER - 1) / PER;
 
   if (tid == 0) {
-    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&cfull[i], NDW); mbar_init(&empty[i], 1); }
+    for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&cfull[i], NCONV); mbar_init(&empty[i], 1); }
     mbar_init(accfull, 1);
     mbar_init(accempty, NDW);
     mbar_init(done, 1);
@@ -518,8 +521,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     mbar_drain(done, 0);
   } else if (warp >= 2) {
     // ---------------- converters + drain (warps 2..17)
+    // The converters are the 12 warps off the MMA warp's sub-partition (warp mod 4 != 1): the
+    // MMA thread blocks in every MMA issue, so issue slots taken from it idle the tensor core.
+    // The other four (they own TMEM lanes 32..63) only drain.
     const int dw = warp - 2;
-    const int ct = tid - 64;                            // 0..511
+    const bool conv = (warp & 3) != 1;
+    const int ct = (dw - (dw + 1) / 4) * 32 + lane;      // 0..383 over the converter warps
     const int quad = warp & 3;
     const int c_lo = (dw >> 2) * 32;
     const int row = quad * 32 + lane;
@@ -530,19 +537,21 @@ __global__ void __launch_bounds__(THREADS, 1)
     bool ok = true;
     int st = 0, ph = 0, cin = 0, per = 0;
     for (int c = 0; c < nchunk; ++c) {
-      if (!mbar_wait_warp(&full[st], ph, abort_flag)) { ok = false; break; }
-      // the (m, im) rows [-Im y, Re y] from the (m, re) rows [Re y, Im y]: same swizzled offsets
-      // (rows r and r + 64 share their 64-byte swizzle pattern)
-      for (int i = ct; i < NS * (HALF / 16); i += NDW * 32) {
-        const int q = i / (HALF / 16), j = i % (HALF / 16);
-        const uint4 v = *reinterpret_cast<const uint4*>(sA + (st * NS + q) * SLA8 + j * 16);
-        uint4 o;
-        o.x = rotate_pairs(v.x); o.y = rotate_pairs(v.y); o.z = rotate_pairs(v.z); o.w = rotate_pairs(v.w);
-        *reinterpret_cast<uint4*>(sA + (st * NS + q) * SLA8 + HALF + j * 16) = o;
+      if (conv) {
+        if (!mbar_wait_warp(&full[st], ph, abort_flag)) { ok = false; break; }
+        // the (m, im) rows [-Im y, Re y] from the (m, re) rows [Re y, Im y]: same swizzled offsets
+        // (rows r and r + 64 share their 64-byte swizzle pattern)
+        for (int i = ct; i < NS * (HALF / 16); i += NCONV * 32) {
+          const int q = i / (HALF / 16), j = i % (HALF / 16);
+          const uint4 v = *reinterpret_cast<const uint4*>(sA + (st * NS + q) * SLA8 + j * 16);
+          uint4 o;
+          o.x = rotate_pairs(v.x); o.y = rotate_pairs(v.y); o.z = rotate_pairs(v.z); o.w = rotate_pairs(v.w);
+          *reinterpret_cast<uint4*>(sA + (st * NS + q) * SLA8 + HALF + j * 16) = o;
+        }
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&cfull[st]);
       }
-      fence_async_smem();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&cfull[st]);
       if (++st == NST) { st = 0; ph ^= 1; }
       const bool last = cin == PER - 1 || c == nchunk - 1;
       if (!last) { ++cin; continue; }
