@@ -1,9 +1,11 @@
-// Complex FP64 GEMM engine on the FP64 tensor pipe (mma.sync m8n8k4 f64,
+// Complex FP64 GEMM engine on the FP64 tensor pipe (mma.sync m16n8k8 f64,
 // "DMMA"), shared by chi0 (x0gemm), W (basis changes, Gauss-Jordan updates)
 // and Sigma_c.  One CTA computes a 64x64 complex tile with 4 warps (each
-// 32x32 = 4x4 m8n8 fragments, re and im accumulators); operands stream
+// 32x32 = 2x4 m16n8 fragments, re and im accumulators); operands stream
 // through a 3-stage cp.async pipeline in shared memory laid out [k][row]
-// with a pitch of 66 complex (conflict-free fragment loads).
+// with a pitch of 66 complex (conflict-free fragment loads).  The m16n8k8
+// shape does 4x the work of the m8n8k4 one per instruction with the same
+// shared-memory reads per multiply-add.
 //
 // Three problem modes share the main loop:
 //   ZM_GEMM  C = alpha op(A) op(B) + beta C, batched, optional split-K.
@@ -67,10 +69,14 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+// D(16x8) += A(16x8) B(8x8), FP64.  Lane (g = lane / 4, t = lane % 4) holds A(g, t), A(g+8, t),
+// A(g, t+4), A(g+8, t+4); B(t, g), B(t+4, g); D(g, 2t), D(g, 2t+1), D(g+8, 2t), D(g+8, 2t+1).
+__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[4], double b0, double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
 }
 
 // Decode the t-th lower-triangle tile (tm >= tn).
@@ -195,14 +201,13 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_f64_kernel(const ZParams 
     }
   };
 
-  double accr[4][4][2], acci[4][4][2];
+  double accr[2][4][4], acci[2][4][4];       // [m16 block][n8 block][fragment element]
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      accr[i][j][0] = accr[i][j][1] = 0.0;
-      acci[i][j][0] = acci[i][j][1] = 0.0;
-    }
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) accr[i][j][e] = acci[i][j][e] = 0.0;
 
   const int nloc = ch1 - ch0;
 #pragma unroll
@@ -215,35 +220,41 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_f64_kernel(const ZParams 
     __syncthreads();
     const int st = c % ZG_STAGES;
 #pragma unroll
-    for (int k4 = 0; k4 < ZG_BK / 4; ++k4) {
-      const int k = k4 * 4 + t;
-      double ar[4], ai[4], nai[4], br[4], bi[4];
+    for (int k8 = 0; k8 < ZG_BK / 8; ++k8) {
+      const int ka = k8 * 8 + t, kb = ka + 4;       // the lane's two k of the step
+      double ar[2][4], ai[2][4], nai[2][4], br[4][2], bi[4][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const double2 v = sm.a[st][k][wm * 32 + i * 8 + g];
-        ar[i] = v.x;
-        ai[i] = p.a_conj ? -v.y : v.y;
-        nai[i] = -ai[i];
+      for (int i = 0; i < 2; ++i) {
+        const int r0 = wm * 32 + i * 16 + g;
+        const double2 v[4] = {sm.a[st][ka][r0], sm.a[st][ka][r0 + 8], sm.a[st][kb][r0], sm.a[st][kb][r0 + 8]};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          ar[i][e] = v[e].x;
+          ai[i][e] = p.a_conj ? -v[e].y : v[e].y;
+          nai[i][e] = -ai[i][e];
+        }
       }
-      double sk = 1.0;
-      if (MODE == ZM_CHI0) sk = sm.sk[st][k];
+      double ska = 1.0, skb = 1.0;
+      if (MODE == ZM_CHI0) { ska = sm.sk[st][ka]; skb = sm.sk[st][kb]; }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int nn = wn * 32 + j * 8 + g;
-        const double2 v = sm.b[st][k][nn];
-        double s = sk;
-        if (MODE == ZM_SEG) s = sm.sn[st][nn];
-        br[j] = v.x * s;
-        bi[j] = (p.b_conj ? -v.y : v.y) * s;
+        const double2 va = sm.b[st][ka][nn], vb = sm.b[st][kb][nn];
+        double sa = ska, sb = skb;
+        if (MODE == ZM_SEG) sa = sb = sm.sn[st][nn];
+        br[j][0] = va.x * sa;
+        br[j][1] = vb.x * sb;
+        bi[j][0] = (p.b_conj ? -va.y : va.y) * sa;
+        bi[j][1] = (p.b_conj ? -vb.y : vb.y) * sb;
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          dmma(accr[i][j][0], accr[i][j][1], ar[i], br[j]);
-          dmma(accr[i][j][0], accr[i][j][1], nai[i], bi[j]);
-          dmma(acci[i][j][0], acci[i][j][1], ar[i], bi[j]);
-          dmma(acci[i][j][0], acci[i][j][1], ai[i], br[j]);
+          dmma16(accr[i][j], ar[i], br[j][0], br[j][1]);
+          dmma16(accr[i][j], nai[i], bi[j][0], bi[j][1]);
+          dmma16(acci[i][j], ar[i], bi[j][0], bi[j][1]);
+          dmma16(acci[i][j], ai[i], br[j][0], br[j][1]);
         }
     }
     const int cn = c + ZG_STAGES - 1;
@@ -255,14 +266,16 @@ __global__ void __launch_bounds__(ZG_THREADS, 2) zgemm_f64_kernel(const ZParams 
 
   // ---- epilogue ----
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int row = m0 + wm * 32 + i * 8 + g;
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+    const int row = m0 + wm * 32 + i * 16 + h * 8 + g;
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int cl = wn * 32 + j * 8 + 2 * t + e;
-        double vr = accr[i][j][e], vi = acci[i][j][e];
+        double vr = accr[i][j][2 * h + e], vi = acci[i][j][2 * h + e];
         if (MODE == ZM_GEMM) {
           const int col = n0 + cl;
           if (row >= p.M || col >= p.N) continue;
