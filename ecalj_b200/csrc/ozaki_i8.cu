@@ -185,26 +185,27 @@ __host__ __device__ constexpr double slice_unit() { return static_cast<double>(1
 // V = rint(x * scale) (|V| <= 64 * 128^(NS-1) <= 2^27, an int32) written in base 128 from the
 // bottom with digits d = sign(V) r, r = |V| mod 128 taken in [-63, 64]; the top digit holds the
 // rest.  Every digit lies in [-64, 64] (one int8), negation commutes with the slicing, and the
-// digits rebuild x to mu 2^-(7 NS).  One FP64 multiply and round, then 32-bit integer work
-// (about seven operations a digit: these kernels are bound by it, not by HBM).
+// digits rebuild x to mu 2^-(7 NS).  One FP64 multiply and round, then 32-bit integer work:
+// the rule above is q = v / 128 rounded to nearest with ties toward zero, d = v - 128 q, i.e.
+// q = (v + 63 + [v < 0]) >> 7 (arithmetic shift), four operations a digit (these kernels are
+// bound by the integer pipe, not by HBM).
 template <int NS>
 __device__ __forceinline__ void slice(double x, double scale, int (&s)[NS]) {
   static_assert(6 + 7 * (NS - 1) <= 30, "V must fit an int32");
   int v = __double2int_rn(x * scale);
 #pragma unroll
   for (int i = NS - 1; i >= 1; --i) {
-    const int sg = v >> 31;                  // 0 or -1
-    const int u = (v ^ sg) - sg;             // |v|
-    const int r = ((u + 63) & 127) - 63;     // |v| mod 128 in [-63, 64]
-    const int d = (r ^ sg) - sg;             // sign(v) r
-    s[i] = d;
-    v = (v - d) >> 7;                        // exact: v - d is a multiple of 128
+    const int q = (v + 63 - (v >> 31)) >> 7;
+    s[i] = v - (q << 7);
+    v = q;
   }
   s[0] = v;
 }
+// the low bytes of a, b, c, d (two's complement int8) as one word, a lowest
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
-  return (static_cast<uint32_t>(a) & 0xFFu) | ((static_cast<uint32_t>(b) & 0xFFu) << 8) |
-         ((static_cast<uint32_t>(c) & 0xFFu) << 16) | ((static_cast<uint32_t>(d) & 0xFFu) << 24);
+  const uint32_t ab = __byte_perm(static_cast<uint32_t>(a), static_cast<uint32_t>(b), 0x0040);
+  const uint32_t cd = __byte_perm(static_cast<uint32_t>(c), static_cast<uint32_t>(d), 0x0040);
+  return __byte_perm(ab, cd, 0x5410);
 }
 // (re, im) byte pairs -> (-im, re): the (m, im) row of A' from its (m, re) row
 __device__ __forceinline__ uint32_t rotate_pairs(uint32_t w) {
@@ -763,10 +764,12 @@ __device__ __forceinline__ void y_tile_pack(int8_t (*tile)[64][80], int mm, int 
 #pragma unroll
   for (int jp = 0; jp < 4; ++jp) {
     int r0[NS], i0[NS], r1[NS], i1[NS];
-    slice<NS>(f[2 * jp] * zv[2 * jp].x, scale, r0);
-    slice<NS>(f[2 * jp] * zv[2 * jp].y, scale, i0);
-    slice<NS>(f[2 * jp + 1] * zv[2 * jp + 1].x, scale, r1);
-    slice<NS>(f[2 * jp + 1] * zv[2 * jp + 1].y, scale, i1);
+    // (f z) scale with scale a power of two is z (f scale), rounded the same way
+    const double fs0 = f[2 * jp] * scale, fs1 = f[2 * jp + 1] * scale;
+    slice<NS>(zv[2 * jp].x, fs0, r0);
+    slice<NS>(zv[2 * jp].y, fs0, i0);
+    slice<NS>(zv[2 * jp + 1].x, fs1, r1);
+    slice<NS>(zv[2 * jp + 1].y, fs1, i1);
 #pragma unroll
     for (int q = 0; q < NS; ++q) w[q][jp] = pack4(r0[q], i0[q], r1[q], i1[q]);
   }
