@@ -393,8 +393,11 @@ static int sxcf_finish(const qsgw_sxcf_args& a, const double2* cz) {
   cudaStream_t s = ctx().stream;
   const long long kk = static_cast<long long>(a.ngb) * (a.ns2 - a.ns1 + 1);
   const double2* zmel = reinterpret_cast<const double2*>(a.zmel);
-  int rc = zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,
-                     make_double2(1, 0), reinterpret_cast<double2*>(a.zsec), a.ntq, 0, 1, s);
+  // a thin product (ntqxx x ntqxx over K = ngb nm): padded to 16 x 8 fragments instead of 64 x 64 tiles
+  int rc = a.ntqxx <= 64
+               ? zgemm_hn_thin(a.ntqxx, kk, cz, kk, zmel, kk, reinterpret_cast<double2*>(a.zsec), a.ntq, s)
+               : zgemm_f64(2, 0, a.ntqxx, a.ntqxx, static_cast<int>(kk), make_double2(1, 0), cz, kk, 0, zmel, kk, 0,
+                           make_double2(1, 0), reinterpret_cast<double2*>(a.zsec), a.ntq, 0, 1, s);
   if (rc) return rc;
   clamp_diag_kernel<<<(a.ntqxx + 127) / 128, 128, 0, s>>>(reinterpret_cast<double2*>(a.zsec), a.ntqxx, a.ntq);
   count_launch();

@@ -1,6 +1,8 @@
 // Host side of the FP64 complex GEMM engine and the ZGEMM entry points that
 // replace the reference's BLAS shim zmm_h / zmm_d (m_blas.f90:198-228,
 // 469-498).
+#include <algorithm>
+#include <type_traits>
 #include "zgemm_f64.cuh"
 
 namespace qsgw {
@@ -17,6 +19,124 @@ static int launch_kernel(const ZParams& p, dim3 grid, cudaStream_t s) {
   prof_end(pi, s);
   count_launch();
   QSGW_LAUNCH_CHECK("zgemm_f64_kernel");
+  return QSGW_OK;
+}
+
+// ---- thin A^H B: C(0:n, 0:n) += A^H B for complex A, B of K x n (column-major, leading dimensions
+// lda, ldb), n <= 64 and K large: the last contraction of Sigma_c, zsec += czmelwc^H zmel over
+// K = ngb (ns2 - ns1 + 1) (m_sxcf_gemm.f90:599).  The general engine's 64 x 64 tiles would run
+// 2.6x the needed DMMA work at n = 40; here n is padded only to 16 (rows) and 8 (columns).  A CTA
+// (4 warps) takes a K range; the MB x NB fragments (m16 x n8) of the output are dealt round-robin
+// to its warps, which share the staged operands; the CTA's partial sums go to C by FP64 atomics.
+constexpr int TH_BK = 16;                          // k per stage
+template <int MB>
+constexpr int thin_smem_bytes() { return 2 * 2 * TH_BK * (MB * 16 + 2) * static_cast<int>(sizeof(double2)); }
+template <int MB>
+__global__ void __launch_bounds__(128) zgemm_hn_thin_kernel(const double2* __restrict__ A, long long lda,
+                                                            const double2* __restrict__ B, long long ldb, int n,
+                                                            long long K, long long kper, double2* __restrict__ C,
+                                                            long long ldc) {
+  constexpr int NB = 2 * MB, NF = MB * NB, FPW = (NF + 3) / 4;
+  constexpr int R = MB * 16, PR = R + 2;           // padded rows of A^H (= columns of B); pitch
+  extern __shared__ __align__(16) unsigned char th_smem[];       // thin_smem_bytes<MB>()
+  double2 (*sa)[TH_BK][PR] = reinterpret_cast<double2 (*)[TH_BK][PR]>(th_smem);
+  double2 (*sb)[TH_BK][PR] = reinterpret_cast<double2 (*)[TH_BK][PR]>(th_smem + 2 * TH_BK * PR * sizeof(double2));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const long long k0 = blockIdx.x * kper, k1 = min(K, k0 + kper);
+  if (k0 >= k1) return;
+  const int nch = static_cast<int>((k1 - k0 + TH_BK - 1) / TH_BK);
+  auto load = [&](int c, int st) {
+#pragma unroll
+    for (int e = tid; e < TH_BK * R; e += 128) {
+      const int kk = e % TH_BK, r = e / TH_BK;
+      const long long k = k0 + static_cast<long long>(c) * TH_BK + kk;
+      const bool ok = r < n && k < k1;
+      cp_async16(&sa[st][kk][r], ok ? A + r * lda + k : A, ok);
+      cp_async16(&sb[st][kk][r], ok ? B + r * ldb + k : B, ok);
+    }
+  };
+  double accr[FPW][4], acci[FPW][4];
+#pragma unroll
+  for (int u = 0; u < FPW; ++u)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) accr[u][e] = acci[u][e] = 0.0;
+  load(0, 0);
+  cp_async_commit();
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) load(c + 1, (c + 1) & 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int st = c & 1;
+#pragma unroll
+    for (int k8 = 0; k8 < TH_BK / 8; ++k8) {
+      const int ka = k8 * 8 + t, kb = ka + 4;
+#pragma unroll
+      for (int u = 0; u < FPW; ++u) {
+        const int f = warp + 4 * u;
+        if (f >= NF) break;
+        const int i = f / NB, j = f % NB;
+        const int r0 = i * 16 + g, nn = j * 8 + g;
+        const double2 v[4] = {sa[st][ka][r0], sa[st][ka][r0 + 8], sa[st][kb][r0], sa[st][kb][r0 + 8]};
+        double ar[4], ai[4], nai[4];                 // a = conj(A(k, m))
+#pragma unroll
+        for (int e = 0; e < 4; ++e) { ar[e] = v[e].x; ai[e] = -v[e].y; nai[e] = v[e].y; }
+        const double2 b0 = sb[st][ka][nn], b1 = sb[st][kb][nn];
+        dmma16(accr[u], ar, b0.x, b1.x);
+        dmma16(accr[u], nai, b0.y, b1.y);
+        dmma16(acci[u], ar, b0.y, b1.y);
+        dmma16(acci[u], ai, b0.x, b1.x);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < FPW; ++u) {
+    const int f = warp + 4 * u;
+    if (f >= NF) break;
+    const int i = f / NB, j = f % NB;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int row = i * 16 + g + (e >= 2 ? 8 : 0), col = j * 8 + 2 * t + (e & 1);
+      if (row < n && col < n) {
+        double* d = reinterpret_cast<double*>(C + row + static_cast<long long>(col) * ldc);
+        atomicAdd(d, accr[u][e]);
+        atomicAdd(d + 1, acci[u][e]);
+      }
+    }
+  }
+}
+
+int zgemm_hn_thin(int n, long long K, const double2* A, long long lda, const double2* B, long long ldb, double2* C,
+                  long long ldc, cudaStream_t s) {
+  QSGW_ARG(n >= 1 && n <= 64 && K >= 0, "zgemm_hn_thin: n=%d (1..64), K=%lld", n, K);
+  if (K == 0) return QSGW_OK;
+  const long long nch = (K + TH_BK - 1) / TH_BK;
+  auto run = [&](auto mb) -> int {
+    constexpr int MB = decltype(mb)::value;
+    static uint64_t attr = 0;                       // one bit per device
+    int rc = smem_limit_once(reinterpret_cast<const void*>(zgemm_hn_thin_kernel<MB>), thin_smem_bytes<MB>(), attr);
+    if (rc) return rc;
+    // one wave: as many K ranges as CTAs fit on the GPU at once
+    int per_sm = 0;
+    QSGW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zgemm_hn_thin_kernel<MB>, 128,
+                                                            thin_smem_bytes<MB>()));
+    const long long nsplit = std::max<long long>(1, std::min<long long>(nch, std::max(per_sm, 1) * 1LL * ctx().sm_count));
+    const long long kper = ((nch + nsplit - 1) / nsplit) * TH_BK;
+    const unsigned grid = static_cast<unsigned>((K + kper - 1) / kper);
+    zgemm_hn_thin_kernel<MB><<<grid, 128, thin_smem_bytes<MB>(), s>>>(A, lda, B, ldb, n, K, kper, C, ldc);
+    return QSGW_OK;
+  };
+  const int pi = prof_begin("gemm_dmma", s);
+  int rc;
+  if (n <= 16) rc = run(std::integral_constant<int, 1>());
+  else if (n <= 32) rc = run(std::integral_constant<int, 2>());
+  else if (n <= 48) rc = run(std::integral_constant<int, 3>());
+  else rc = run(std::integral_constant<int, 4>());
+  if (rc) return rc;
+  prof_end(pi, s);
+  count_launch();
+  QSGW_LAUNCH_CHECK("zgemm_hn_thin_kernel");
   return QSGW_OK;
 }
 

@@ -326,6 +326,9 @@ int zgemm_f64(int opa, int opb, int m, int n, int k, double2 alpha,
               const double2* B, long long ldb, long long b_bs, double2 beta,
               double2* C, long long ldc, long long c_bs, int nbatch, cudaStream_t s);
 int zgemm_chi0_launch(ZParams p, int nbins, int herm, int splitk, cudaStream_t s);
+// C(0:n, 0:n) += A^H B for complex A, B of K x n (column-major), n <= 64, any K (FP64 atomics)
+int zgemm_hn_thin(int n, long long K, const double2* A, long long lda, const double2* B, long long ldb, double2* C,
+                  long long ldc, cudaStream_t s);
 int zgemm_seg_launch(ZParams p, int ncol_tiles, cudaStream_t s);
 // Batched inverses (wv.cu: Hermitian positive definite; zminv_piv.cu: general, partial pivoting).
 int zminv_hpd_batched(double2* A, int n, long long lda, long long a_bs, int nbatch, cudaStream_t s);
