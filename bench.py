@@ -215,7 +215,27 @@ def run_sigc(lib, s, host=None):
         lib.sxcf_correlation_batch_d([kw(t, t) for t in s["tasks"]])
         return
     for i, t in enumerate(s["tasks"]):
-        lib.sxcf_correlation(**kw(t, host["tasks"][i]))
+        lib.sxcf_correlation(**kw(t, host["tasks"][i]), keepwv=host.get("keepwv", False))
+
+
+_PACK_IDX = {}
+
+
+def pack_upper_device(torch, w, n, nrec, hermitize):
+    """W records (n x n, column-major, nrec of them, device) in ecalj's keepwv layout: the upper
+    triangle of each record in column order (j, i <= j); real-axis records symmetrised first,
+    (W(i,j) + conj(W(j,i)))/2, as the keepwv mode stores them (m_sxcf_gemm.f90:327-358)."""
+    m = w.view(nrec, n, n)                               # [record][column j][row i]
+    if hermitize:
+        m = 0.5 * (m + m.transpose(1, 2).conj())
+    key = (n, str(w.device))
+    if key not in _PACK_IDX:
+        j = torch.arange(n, device=w.device)
+        cols = torch.repeat_interleave(j, j + 1)         # j of each packed entry
+        rows = torch.arange(cols.numel(), device=w.device) - (cols * (cols + 1)) // 2
+        _PACK_IDX[key] = (cols, rows)
+    cols, rows = _PACK_IDX[key]
+    return m[:, cols, rows].reshape(-1).contiguous()
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -478,7 +498,9 @@ def main():
     e2e = None
     if not args.no_e2e:
         lib.set_precision(*modes[prec])
-        e2e = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist)
+        e2e = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=True)
+        full = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=False)
+        e2e["full_w_records"] = {k: full[k] for k in ("value", "ms_per_step", "h2d_bytes_per_step")}
     sur = None
     if not args.no_surrogate:
         lib.set_autotune(0, None)          # no tuning trials inside the study's timed calls
@@ -751,33 +773,43 @@ def measure_fp64_peak():
     return best
 
 
-def run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist):
+def run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=True):
     """Same step through the host-pointer C-ABI entry points: every step copies
     its inputs from pinned host memory and reads the results back.  The calls
     run in the library's asynchronous host mode (each returns once enqueued,
     so one call's copies overlap the previous call's kernels) and every step
-    ends with qsgw_synchronize, after which its outputs are on the host."""
+    ends with qsgw_synchronize, after which its outputs are on the host.
+    keepwv: the W records are held on the host in ecalj's keepwv layout (packed
+    upper triangles, half the bytes of the full records); else as full records."""
     N, niw = cfg_chi["N"], cfg_chi["niw"]
     zc_h = torch.empty(zc.numel(), dtype=torch.complex128, pin_memory=True)
     zc_h.copy_(zc)
     chi_h = torch.empty(N * N * niw, dtype=torch.complex128, pin_memory=True)
-    host = {"tasks": []}
+    host = {"tasks": [], "keepwv": keepwv}
     h2d = zc_h.numel() * 16
+    rec = N * (N + 1) // 2 if keepwv else N * N              # complex elements per W record
     for t in s["tasks"]:
         d = {}
+        src = {"zmel": t["zmel"]}
+        if keepwv:
+            src["wi"] = pack_upper_device(torch, t["wi"], N, s["niw"] + 1, False)
+            src["wr"] = pack_upper_device(torch, t["wr"], N, len(s["fr"]), True)
+        else:
+            src["wi"], src["wr"] = t["wi"], t["wr"]
         for k in ("zmel", "wi", "wr"):
-            d[k] = torch.empty(t[k].numel(), dtype=torch.complex128, pin_memory=True)
-            d[k].copy_(t[k])
+            d[k] = torch.empty(src[k].numel(), dtype=torch.complex128, pin_memory=True)
+            d[k].copy_(src[k])
+        del src
         d["zsec"] = torch.zeros(s["ntq"] * s["ntq"], dtype=torch.complex128, pin_memory=True)
         for k in ("zmel", "wi", "wr", "zsec"):
             d[k] = d[k].numpy().reshape(-1)
         d["zmel"] = d["zmel"].reshape((s["N"], s["nm"], s["ntq"]), order="F")
-        d["wi"] = d["wi"].reshape((s["N"], s["N"], s["niw"] + 1), order="F")
-        d["wr"] = d["wr"].reshape((s["N"], s["N"], len(s["fr"])), order="F")
+        d["wi"] = d["wi"].reshape((rec, s["niw"] + 1), order="F")
+        d["wr"] = d["wr"].reshape((rec, len(s["fr"])), order="F")
         d["zsec"] = d["zsec"].reshape((s["ntq"], s["ntq"]), order="F")
         host["tasks"].append(d)
-        h2d += (t["zmel"].numel() + t["wi"].numel()) * 16 + 16 * s["ntq"] ** 2
-        h2d += 16 * N * N * n_real_records(t, s)
+        h2d += t["zmel"].numel() * 16 + 16 * rec * (s["niw"] + 1) + 16 * s["ntq"] ** 2
+        h2d += 16 * rec * n_real_records(t, s)
     d2h = chi_h.numel() * 16 + len(s["tasks"]) * 16 * s["ntq"] ** 2
     zc_np = zc_h.numpy()
     chi_np = chi_h.numpy()
@@ -812,7 +844,9 @@ def run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist):
     return {"value": round(ws * flops / (ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(ms, 3),
             "steps": nst, "api": "qsgw_chi0_lorentz + qsgw_sxcf_correlation (host pointers, "
-                                 "qsgw_set_host_async(1), one qsgw_synchronize per step)"}
+                                 "qsgw_set_host_async(1), one qsgw_synchronize per step)",
+            "w_layout": ("keepwv: W records as packed upper triangles (ecalj --keepwv layout, half the bytes)"
+                         if keepwv else "full W records")}
 
 
 def n_real_records(t, s):
