@@ -498,8 +498,11 @@ def main():
     e2e = None
     if not args.no_e2e:
         lib.set_precision(*modes[prec])
-        e2e = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=True)
+        # the full-record run first: its pinned buffers are the larger, and the keepwv run's fit in them
         full = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=False)
+        release_pinned(torch)
+        e2e = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=True)
+        release_pinned(torch)
         e2e["full_w_records"] = {k: full[k] for k in ("value", "ms_per_step", "h2d_bytes_per_step")}
     sur = None
     if not args.no_surrogate:
@@ -855,6 +858,15 @@ def run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=True):
                                  "qsgw_set_host_async(1), one qsgw_synchronize per step)",
             "w_layout": ("keepwv: W records as packed upper triangles (ecalj --keepwv layout, half the bytes)"
                          if keepwv else "full W records")}
+
+
+def release_pinned(torch):
+    """Return the pinned host blocks torch keeps cached (tens of GB after an end-to-end run)."""
+    import gc
+    gc.collect()
+    fn = getattr(torch._C, "_host_emptyCache", None)
+    if fn is not None:
+        fn()
 
 
 def n_real_records(t, s):
