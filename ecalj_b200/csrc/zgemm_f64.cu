@@ -117,10 +117,11 @@ int zgemm_hn_thin(int n, long long K, const double2* A, long long lda, const dou
     static uint64_t attr = 0;                       // one bit per device
     int rc = smem_limit_once(reinterpret_cast<const void*>(zgemm_hn_thin_kernel<MB>), thin_smem_bytes<MB>(), attr);
     if (rc) return rc;
-    // one wave: as many K ranges as CTAs fit on the GPU at once
-    int per_sm = 0;
-    QSGW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zgemm_hn_thin_kernel<MB>, 128,
-                                                            thin_smem_bytes<MB>()));
+    // one wave: as many K ranges as CTAs fit on the GPU at once (occupancy queried once)
+    static int per_sm = 0;
+    if (per_sm == 0)
+      QSGW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zgemm_hn_thin_kernel<MB>, 128,
+                                                              thin_smem_bytes<MB>()));
     const long long nsplit = std::max<long long>(1, std::min<long long>(nch, std::max(per_sm, 1) * 1LL * ctx().sm_count));
     const long long kper = ((nch + nsplit - 1) / nsplit) * TH_BK;
     const unsigned grid = static_cast<unsigned>((K + kper - 1) / kper);
