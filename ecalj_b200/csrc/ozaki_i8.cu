@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 #include "split_common.cuh"
 #include "ozaki_i8.cuh"
@@ -66,8 +67,8 @@ struct Cfg {
   static constexpr int NST = STAGE_BUDGET / STAGE;                // 6, 4, 3 stages for NS = 2, 3, 4
   static constexpr int OFF_A = 0;                                 // [NST][NS] A' slices
   static constexpr int OFF_B = OFF_A + NST * NS * SLA8;        // [NST][NS] B slices
-  static constexpr int OFF_W = OFF_B + NST * NS * SLB8;        // drain column factors [16][32]
-  static constexpr int OFF_BAR = OFF_W + NDW * 32 * 8;
+  static constexpr int OFF_W = OFF_B + NST * NS * SLB8;        // drain column factors [16][2][32]
+  static constexpr int OFF_BAR = OFF_W + NDW * 64 * 8;
   static constexpr int NBAR = 3 * NST + 3;                        // full, cfull, empty [NST]; accfull, accempty, done
   static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
   static constexpr int SMEM = OFF_MISC + 64 + 1024;               // + slack for the 1024-byte alignment
@@ -237,13 +238,18 @@ struct SegParams {
   double post;                // 2^-(12 + 7 (NS - 1))
   double2* const* tile_out;   // [tile] output of the tile's task: column col at tile_out[t] + col ldc
   long long ldc;
+  int tail;                   // 1: M mod 64 <= 32 and the last row tile holds segment pairs (mapT)
   int* err;
 };
 
-template <int NS>
+// Paired tail.  When the last 64-row tile has at most 32 valid rows, its CTAs run the segments two at
+// a time: complex rows 0..31 of the A' tile are the tail rows of segment 2i, rows 32..63 those of
+// segment 2i + 1 (each half read from the half-height tail slices through mapT), so those CTAs do
+// half the MMAs; the drain weights each half with its own segment and adds the halves at the end.
+template <int NS, bool PAIRED>
 __global__ void __launch_bounds__(THREADS, 1)
     oz_seg_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                  const SegParams p) {
+                  const __grid_constant__ CUtensorMap mapT, const SegParams p) {
   using L = Cfg<NS>;
   constexpr int NST = L::NST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -261,11 +267,14 @@ __global__ void __launch_bounds__(THREADS, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::OFF_MISC + 8);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int mt = blockIdx.x % p.ntm, nt = blockIdx.x / p.ntm;   // the row tiles of a column tile adjacent
+  // the row tiles of a column tile adjacent; the paired launch covers the last row tile only
+  const int mt = PAIRED ? p.T - 1 : blockIdx.x % p.ntm, nt = PAIRED ? blockIdx.x : blockIdx.x / p.ntm;
   const int group = p.tile_group[nt];
   const int nseg = p.group_nseg[group];
   const int seg0 = p.group_seg_off[group];
-  const int nchunk = nseg * p.cps;
+  constexpr bool paired = PAIRED;
+  const int nstep = paired ? (nseg + 1) / 2 : nseg;   // accumulation periods: segments or segment pairs
+  const int nchunk = nstep * p.cps;
 
   if (tid == 0) {
     for (int i = 0; i < NST; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
@@ -290,7 +299,14 @@ __global__ void __launch_bounds__(THREADS, 1)
       // ---------------- TMA producer: NS slices of the segment's A' tile and of the B tile
       constexpr uint32_t bytes = NS * (SLA8 + SLB8);
       int issued = 0, sg = 0, cin = 0, st = 0, ph = 0;
-      int slot = p.seg_slot[seg0];
+      // this step's slot (paired: the slots of segments 2 sg and 2 sg + 1, the second repeated when absent)
+      auto step_slots = [&](int g, int& s0, int& s1) {
+        if (!paired) { s0 = s1 = p.seg_slot[seg0 + g]; return; }
+        s0 = p.seg_slot[seg0 + 2 * g];
+        s1 = 2 * g + 1 < nseg ? p.seg_slot[seg0 + 2 * g + 1] : s0;
+      };
+      int slot = 0, slot1 = 0;
+      step_slots(0, slot, slot1);
       for (int c = 0; c < nchunk; ++c) {
         if (c >= NST && !mbar_wait(&empty[st], ph ^ 1, abort_flag)) break;
         issued = c + 1;
@@ -298,12 +314,20 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int x = cin * K8;
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
-          tma_load_4d(sA + (st * NS + q) * SLA8, &mapA, &full[st], x, 0, 0, (q * p.nslot + slot) * p.T + mt);
+          unsigned char* dA = sA + (st * NS + q) * SLA8;
+          if constexpr (PAIRED) {                     // rows 0-31 / 32-63 re, 64-95 / 96-127 im
+            tma_load_4d(dA, &mapT, &full[st], x, 0, 0, q * p.nslot + slot);
+            tma_load_4d(dA + SLA8 / 4, &mapT, &full[st], x, 0, 0, q * p.nslot + slot1);
+            tma_load_4d(dA + SLA8 / 2, &mapT, &full[st], x, 0, 1, q * p.nslot + slot);
+            tma_load_4d(dA + 3 * SLA8 / 4, &mapT, &full[st], x, 0, 1, q * p.nslot + slot1);
+          } else {
+            tma_load_4d(dA, &mapA, &full[st], x, 0, 0, (q * p.nslot + slot) * p.T + mt);
+          }
           tma_load_3d(sB + (st * NS + q) * SLB8, &mapB, &full[st], x, nt * BN, q);
         }
         if (++cin == p.cps) {
           cin = 0;
-          if (++sg < nseg) slot = p.seg_slot[seg0 + sg];
+          if (++sg < nstep) step_slots(sg, slot, slot1);
         }
         if (++st == NST) { st = 0; ph ^= 1; }
       }
@@ -340,48 +364,83 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int c_lo = (dw >> 2) * 32;
       const int row = quad * 32 + lane;                 // accumulator row: 0..63 re, 64..127 im
       const int mloc = row & 63;
+      // paired tail: rows 32..63 (and 96..127) belong to the second segment of each pair
+      const int hb = paired ? (mloc >> 5) : 0;
+      const int mrow = paired ? (mloc & 31) : mloc;     // the row within the tile's output rows
       const uint32_t lane_base = static_cast<uint32_t>(quad * 32) << 16;
-      double* wsm = sW + dw * 32;
+      double* wsm = sW + dw * 64;                       // [2][32]: the pair's two weight sets
       double acc[32];
 #pragma unroll
       for (int j = 0; j < 32; ++j) acc[j] = 0.0;
-      bool ok = true;
       const int rtile = nt * BN + c_lo;
-      for (int seg = 0; seg < nseg; ++seg) {
-        const ZSeg zs = p.segs[seg0 + seg];
-        const int slot = p.seg_slot[seg0 + seg];
-        __syncwarp();                                   // the previous segment's reads of wsm are done
-        {
-          const int col = p.tile_cols[rtile + lane];
-          wsm[lane] = (col >= 0) ? zs.scale[static_cast<long long>(col) * zs.scale_cs] * p.nu_b[rtile + lane] : 0.0;
+      auto drain = [&]() -> bool {
+        for (int seg = 0; seg < nstep; ++seg) {
+          // this period's segment(s): one, or a pair (the second absent past the end: weight 0)
+          const int sa = PAIRED ? seg0 + 2 * seg : seg0 + seg;
+          int slot;
+          __syncwarp();                                 // the previous period's reads of wsm are done
+          {
+            const int col = p.tile_cols[rtile + lane];
+            const ZSeg z0 = p.segs[sa];
+            wsm[lane] = (col >= 0) ? z0.scale[static_cast<long long>(col) * z0.scale_cs] * p.nu_b[rtile + lane] : 0.0;
+            if constexpr (PAIRED) {
+              const bool has1 = 2 * seg + 1 < nseg;
+              double v1 = 0.0;
+              if (has1 && col >= 0) {
+                const ZSeg z1 = p.segs[sa + 1];
+                v1 = z1.scale[static_cast<long long>(col) * z1.scale_cs] * p.nu_b[rtile + lane];
+              }
+              wsm[32 + lane] = v1;
+              slot = p.seg_slot[hb && has1 ? sa + 1 : sa];
+            } else {
+              slot = p.seg_slot[sa];
+            }
+          }
+          const double rf = p.mu_a[static_cast<long long>(slot) * p.T * 64 + mt * 64 + mrow] * p.post;
+          const double* wuse = PAIRED ? wsm + 32 * hb : wsm;
+          __syncwarp();
+          if (!mbar_wait_warp(accfull, seg & 1, abort_flag)) return false;
+          tc_fence_after();
+#pragma unroll
+          for (int blk = 0; blk < 8; ++blk) {           // 4 columns at a time (96 registers per thread)
+            uint32_t v[NS][4];
+#pragma unroll
+            for (int lv = 0; lv < NS; ++lv)
+              tmem_ld4(tmem + lane_base + static_cast<uint32_t>(lv * BN + c_lo + blk * 4), v[lv]);
+            tmem_wait_ld();
+            if (blk == 7) {                             // every TMEM read of this segment is done
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(accempty);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              long long comb = static_cast<int>(v[0][j]);
+#pragma unroll
+              for (int lv = 1; lv < NS; ++lv) comb = comb * 128 + static_cast<int>(v[lv][j]);
+              acc[blk * 4 + j] = fma(static_cast<double>(comb) * rf, wuse[blk * 4 + j], acc[blk * 4 + j]);
+            }
+          }
         }
-        const double rf = p.mu_a[static_cast<long long>(slot) * p.T * 64 + mt * 64 + mloc] * p.post;
-        __syncwarp();
-        if (!mbar_wait_warp(accfull, seg & 1, abort_flag)) { ok = false; break; }
-        tc_fence_after();
+        return true;
+      };
+      const bool ok = drain();
+      if constexpr (PAIRED) {
+        // add the second segments' sums (rows 32..63, 96..127) to the first ones': through the A'
+        // stage buffers, free once the last period's MMAs are done (its accfull was seen above)
+        double* xb = reinterpret_cast<double*>(sA) + (((dw >> 2) * 2 + (quad >> 1)) * 32) * 32;
+        if (hb) {
 #pragma unroll
-        for (int blk = 0; blk < 8; ++blk) {             // 4 columns at a time (96 registers per thread)
-          uint32_t v[NS][4];
+          for (int j = 0; j < 32; ++j) xb[j * 32 + lane] = acc[j];
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(NDW * 32) : "memory");
+        if (!hb) {
 #pragma unroll
-          for (int lv = 0; lv < NS; ++lv)
-            tmem_ld4(tmem + lane_base + static_cast<uint32_t>(lv * BN + c_lo + blk * 4), v[lv]);
-          tmem_wait_ld();
-          if (blk == 7) {                               // every TMEM read of this segment is done
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(accempty);
-          }
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            long long comb = static_cast<int>(v[0][j]);
-#pragma unroll
-            for (int lv = 1; lv < NS; ++lv) comb = comb * 128 + static_cast<int>(v[lv][j]);
-            acc[blk * 4 + j] = fma(static_cast<double>(comb) * rf, wsm[blk * 4 + j], acc[blk * 4 + j]);
-          }
+          for (int j = 0; j < 32; ++j) acc[j] += xb[j * 32 + lane];
         }
       }
-      if (ok && !*abort_flag) {
-        const int m = mt * 64 + mloc;
+      if (ok && !*abort_flag && !hb) {
+        const int m = mt * 64 + mrow;
         const int part = row >= 64 ? 1 : 0;
         double2* const C = p.tile_out[nt];
         if (m < p.M) {
@@ -643,16 +702,20 @@ __global__ void oz_colscale_kernel(const double2* __restrict__ src, long long ld
 // Sigma_c A' slices from W (K x M per slot): A(m, k) = conj(W_slot[k + m ld]) into
 // [q][slot_out0 + slot][t][half][64][Kp] int8; each thread four consecutive k of one row.
 // grid (ceil(Kp/2 / 128), nslot * T), block 256: warp w rows w, w + 8, ..
-template <int NS>
+// TAIL: only the first 32 complex rows of the last row tile t = T - 1 (grid y = slot), into the
+// half-height tail layout [q][slot_out0 + slot][half][32][Kp] that the paired tail tiles read.
+// Tw: row tiles written per slot (T, or T - 1 when the last one is read from the tail slices).
+template <int NS, bool TAIL = false>
 __global__ void oz_slice_w_kernel(int8_t* __restrict__ out, const double2* __restrict__ w, long long ld,
-                                  long long slot_stride, int M, int K, int T, int nslot_total, int slot_out0, int Kp,
-                                  const double* __restrict__ mu) {
-  const int st = blockIdx.y;                           // slot * T + t of this launch
-  const int t = st % T, slot = st / T;
+                                  long long slot_stride, int M, int K, int T, int Tw, int nslot_total, int slot_out0,
+                                  int Kp, const double* __restrict__ mu) {
+  const int st = blockIdx.y;                           // slot * Tw + t of this launch (TAIL: slot)
+  const int t = TAIL ? T - 1 : st % Tw, slot = TAIL ? st : st / Tw;
   const int k0 = (blockIdx.x * 32 + (threadIdx.x & 31)) * 4;
   if (k0 >= Kp / 2) return;
   const int gslot = slot_out0 + slot;
-  for (int mm = threadIdx.x >> 5; mm < 64; mm += 8) {
+  constexpr int ROWS = TAIL ? 32 : 64;
+  for (int mm = threadIdx.x >> 5; mm < ROWS; mm += 8) {
     const int m = t * 64 + mm;
     const double inv = slice_unit<NS>() / mu[static_cast<long long>(gslot) * T * 64 + m];
     int sr[4][NS], si[4][NS];
@@ -666,14 +729,15 @@ __global__ void oz_slice_w_kernel(int8_t* __restrict__ out, const double2* __res
     }
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
-      const long long r0 = ((static_cast<long long>(q) * nslot_total + gslot) * T + t) * 128 + mm;
+      const long long r0 = TAIL ? (static_cast<long long>(q) * nslot_total + gslot) * 64 + mm
+                                : ((static_cast<long long>(q) * nslot_total + gslot) * T + t) * 128 + mm;
       uint2 h0, h1;                                    // half 0: [Re a, -Im a]; half 1: [Im a, Re a]
       h0.x = pack4(sr[0][q], -si[0][q], sr[1][q], -si[1][q]);
       h0.y = pack4(sr[2][q], -si[2][q], sr[3][q], -si[3][q]);
       h1.x = pack4(si[0][q], sr[0][q], si[1][q], sr[1][q]);
       h1.y = pack4(si[2][q], sr[2][q], si[3][q], sr[3][q]);
       *reinterpret_cast<uint2*>(out + r0 * Kp + 2 * k0) = h0;
-      *reinterpret_cast<uint2*>(out + (r0 + 64) * Kp + 2 * k0) = h1;
+      *reinterpret_cast<uint2*>(out + (r0 + ROWS) * Kp + 2 * k0) = h1;
     }
   }
 }
@@ -906,13 +970,14 @@ __global__ void oz_diff_norm_kernel(const double2* __restrict__ a, const double2
 static DevBuf g_a8, g_b8, g_mu, g_nu, g_tabs;          // Sigma_c
 static DevBuf g_y8, g_ymu, g_zmax, g_wr, g_bins;       // chi0
 
-template <int NS>
-static int launch_seg(const CUtensorMap& ma, const CUtensorMap& mb, const SegParams& p, dim3 grid, cudaStream_t s) {
+template <int NS, bool PAIRED>
+static int launch_seg(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mt, const SegParams& p,
+                      dim3 grid, cudaStream_t s) {
   static uint64_t attr = 0;                             // one bit per device
-  int rc = smem_limit_once(reinterpret_cast<const void*>(oz_seg_kernel<NS>), Cfg<NS>::SMEM, attr);
+  int rc = smem_limit_once(reinterpret_cast<const void*>(oz_seg_kernel<NS, PAIRED>), Cfg<NS>::SMEM, attr);
   if (rc) return rc;
   const int pi = prof_begin("sigc_seg_tc", s);
-  oz_seg_kernel<NS><<<grid, THREADS, Cfg<NS>::SMEM, s>>>(ma, mb, p);
+  oz_seg_kernel<NS, PAIRED><<<grid, THREADS, Cfg<NS>::SMEM, s>>>(ma, mb, mt, p);
   prof_end(pi, s);
   count_launch();
   QSGW_LAUNCH_CHECK("oz_seg_kernel");
@@ -956,12 +1021,16 @@ int rel_diff_fro(const double2* a, const double2* b, long long n, cudaStream_t s
 }
 
 static DevBuf g_cols;                                   // Sigma_c column map of every tile of a batch
+static DevBuf g_t8;                                     // Sigma_c half-height tail slices (paired tail)
+
+// the last row tile runs segment pairs when it has at most 32 valid rows
+static bool paired_tail(int M) { return M % 64 != 0 && M % 64 <= 32; }
 
 size_t OzSigcBatch::bytes_per(int ns, int ngb, int mrows, long long nslot, long long ntiles) {
   const long long T = (mrows + 63) / 64;
   const long long Kp = ((2LL * ngb + K8 - 1) / K8) * K8;
-  return static_cast<size_t>(ns) * (nslot * T * 128 + ntiles * BN) * Kp + (nslot * T * 64 + ntiles * BN) * 8 +
-         ntiles * BN * 4;
+  return static_cast<size_t>(ns) * (nslot * T * 128 + ntiles * BN + (paired_tail(mrows) ? nslot * 64 : 0)) * Kp +
+         (nslot * T * 64 + ntiles * BN) * 8 + ntiles * BN * 4;
 }
 
 int OzSigcBatch::reserve(int ns, int ngb, int mrows, long long ldc, long long nslot, long long ntiles) {
@@ -984,6 +1053,7 @@ int OzSigcBatch::reserve(int ns, int ngb, int mrows, long long ldc, long long ns
   if ((rc = g_b8.ensure(static_cast<size_t>(ns) * ntiles * BN * Kp))) return rc;
   if ((rc = g_mu.ensure(static_cast<size_t>(nslot) * T * 64 * sizeof(double)))) return rc;
   if ((rc = g_nu.ensure(static_cast<size_t>(ntiles) * BN * sizeof(double)))) return rc;
+  if (paired_tail(mrows) && (rc = g_t8.ensure(static_cast<size_t>(ns) * nslot * 64 * Kp))) return rc;
   return g_cols.ensure(static_cast<size_t>(ntiles) * BN * sizeof(int));
 }
 
@@ -1041,12 +1111,26 @@ int OzSigcBatch::add(const SigcSplitArgs& a, cudaStream_t s) {
   const int nst = static_cast<int>(cap_slot_);
   const long long rs = cap_tiles_ * BN;
   const dim3 gk(static_cast<unsigned>((Kp / 2 + 127) / 128));
+  const bool tail = paired_tail(M);
+  const int Tw = tail ? T - 1 : T;                     // the last row tile goes to the tail slices instead
   auto slice_w = [&](const double2* w, int n, int gslot0) {
-    const dim3 g(gk.x, static_cast<unsigned>(n * T));
-    if (ns == 2) oz_slice_w_kernel<2><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, nst, gslot0, Kp, mu);
-    else if (ns == 3) oz_slice_w_kernel<3><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, nst, gslot0, Kp, mu);
-    else oz_slice_w_kernel<4><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, nst, gslot0, Kp, mu);
-    count_launch();
+    if (Tw > 0) {
+      const dim3 g(gk.x, static_cast<unsigned>(n * Tw));
+      if (ns == 2) oz_slice_w_kernel<2><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, Tw, nst, gslot0, Kp, mu);
+      else if (ns == 3) oz_slice_w_kernel<3><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, Tw, nst, gslot0, Kp, mu);
+      else oz_slice_w_kernel<4><<<g, 256, 0, s>>>(A8, w, a.ldw, wst, M, ngb, T, Tw, nst, gslot0, Kp, mu);
+      count_launch();
+    }
+    if (tail) {                                        // the last row tile, half height
+      int8_t* T8 = g_t8.as<int8_t>();
+      const dim3 gt(gk.x, static_cast<unsigned>(n));
+      if (ns == 2)
+        oz_slice_w_kernel<2, true><<<gt, 256, 0, s>>>(T8, w, a.ldw, wst, M, ngb, T, Tw, nst, gslot0, Kp, mu);
+      else if (ns == 3)
+        oz_slice_w_kernel<3, true><<<gt, 256, 0, s>>>(T8, w, a.ldw, wst, M, ngb, T, Tw, nst, gslot0, Kp, mu);
+      else oz_slice_w_kernel<4, true><<<gt, 256, 0, s>>>(T8, w, a.ldw, wst, M, ngb, T, Tw, nst, gslot0, Kp, mu);
+      count_launch();
+    }
   };
   slice_w(a.wi, a.nimag, static_cast<int>(slot0));
   if (a.nreal > 0) slice_w(a.wr, a.nreal, static_cast<int>(slot0) + a.nimag);
@@ -1121,6 +1205,19 @@ int OzSigcBatch::launch(cudaStream_t s) {
     rc = make_tensor_map(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, g_b8.p, 3, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc) return rc;
   }
+  // paired tail: T8 [Kp, 32, 2, ns * cap_slot] box {64, 32, 1, 1} (one half of one slot's tail rows);
+  // without it the map is a copy of A's and never read
+  CUtensorMap mt = ma;
+  const bool tail = paired_tail(M_);
+  if (tail) {
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(Kp), 32, 2, static_cast<cuuint64_t>(ns) * cap_slot_};
+    const cuuint64_t str[3] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(Kp) * 32,
+                               static_cast<cuuint64_t>(Kp) * 64};
+    const cuuint32_t box[4] = {K8, 32, 1, 1};
+    rc = make_tensor_map(&mt, CU_TENSOR_MAP_DATA_TYPE_UINT8, g_t8.p, 4, dims, str, box, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc) return rc;
+  }
+  p.tail = tail ? 1 : 0;
   p.M = M_;
   p.ntm = T;
   p.cps = Kp / K8;
@@ -1132,11 +1229,21 @@ int OzSigcBatch::launch(cudaStream_t s) {
   p.post = post_scale(ns);
   p.ldc = ldc_;
   p.err = ctx().d_flags + 1;
-  const dim3 grid(static_cast<unsigned>(static_cast<long long>(T) * ntiles_));
+  // the full row tiles in one launch, the paired last row tile (if any) in a second
+  const int tmain = tail ? T - 1 : T;
+  p.ntm = tmain;
+  const long long nt_all = ntiles_;
   nslot_ = 0; ntiles_ = 0; cap_slot_ = 0; cap_tiles_ = 0;      // the next batch starts with reserve()
-  if (ns == 2) return launch_seg<2>(ma, mb, p, grid, s);
-  if (ns == 3) return launch_seg<3>(ma, mb, p, grid, s);
-  return launch_seg<4>(ma, mb, p, grid, s);
+  auto run = [&](auto nsc) -> int {
+    constexpr int NSV = decltype(nsc)::value;
+    int r = QSGW_OK;
+    if (tmain > 0) r = launch_seg<NSV, false>(ma, mb, mt, p, dim3(static_cast<unsigned>(tmain * nt_all)), s);
+    if (!r && tail) r = launch_seg<NSV, true>(ma, mb, mt, p, dim3(static_cast<unsigned>(nt_all)), s);
+    return r;
+  };
+  if (ns == 2) return run(std::integral_constant<int, 2>());
+  if (ns == 3) return run(std::integral_constant<int, 3>());
+  return run(std::integral_constant<int, 4>());
 }
 
 int sigc_split_i8(const SigcSplitArgs& a, int ns, cudaStream_t s) {
