@@ -481,15 +481,17 @@ def main():
     else:
         peak = fp64_peak
         peak_note = "cuBLAS ZGEMM (complex128, 4096^3) measured in this run; MEASURED_PEAKS.json has no FP64 figure"
-    # Sigma_c tasks per launch of the dominant kernel (the int8 path batches the step's tasks)
+    # Sigma_c tasks per launch of the dominant kernel (the int8 path batches the step's tasks; a batch is
+    # a launch over the full row tiles plus one over the paired last row tile): the per-launch figures
+    # below are averages over the step's launches of the kernel
     tasks_per_launch = len(s["tasks"]) * args.steps / max(k_n, 1)
     traffic = SIGC_TC_TRAFFIC.get(prec)
     roof = {"bound": "tensor", "achieved": round(achieved, 3) if achieved else None, "peak": round(peak, 3),
             "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if achieved else None,
             "traffic": traffic * tasks_per_launch if traffic else None,
-            "traffic_source": (f"dram__bytes_read.sum + dram__bytes_write.sum of the kernel on one Sigma_c task "
-                               f"of the same shape from ncu ({traffic:.4g} B), times the {tasks_per_launch:g} "
-                               f"tasks a launch runs" if traffic else "not captured"),
+            "traffic_source": (f"dram__bytes_read.sum + dram__bytes_write.sum of the kernel's launches on one "
+                               f"Sigma_c task of the same shape from ncu ({traffic:.4g} B), times the "
+                               f"{tasks_per_launch:g} tasks a launch runs on average" if traffic else "not captured"),
             "tasks_per_launch": tasks_per_launch,
             "kernel": dom_tag, "launch_ms": round(per_launch_ms, 4), "peak_source": peak_note,
             "algorithmic_flops_per_launch": dom_flops * args.steps / max(k_n, 1)}
