@@ -38,7 +38,7 @@ METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err 
 # (N=600, 40 x 400 states, 25 imaginary slots + real-axis pole columns),
 # measured with ncu on that launch, per kernel of the path.
 # split-i8: the 4-slice launch, the count the automatic choice makes on this workload.
-SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": 2.039e9}
+SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": 1.911e9}
 
 
 def load_peaks():

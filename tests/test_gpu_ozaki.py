@@ -60,6 +60,22 @@ def test_sigc_i8_matches_emulation_and_oracle(i8, ns, ngb):
     assert e_ref < GATE[ns]
 
 
+@pytest.mark.parametrize("ngb", [129, 160, 161])
+def test_sigc_i8_paired_tail_edges(i8, ngb):
+    """The last row tile runs segment pairs when it holds 1..32 of its 64 rows: ngb = 129 (1 row),
+    160 (32 rows, both halves full) paired, 161 (33 rows) not.  Each equals the emulation."""
+    s = _sigc_problem(ngb, 8, 40, 5, 10, seed=ngb)
+    args = _sigc_args(s)
+    emu = np.zeros((s['ntq'], s['ntq']), complex, order='F')
+    ozaki_emul.correlation_block(emu, s['z'], *args, ns=4)
+    i8.set_precision(i8.PREC_SPLIT_I8, 4)
+    got = np.zeros((s['ntq'], s['ntq']), complex, order='F')
+    i8.sxcf_correlation(got, s['z'], *args)
+    e = rel_fro(got, emu)
+    print(f"sigc i8x4 ngb={ngb} (last tile {ngb % 64} rows): vs emulation {e:.2e}")
+    assert e < EXACT
+
+
 @pytest.mark.parametrize("keepwv", [False, True])
 def test_sigc_i8_golden_case_vs_oracle(i8, keepwv):
     """The golden Sigma_c case, W given in full or as the packed upper
