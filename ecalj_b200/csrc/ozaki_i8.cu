@@ -21,13 +21,24 @@
 //     v = sum_L acc_L 2^(7 (NS - 1 - L)),
 // and scales v by mu_row nu_col 2^-(12 + 7 (NS - 1)) in FP64.  A level holds at
 // most NS products of |s| <= 64 over K' real K, so |acc| < NS 2^12 K', which
-// bounds K' between drains (INT32).
+// bounds K' between drains (INT32).  These base-128 digits are the chi0
+// kernel's: symmetric, so negation commutes with the slicing (rint is
+// symmetric) and the slices of -x are the negated slices of x, which the chi0
+// kernel uses to build rows in shared memory.
+//
+// The Sigma_c kernel (also behind the zmel M -> E product) slices every
+// operand in HBM, negated parts included, and so uses base-256 digits over the
+// whole int8 range [-128, 127] (slice8): V = rint(x U8 / mu), U8 just under
+// 2^(8 NS - 1), mu = max |x| of the row (column) itself rather than a power of
+// two above it, eight bits a slice instead of seven, v = sum_L acc_L
+// 256^(NS - 1 - L) scaled by mu nu 256^(NS - 1) / U8^2.  Three base-256 slices
+// hold 23 bits, four base-128 ones 27: six slice products instead of ten for
+// an error within the QP-energy target.  |acc| < NS 2^14 K'.
 //
 // A complex product C = A B is one real GEMM with M doubled and K interleaved
 // (k' = 2k + {re, im}): rows (m, re) of A' = [Re a, -Im a], rows (m, im) =
 // [Im a, Re a], B' row n = [Re b, Im b]; lanes 0..63 of an accumulator hold
-// Re C, 64..127 Im C.  Negation commutes with the slicing (rint is symmetric),
-// so the slices of -x are the negated slices of x.
+// Re C, 64..127 Im C.
 //
 // Kernels (576 threads, one CTA per SM):
 //     warp 0        TMA producer
@@ -202,6 +213,30 @@ __device__ __forceinline__ void slice(double x, double scale, int (&s)[NS]) {
   }
   s[0] = v;
 }
+// The Sigma_c kernel's digits: base 256, every int8 value.  U8 = 127 256^(NS-1) - 128 (256^(NS-1) - 1)
+// / 255, so that x / mu in [-1, 1] times U8 is an integer V with |V| <= U8 whose NS digits, taken
+// from the bottom in [-128, 127], leave a top digit in [-128, 127] too (the lower digits sum to at
+// most 128 (256^(NS-1) - 1) / 255 in magnitude).  One bit more per slice than the base-128 digits;
+// negation does not commute with this slicing, so the kernels that need -x slice it on their own.
+template <int NS>
+__host__ __device__ constexpr double slice_unit8() {
+  return static_cast<double>(127LL * (1LL << (8 * (NS - 1))) - 128LL * (((1LL << (8 * (NS - 1))) - 1) / 255));
+}
+// NS base-256 slices of x given scale = slice_unit8<NS>() / mu, mu = max |x| of the row or column
+// (x * scale rounded once; |x| <= mu keeps |V| <= U8 < 2^31 - 128 after the rounding, as U8 is an
+// integer): V = rint(x * scale), digits d = v - 256 q, q = floor((v + 128) / 256) (arithmetic
+// shift), three integer operations a digit
+template <int NS>
+__device__ __forceinline__ void slice8(double x, double scale, int (&s)[NS]) {
+  int v = __double2int_rn(x * scale);
+#pragma unroll
+  for (int i = NS - 1; i >= 1; --i) {
+    const int q = (v + 128) >> 8;
+    s[i] = v - (q << 8);
+    v = q;
+  }
+  s[0] = v;
+}
 // the low bytes of a, b, c, d (two's complement int8) as one word, a lowest
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
   const uint32_t ab = __byte_perm(static_cast<uint32_t>(a), static_cast<uint32_t>(b), 0x0040);
@@ -235,7 +270,7 @@ struct SegParams {
   const ZSeg* segs;
   const double* mu_a;         // [slot][T * 64] row scales
   const double* nu_b;         // [nrows] column scales
-  double post;                // 2^-(12 + 7 (NS - 1))
+  double post;                // 256^(NS - 1) / U8^2 (slice_unit8)
   double2* const* tile_out;   // [tile] output of the tile's task: column col at tile_out[t] + col ldc
   long long ldc;
   int tail;                   // 1: M mod 64 <= 32 and the last row tile holds segment pairs (mapT)
@@ -417,7 +452,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (int j = 0; j < 4; ++j) {
               long long comb = static_cast<int>(v[0][j]);
 #pragma unroll
-              for (int lv = 1; lv < NS; ++lv) comb = comb * 128 + static_cast<int>(v[lv][j]);
+              for (int lv = 1; lv < NS; ++lv) comb = comb * 256 + static_cast<int>(v[lv][j]);
               acc[blk * 4 + j] = fma(static_cast<double>(comb) * rf, wuse[blk * 4 + j], acc[blk * 4 + j]);
             }
           }
@@ -676,9 +711,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 // =====================================================================================
 // operand preparation (HBM-bound)
 
-// out[slot * ncols_out + j] = power-of-two scale of column c = colmap[j] (or j) of the complex
-// column-major matrix src + slot * slot_stride (leading dimension ld): max over k < K of
-// max(|Re|, |Im|); 1 for absent columns.  One warp per column.
+// out[slot * ncols_out + j] = scale of column c = colmap[j] (or j) of the complex column-major
+// matrix src + slot * slot_stride (leading dimension ld): the max over k < K of max(|Re|, |Im|)
+// itself (the base-256 slicing divides by it, so no power of two is needed, and the full
+// digit range is used); 1 for absent, zero or non-finite columns.  One warp per column.
 __global__ void oz_colscale_kernel(const double2* __restrict__ src, long long ld, long long slot_stride, int K,
                                    int ncols_valid, const int* __restrict__ colmap, int ncols_out,
                                    double* __restrict__ out) {
@@ -696,7 +732,7 @@ __global__ void oz_colscale_kernel(const double2* __restrict__ src, long long ld
     }
   }
   for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0) out[static_cast<long long>(slot) * ncols_out + j] = pow2_at_least(m);
+  if (lane == 0) out[static_cast<long long>(slot) * ncols_out + j] = (m > 0.0 && isfinite(m)) ? m : 1.0;
 }
 
 // Sigma_c A' slices from W (K x M per slot): A(m, k) = conj(W_slot[k + m ld]) into
@@ -717,23 +753,24 @@ __global__ void oz_slice_w_kernel(int8_t* __restrict__ out, const double2* __res
   constexpr int ROWS = TAIL ? 32 : 64;
   for (int mm = threadIdx.x >> 5; mm < ROWS; mm += 8) {
     const int m = t * 64 + mm;
-    const double inv = slice_unit<NS>() / mu[static_cast<long long>(gslot) * T * 64 + m];
-    int sr[4][NS], si[4][NS];
+    const double inv = slice_unit8<NS>() / mu[static_cast<long long>(gslot) * T * 64 + m];
+    int sr[4][NS], si[4][NS], sn[4][NS];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int k = k0 + i;
       double2 v = make_double2(0.0, 0.0);
       if (m < M && k < K) v = w[static_cast<long long>(slot) * slot_stride + k + static_cast<long long>(m) * ld];
-      slice<NS>(v.x, inv, sr[i]);                      // Re a
-      slice<NS>(-v.y, inv, si[i]);                     // Im a  (a = conj(W))
+      slice8<NS>(v.x, inv, sr[i]);                     // Re a
+      slice8<NS>(-v.y, inv, si[i]);                    // Im a  (a = conj(W))
+      slice8<NS>(v.y, inv, sn[i]);                     // -Im a, sliced on its own (base-256 digits)
     }
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
       const long long r0 = TAIL ? (static_cast<long long>(q) * nslot_total + gslot) * 64 + mm
                                 : ((static_cast<long long>(q) * nslot_total + gslot) * T + t) * 128 + mm;
       uint2 h0, h1;                                    // half 0: [Re a, -Im a]; half 1: [Im a, Re a]
-      h0.x = pack4(sr[0][q], -si[0][q], sr[1][q], -si[1][q]);
-      h0.y = pack4(sr[2][q], -si[2][q], sr[3][q], -si[3][q]);
+      h0.x = pack4(sr[0][q], sn[0][q], sr[1][q], sn[1][q]);
+      h0.y = pack4(sr[2][q], sn[2][q], sr[3][q], sn[3][q]);
       h1.x = pack4(si[0][q], sr[0][q], si[1][q], sr[1][q]);
       h1.y = pack4(si[2][q], sr[2][q], si[3][q], sr[3][q]);
       *reinterpret_cast<uint2*>(out + r0 * Kp + 2 * k0) = h0;
@@ -753,15 +790,15 @@ __global__ void oz_slice_z_kernel(int8_t* __restrict__ out, const double2* __res
   const int k0 = (blockIdx.x * 32 + (threadIdx.x & 31)) * 4;
   if (r >= nrows || k0 >= Kp / 2) return;
   const int c = cols[r];
-  const double inv = slice_unit<NS>() / nu[r];
+  const double inv = slice_unit8<NS>() / nu[r];
   int sr[4][NS], si[4][NS];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int k = k0 + i;
     double2 v = make_double2(0.0, 0.0);
     if (c >= 0 && k < K) v = z[k + static_cast<long long>(c) * ld];
-    slice<NS>(v.x, inv, sr[i]);
-    slice<NS>(v.y, inv, si[i]);
+    slice8<NS>(v.x, inv, sr[i]);
+    slice8<NS>(v.y, inv, si[i]);
   }
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
@@ -821,9 +858,10 @@ __global__ void oz_mu_kernel(const unsigned long long* __restrict__ zmax, const 
 // Thread (row mm, group g) slices the 8 consecutive entries 8 g .. 8 g + 7 of its row (loads
 // coalesced along m), the 16 bytes per slice go to a shared tile with 80-byte rows (no bank
 // conflicts), and 64 rows x 64 bytes per slice leave coalesced along K.
+// the NS slices of the 8 entries (f z) of one row as 16 bytes each: (re, im) int8 pairs in entry order
 template <int NS>
-__device__ __forceinline__ void y_tile_pack(int8_t (*tile)[64][80], int mm, int g, const double (&f)[8],
-                                            const double2 (&zv)[8], double scale) {
+__device__ __forceinline__ void y_pack(uint4 (&out)[NS], const double (&f)[8], const double2 (&zv)[8],
+                                       double scale) {
   uint32_t w[NS][4];
 #pragma unroll
   for (int jp = 0; jp < 4; ++jp) {
@@ -838,8 +876,15 @@ __device__ __forceinline__ void y_tile_pack(int8_t (*tile)[64][80], int mm, int 
     for (int q = 0; q < NS; ++q) w[q][jp] = pack4(r0[q], i0[q], r1[q], i1[q]);
   }
 #pragma unroll
-  for (int q = 0; q < NS; ++q)
-    *reinterpret_cast<uint4*>(&tile[q][mm][g * 16]) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+  for (int q = 0; q < NS; ++q) out[q] = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+}
+template <int NS>
+__device__ __forceinline__ void y_tile_pack(int8_t (*tile)[64][80], int mm, int g, const double (&f)[8],
+                                            const double2 (&zv)[8], double scale) {
+  uint4 out[NS];
+  y_pack<NS>(out, f, zv, scale);
+#pragma unroll
+  for (int q = 0; q < NS; ++q) *reinterpret_cast<uint4*>(&tile[q][mm][g * 16]) = out[q];
 }
 
 // Y8 is chunk-major: [chunk][slice][row][64 bytes], so one TMA box (64 or 128 rows of one chunk
@@ -899,19 +944,23 @@ __global__ void __launch_bounds__(256)
 }
 
 // chi0, every bin over the same columns 0..n-1 in order (bin b's weights at ew[b * n + e]): z is read
-// once per (32-column block, 64-row tile) item and sliced for every bin with a weight of this sign;
-// the 32 weights' square roots of a bin are formed once per item in shared memory.
+// once per (32-column block, 64-row tile) item and sliced for every bin with a weight of this sign.
+// Thread (row mm = tid / 4, group g = tid % 4) slices the 8 consecutive entries 8 g .. 8 g + 7 of
+// its row; their 16 bytes per slice are one piece of the row's 64-byte chunk, so a warp (8 rows x
+// 4 groups) stores 512 contiguous bytes per slice straight from registers and loads 4 x 128
+// contiguous bytes of z per entry.  The square roots of the weights of up to kDenseBins bins are
+// formed once per item in shared memory: two barriers per item and bin group, none per bin.
+constexpr int kDenseBins = 32;
 template <int NS>
 __global__ void __launch_bounds__(256)
     oz_slice_y_dense_kernel(int8_t* __restrict__ y8, int Rows, const double2* __restrict__ z,
                             long long ldz, int n, int nbins, const double* __restrict__ ew,
                             const long long* __restrict__ bin_k0, const double* __restrict__ wr,
                             const double* __restrict__ mu, double sign) {
-  __shared__ __align__(16) int8_t tile[NS][64][80];
-  __shared__ double sf[32];
+  __shared__ double sf[kDenseBins][32];
   const int neb = (n + 31) / 32;
   const int nrt = (Rows + 63) / 64;
-  const int mm = threadIdx.x & 63, g = threadIdx.x >> 6;
+  const int mm = threadIdx.x >> 2, g = threadIdx.x & 3;
   for (long long item = blockIdx.x; item < static_cast<long long>(neb) * nrt; item += gridDim.x) {
     const int eb = static_cast<int>(item % neb), rt = static_cast<int>(item / neb);
     const int m = rt * 64 + mm;
@@ -921,21 +970,28 @@ __global__ void __launch_bounds__(256)
       const int e = eb * 32 + g * 8 + jj;
       zv[jj] = (e < n && m < Rows) ? z[m + static_cast<long long>(e) * ldz] : make_double2(0.0, 0.0);
     }
-    for (int b = 0; b < nbins; ++b) {
-      if (!(w_extent(wr, b, sign) > 0.0)) continue;                 // uniform over the block
-      if (threadIdx.x < 32) {
-        const int e = eb * 32 + threadIdx.x;
-        sf[threadIdx.x] = (e < n) ? sqrt(fmax(sign * ew[static_cast<long long>(b) * n + e], 0.0)) : 0.0;
+    for (int b0 = 0; b0 < nbins; b0 += kDenseBins) {
+      const int nb = min(kDenseBins, nbins - b0);
+      __syncthreads();                                   // every read of the previous group's sf is done
+      for (int i = threadIdx.x; i < nb * 32; i += 256) {
+        const int bb = i >> 5, c = i & 31, e = eb * 32 + c;
+        sf[bb][c] = (e < n) ? sqrt(fmax(sign * ew[static_cast<long long>(b0 + bb) * n + e], 0.0)) : 0.0;
       }
       __syncthreads();
-      double f[8];
+      if (m >= Rows) continue;
+      for (int bb = 0; bb < nb; ++bb) {
+        const int b = b0 + bb;
+        if (!(w_extent(wr, b, sign) > 0.0)) continue;
+        double f[8];
 #pragma unroll
-      for (int jj = 0; jj < 8; ++jj) f[jj] = sf[g * 8 + jj];
-      const double scale = (m < Rows) ? slice_unit<NS>() / mu[static_cast<long long>(b) * Rows + m] : 0.0;
-      y_tile_pack<NS>(tile, mm, g, f, zv, scale);
-      __syncthreads();
-      y_tile_store<NS>(y8, tile, Rows, rt, bin_k0[b] + eb);
-      __syncthreads();
+        for (int jj = 0; jj < 8; ++jj) f[jj] = sf[bb][g * 8 + jj];
+        uint4 out[NS];
+        y_pack<NS>(out, f, zv, slice_unit<NS>() / mu[static_cast<long long>(b) * Rows + m]);
+        const long long chunk = bin_k0[b] + eb;
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+          *reinterpret_cast<uint4*>(y8 + ((chunk * NS + q) * Rows + m) * 64 + g * 16) = out[q];
+      }
     }
   }
 }
@@ -999,6 +1055,11 @@ static int launch_herk(const CUtensorMap& ma, const CUtensorMap& mb, const HerkP
 }
 
 static double post_scale(int ns) { return std::ldexp(1.0, -(12 + 7 * (ns - 1))); }
+// the Sigma_c kernel's base-256 digits: 256^(ns-1) / U8^2
+static double post_scale8(int ns) {
+  const double u = ns == 2 ? slice_unit8<2>() : (ns == 3 ? slice_unit8<3>() : slice_unit8<4>());
+  return std::ldexp(1.0, 8 * (ns - 1)) / (u * u);
+}
 
 }  // namespace oz
 
@@ -1039,8 +1100,9 @@ int OzSigcBatch::reserve(int ns, int ngb, int mrows, long long ldc, long long ns
            "sigc split-i8: ngb=%d rows=%d slots=%lld tiles=%lld", ngb, mrows, nslot, ntiles);
   const int T = (mrows + 63) / 64;
   const int Kp = ((2 * ngb + K8 - 1) / K8) * K8;
-  // exact INT32 levels over one segment (K' = Kp): ns * 4096 * Kp < 2^31; int tile coordinates
-  QSGW_ARG(static_cast<long long>(ns) * 4096 * Kp < (1LL << 31), "sigc split-i8: ngb=%d too large", ngb);
+  // exact INT32 levels over one segment (K' = Kp, at most ns products of |d| <= 128 per level):
+  // ns * 16384 * Kp < 2^31; int tile coordinates
+  QSGW_ARG(static_cast<long long>(ns) * 16384 * Kp < (1LL << 31), "sigc split-i8: ngb=%d too large", ngb);
   QSGW_ARG(ns * nslot * T < (1LL << 31) && ntiles * BN < (1LL << 31),
            "sigc split-i8: batch of %lld slots, %lld tiles too large", nslot, ntiles);
   ns_ = ns; ngb_ = ngb; M_ = mrows; ldc_ = ldc; T_ = T; Kp_ = Kp;
@@ -1226,7 +1288,7 @@ int OzSigcBatch::launch(cudaStream_t s) {
   p.nrows = static_cast<int>(nrows);
   p.tile_cols = g_cols.as<int>();
   p.mu_a = g_mu.as<double>(); p.nu_b = g_nu.as<double>();
-  p.post = post_scale(ns);
+  p.post = post_scale8(ns);
   p.ldc = ldc_;
   p.err = ctx().d_flags + 1;
   // the full row tiles in one launch, the paired last row tile (if any) in a second

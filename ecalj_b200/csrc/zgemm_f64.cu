@@ -25,18 +25,20 @@ static int launch_kernel(const ZParams& p, dim3 grid, cudaStream_t s) {
 // ---- thin A^H B: C(0:n, 0:n) += A^H B for complex A, B of K x n (column-major, leading dimensions
 // lda, ldb), n <= 64 and K large: the last contraction of Sigma_c, zsec += czmelwc^H zmel over
 // K = ngb (ns2 - ns1 + 1) (m_sxcf_gemm.f90:599).  The general engine's 64 x 64 tiles would run
-// 2.6x the needed DMMA work at n = 40; here n is padded only to 16 (rows) and 8 (columns).  A CTA
-// (4 warps) takes a K range; the MB x NB fragments (m16 x n8) of the output are dealt round-robin
-// to its warps, which share the staged operands; the CTA's partial sums go to C by FP64 atomics.
+// 2.6x the needed DMMA work at n = 40; here n is padded only to 16 (rows, MB m16 blocks) and 8
+// (columns, NB n8 blocks: 48 x 40 at n = 40).  A CTA (4 warps) takes a K range; the MB x NB
+// fragments (m16 x n8) of the output are dealt round-robin to its warps, which share the staged
+// operands; the CTA's partial sums go to C by FP64 atomics.
 constexpr int TH_BK = 16;                          // k per stage
 template <int MB>
 constexpr int thin_smem_bytes() { return 2 * 2 * TH_BK * (MB * 16 + 2) * static_cast<int>(sizeof(double2)); }
-template <int MB>
+template <int MB, int NB>
 __global__ void __launch_bounds__(128) zgemm_hn_thin_kernel(const double2* __restrict__ A, long long lda,
                                                             const double2* __restrict__ B, long long ldb, int n,
                                                             long long K, long long kper, double2* __restrict__ C,
                                                             long long ldc) {
-  constexpr int NB = 2 * MB, NF = MB * NB, FPW = (NF + 3) / 4;
+  static_assert(NB <= 2 * MB, "the staged B columns cover 16 MB");
+  constexpr int NF = MB * NB, FPW = (NF + 3) / 4;
   constexpr int R = MB * 16, PR = R + 2;           // padded rows of A^H (= columns of B); pitch
   extern __shared__ __align__(16) unsigned char th_smem[];       // thin_smem_bytes<MB>()
   double2 (*sa)[TH_BK][PR] = reinterpret_cast<double2 (*)[TH_BK][PR]>(th_smem);
@@ -112,28 +114,34 @@ int zgemm_hn_thin(int n, long long K, const double2* A, long long lda, const dou
   QSGW_ARG(n >= 1 && n <= 64 && K >= 0, "zgemm_hn_thin: n=%d (1..64), K=%lld", n, K);
   if (K == 0) return QSGW_OK;
   const long long nch = (K + TH_BK - 1) / TH_BK;
-  auto run = [&](auto mb) -> int {
-    constexpr int MB = decltype(mb)::value;
+  auto run = [&](auto mb, auto nb) -> int {
+    constexpr int MB = decltype(mb)::value, NB = decltype(nb)::value;
+    auto kern = zgemm_hn_thin_kernel<MB, NB>;
     static uint64_t attr = 0;                       // one bit per device
-    int rc = smem_limit_once(reinterpret_cast<const void*>(zgemm_hn_thin_kernel<MB>), thin_smem_bytes<MB>(), attr);
+    int rc = smem_limit_once(reinterpret_cast<const void*>(kern), thin_smem_bytes<MB>(), attr);
     if (rc) return rc;
     // one wave: as many K ranges as CTAs fit on the GPU at once (occupancy queried once)
     static int per_sm = 0;
     if (per_sm == 0)
-      QSGW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zgemm_hn_thin_kernel<MB>, 128,
-                                                              thin_smem_bytes<MB>()));
+      QSGW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, thin_smem_bytes<MB>()));
     const long long nsplit = std::max<long long>(1, std::min<long long>(nch, std::max(per_sm, 1) * 1LL * ctx().sm_count));
     const long long kper = ((nch + nsplit - 1) / nsplit) * TH_BK;
     const unsigned grid = static_cast<unsigned>((K + kper - 1) / kper);
-    zgemm_hn_thin_kernel<MB><<<grid, 128, thin_smem_bytes<MB>(), s>>>(A, lda, B, ldb, n, K, kper, C, ldc);
+    kern<<<grid, 128, thin_smem_bytes<MB>(), s>>>(A, lda, B, ldb, n, K, kper, C, ldc);
     return QSGW_OK;
   };
+  using std::integral_constant;
   const int pi = prof_begin("gemm_dmma", s);
   int rc;
-  if (n <= 16) rc = run(std::integral_constant<int, 1>());
-  else if (n <= 32) rc = run(std::integral_constant<int, 2>());
-  else if (n <= 48) rc = run(std::integral_constant<int, 3>());
-  else rc = run(std::integral_constant<int, 4>());
+  const bool odd8 = ((n + 7) / 8) % 2 == 1;        // n8 column blocks: 2 MB - 1 or 2 MB
+  if (n <= 16) rc = odd8 ? run(integral_constant<int, 1>(), integral_constant<int, 1>())
+                         : run(integral_constant<int, 1>(), integral_constant<int, 2>());
+  else if (n <= 32) rc = odd8 ? run(integral_constant<int, 2>(), integral_constant<int, 3>())
+                              : run(integral_constant<int, 2>(), integral_constant<int, 4>());
+  else if (n <= 48) rc = odd8 ? run(integral_constant<int, 3>(), integral_constant<int, 5>())
+                              : run(integral_constant<int, 3>(), integral_constant<int, 6>());
+  else rc = odd8 ? run(integral_constant<int, 4>(), integral_constant<int, 7>())
+                 : run(integral_constant<int, 4>(), integral_constant<int, 8>());
   if (rc) return rc;
   prof_end(pi, s);
   count_launch();

@@ -5,8 +5,9 @@ Two kinds of check:
   (same scales, slices and kept slice pairs, exact integer products): the GPU
   must match it to FP64 rounding -- this pins the kernels themselves;
 * against the FP64 oracle: the error the slicing leaves, gated per slice count
-  (about 2^-(7 ns) relative to the largest element of a row or column, and
-  unbiased, since the integer products accumulate exactly).
+  (about 2^-(7 ns) relative to the largest element of a row or column for the
+  chi0 kernel's base-128 digits, 2^-(8 ns) for the Sigma_c kernel's base-256
+  ones, and unbiased, since the integer products accumulate exactly).
 """
 import numpy as np
 import pytest
@@ -221,7 +222,7 @@ def test_zmel_m2e_i8_matches_emulation(i8, ns, conj):
     m2e = _rc(rng, ngb, nbb)
     zmelt = _rc(rng, ngb, nmtot, nqtot)
     ref = (m2e.conj().T @ zmelt.reshape(ngb, -1, order='F')).reshape(nbb, nmtot, nqtot, order='F')
-    emu = ozaki_emul.complex_product(m2e.conj().T, zmelt.reshape(ngb, -1, order='F'), ns)
+    emu = ozaki_emul.complex_product(m2e.conj().T, zmelt.reshape(ngb, -1, order='F'), ns, bits=8)
     emu = emu.reshape(nbb, nmtot, nqtot, order='F')
     if conj:
         ref, emu = ref.conj(), emu.conj()

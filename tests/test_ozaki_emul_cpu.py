@@ -1,7 +1,8 @@
 """The CPU emulation of the int8 Ozaki scheme (tests/ozaki_emul.py), which
 the GPU tests use as the exact reference of the SPLIT_I8 kernels: its slices
-stay in int8 range and rebuild each element to 2^-(7 ns) of the row scale,
-and its products converge to the FP64 product as the slice count grows."""
+stay in int8 range and rebuild each element to 2^-(7 ns) (base-128 digits) or
+about 2^-(8 ns) (base-256 digits) of the row scale, and its products converge
+to the FP64 product as the slice count grows."""
 import numpy as np
 
 from tests import ozaki_emul
@@ -21,6 +22,33 @@ def test_slices_fit_int8_and_rebuild_the_value():
         assert all(np.array_equal(a, -b) for a, b in zip(s, sn))
 
 
+def test_base256_slices_use_the_whole_int8_range_and_rebuild_the_value():
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((40, 300)) * 10.0 ** rng.uniform(-3, 3, (40, 1))
+    x[0, :4] = [1.0, -1.0, 0.5, -0.75]              # values at the scale itself
+    mu = ozaki_emul.pow2_at_least(np.abs(x).max(axis=1))[:, None]
+    for ns in (2, 3, 4):
+        u = ozaki_emul.unit(ns, 8)
+        assert u < 2.0 ** (8 * ns - 1) and u > 0.98 * 2.0 ** (8 * ns - 1)
+        s = ozaki_emul.slices(x, mu, ns, bits=8)
+        lo = min(si.min() for si in s)
+        hi = max(si.max() for si in s)
+        assert lo >= -128 and hi <= 127 and lo == -128 and hi == 127
+        back = sum(si * 256.0 ** (ns - 1 - i) for i, si in enumerate(s)) * (mu / u)
+        assert np.max(np.abs(back - x) / mu) <= 0.5 / u * (1 + 1e-12)
+
+
+def test_base256_top_digit_stays_in_range_at_the_extremes():
+    # every integer V with |V| <= U has digits in [-128, 127]: the extremes and their neighbours
+    for ns in (2, 3, 4):
+        u = int(ozaki_emul.unit(ns, 8))
+        v = np.array([u, u - 1, -u, -u + 1, 0, 127, -128, 128, -129], np.float64)
+        s = ozaki_emul.slices(v, u, ns, bits=8)          # mu = U: V = v exactly
+        assert all(si.min() >= -128 and si.max() <= 127 for si in s)
+        back = sum(si * 256 ** (ns - 1 - i) for i, si in enumerate(s))
+        assert np.array_equal(back, v.astype(np.int64))
+
+
 def test_powers_of_two_bound_the_maximum():
     m = np.array([0.0, 1.0, 0.75, 3.0, 1e-300, 2.0 ** 40])
     p = ozaki_emul.pow2_at_least(m)
@@ -36,6 +64,11 @@ def test_complex_product_converges_with_the_slice_count():
     errs = [np.linalg.norm(ozaki_emul.complex_product(a, b, ns) - ref) / np.linalg.norm(ref) for ns in (2, 3, 4)]
     assert errs[0] < 1e-3 and errs[1] < 1e-5 and errs[2] < 1e-7
     assert errs[0] > errs[1] > errs[2]
+    # base-256 digits: one bit more per slice, so each count is several times closer
+    e8 = [np.linalg.norm(ozaki_emul.complex_product(a, b, ns, bits=8) - ref) / np.linalg.norm(ref)
+          for ns in (2, 3, 4)]
+    assert e8[0] > e8[1] > e8[2]
+    assert all(e8[i] < errs[i] / 3 for i in range(3))
 
 
 def test_chi0_emulation_matches_the_direct_sum():
