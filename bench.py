@@ -37,8 +37,9 @@ METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err 
 # DRAM bytes (read + write) of one split-precision Sigma_c task launch
 # (N=600, 40 x 400 states, 25 imaginary slots + real-axis pole columns),
 # measured with ncu on that launch, per kernel of the path.
-# split-i8: the 4-slice launch, the count the automatic choice makes on this workload.
-SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": 1.911e9}
+# split-i8: the 3-slice launch (base-256 digits), the count the automatic choice makes on
+# this workload: both launches of the task (full row tiles 1.255e9 B, paired last row tile 0.085e9 B).
+SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": 1.340e9}
 
 
 def load_peaks():
@@ -506,6 +507,14 @@ def main():
         e2e = run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=True)
         release_pinned(torch)
         e2e["full_w_records"] = {k: full[k] for k in ("value", "ms_per_step", "h2d_bytes_per_step")}
+        # the copy bound of the step: its host -> device bytes at this box's pinned copy rate
+        gbs = measure_h2d_gbs()
+        e2e["h2d_pinned_gbs"] = round(gbs, 2)
+        e2e["h2d_bound_ms"] = round(e2e["h2d_bytes_per_step"] / (gbs * 1e9) * 1e3, 1)
+        e2e["full_w_records"]["h2d_bound_ms"] = round(full["h2d_bytes_per_step"] / (gbs * 1e9) * 1e3, 1)
+        log(f"e2e: {e2e['ms_per_step']} ms/step (keepwv), copy bound {e2e['h2d_bound_ms']} ms at {gbs:.1f} GB/s "
+            f"pinned host -> device; full records {full['ms_per_step']} ms, bound "
+            f"{e2e['full_w_records']['h2d_bound_ms']} ms")
     sur = None
     if not args.no_surrogate:
         lib.set_autotune(0, None)          # no tuning trials inside the study's timed calls
@@ -759,6 +768,25 @@ def measure_int8_peak():
     sus = reps * 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
     del a, b
     return {"burst_tops": round(best, 1), "sustained_tops": round(sus, 1), "reps": reps}
+
+
+def measure_h2d_gbs():
+    """Pinned host -> device copy rate of this box (1 GiB, cudaMemcpyAsync through torch,
+    best of 5): the bound of the end-to-end step's input copies (a measurement only)."""
+    import torch
+    n = 1 << 30
+    h = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(n, dtype=torch.uint8, device="cuda")
+    d.copy_(h, non_blocking=True)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); d.copy_(h, non_blocking=True); e1.record(); torch.cuda.synchronize()
+        best = max(best, n / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del h, d
+    release_pinned(torch)
+    return best
 
 
 def measure_fp64_peak():
