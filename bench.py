@@ -852,16 +852,12 @@ def run_e2e(lib, torch, cfg_chi, zc, s, args, flops, ws, dist, keepwv=True):
                            cfg_chi["eocc_h"], cfg_chi["eun_h"], zc_np, host=True)
 
     def step():
-        # keepwv: Sigma_c first, so its first task's inputs (0.3 GB) reach the device in a few ms and
-        # chi0's 3.75 GB of pair columns travel under the Sigma_c kernels (534 vs 544 ms); with full
-        # records the copies are the bound and chi0 first overlaps them better (673 vs 731 ms)
+        # chi0 first: the step is bound by its host -> device copies (the device work is shorter),
+        # so chi0's 67 ms of kernels run under the Sigma_c copies instead of after the last copy
         for d in host["tasks"]:
             d["zsec"][:] = 0
-        if not keepwv:
-            chi0()
+        chi0()
         run_sigc(lib, s, host=host)
-        if keepwv:
-            chi0()
         lib.synchronize()
 
     lib.set_host_async(True)

@@ -22,8 +22,11 @@ from tests.golden.make_golden import sigc_window
 
 pytestmark = pytest.mark.gpu
 HARTREE_MEV = 27211.386245988
-# gate on the relative Frobenius error against the FP64 oracle, per slice count
+# gate on the relative Frobenius error against the FP64 oracle, per slice count: chi0 (base-128
+# digits) and the Sigma_c kernel (base-256 digits; also the zmel M -> E product), the latter
+# about 5x above the measured 6.8e-5 / 3.2e-7 / 1.6e-9
 GATE = {2: 5e-3, 3: 2e-5, 4: 2e-7}
+GATE8 = {2: 3e-4, 3: 2e-6, 4: 1e-8}
 EXACT = 1e-12      # against the emulation of the same scheme
 
 
@@ -58,7 +61,7 @@ def test_sigc_i8_matches_emulation_and_oracle(i8, ns, ngb):
     print(f"sigc i8x{ns} ngb={ngb}: vs emulation {e_emu:.2e}, vs FP64 oracle {e_ref:.2e} "
           f"(emulation vs oracle {rel_fro(emu, ref):.2e}), max QP shift {dqp:.3e} meV")
     assert e_emu < EXACT
-    assert e_ref < GATE[ns]
+    assert e_ref < GATE8[ns]
 
 
 @pytest.mark.parametrize("ngb", [129, 160, 161])
@@ -105,7 +108,7 @@ def test_sigc_i8_golden_case_vs_oracle(i8, keepwv):
     err = rel_fro(got, ref)
     dqp = np.max(np.abs(np.real(np.diag(got) - np.diag(ref)))) * HARTREE_MEV
     print(f"sigc i8x3 golden keepwv={keepwv}: rel err {err:.2e}, max QP shift {dqp:.3e} meV")
-    assert err < GATE[3]
+    assert err < GATE8[3]
     assert dqp < 1.0
 
 
@@ -234,4 +237,4 @@ def test_zmel_m2e_i8_matches_emulation(i8, ns, conj):
     e_emu, e_ref = rel_fro(got, emu), rel_fro(got, ref)
     print(f"zmel m2e i8x{ns} conj={conj}: vs emulation {e_emu:.2e}, vs FP64 {e_ref:.2e}")
     assert e_emu < EXACT
-    assert e_ref < GATE[ns]
+    assert e_ref < GATE8[ns]
