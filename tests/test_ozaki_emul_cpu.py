@@ -79,3 +79,32 @@ def test_chi0_emulation_matches_the_direct_sum():
     ref = np.stack([(np.conj(z) * w[j]) @ z.T for j in range(3)], axis=2)
     got = ozaki_emul.chi0_dense(z, w, 4)
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-6
+
+
+def test_base256_product_equals_exact_integer_sum_of_the_kept_pairs():
+    """The emulated base-256 product against the same sum formed in exact
+    integers: (mu_m nu_n / U^2) sum_k sum_{p + q <= ns - 1} A_p B_q 256^(2 (ns - 1) - p - q),
+    with the A' rows [Re a, -Im a] and [Im a, Re a] sliced value by value."""
+    from fractions import Fraction
+    rng = np.random.default_rng(11)
+    a = rng.standard_normal((3, 7)) + 1j * rng.standard_normal((3, 7))
+    b = rng.standard_normal((7, 2)) + 1j * rng.standard_normal((7, 2))
+    for ns in (2, 3):
+        got = ozaki_emul.complex_product(a, b, ns, bits=8)
+        mu = ozaki_emul.max_scale(np.maximum(np.abs(a.real), np.abs(a.imag)).max(axis=1))
+        nu = ozaki_emul.max_scale(np.maximum(np.abs(b.real), np.abs(b.imag)).max(axis=0))
+        u = int(ozaki_emul.unit(ns, 8))
+        sl = {name: ozaki_emul.slices(x, sc, ns, bits=8) for name, x, sc in
+              (("ar", a.real, mu[:, None]), ("ai", a.imag, mu[:, None]), ("an", -a.imag, mu[:, None]),
+               ("br", b.real, nu[None, :]), ("bi", b.imag, nu[None, :]))}
+
+        def level_sum(x, y, m, n):
+            return sum(int(sl[x][p][m, k]) * int(sl[y][q][k, n]) * 256 ** (2 * (ns - 1) - p - q)
+                       for k in range(7) for p in range(ns) for q in range(ns - p))
+        for m in range(3):
+            for n in range(2):
+                f = Fraction(float(mu[m])) * Fraction(float(nu[n])) / (u * u)
+                re = f * (level_sum("ar", "br", m, n) + level_sum("an", "bi", m, n))
+                im = f * (level_sum("ai", "br", m, n) + level_sum("ar", "bi", m, n))
+                assert abs(got[m, n].real - float(re)) <= 1e-14 * abs(float(re)) + 1e-300
+                assert abs(got[m, n].imag - float(im)) <= 1e-14 * abs(float(im)) + 1e-300
