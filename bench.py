@@ -466,7 +466,7 @@ def main():
     achieved = (dom_flops * args.steps / max(k_n, 1)) / (per_launch_ms * 1e-3) / 1e12 if k_n else None
     fp64_peak = measure_fp64_peak()
     i8_peak = None
-    slices_used = chosen_slices(lib, args.slices) if prec == "split-i8" else None
+    slices_used = chosen_slices(lib, args.slices, (f"={N} ", f"niw={niw}")) if prec == "split-i8" else None
     if prec == "split-i8":
         i8_peak = measure_int8_peak()
         ns_sig = slices_used["sigc"]
@@ -691,7 +691,7 @@ def c4_study(lib, torch, log, modes, prec, nk_timed=16):
            "sigc_rel_err_vs_fp64_chain": rel(a["zsec"], b["zsec"]),
            "qp_err_mev_max_chain": qp, "qp_gate_1mev_met": qp <= 1.0,
            "oracle_chi0_k0_2iw_rel_err": oracle_err, "oracle_frequencies": [int(i) for i in sel],
-           "slices": chosen_slices(lib, modes[prec][1]) if prec == "split-i8" else None}
+           "slices": chosen_slices(lib, modes[prec][1], (f"={N} ",)) if prec == "split-i8" else None}
     del out, zs
     torch.cuda.empty_cache()
     return res
@@ -731,17 +731,21 @@ def mean_d(rows, k):
             "dominant_block": float(np.mean([r[k]["w_rel_block"] for r in rows]))}
 
 
-def chosen_slices(lib, requested):
+def chosen_slices(lib, requested, match=()):
     """int8 slices per operand of the chi0 and Sigma_c contractions: the requested
-    count, or the automatic choices the library recorded for this workload."""
+    count, or the automatic choices the library recorded for the shapes whose keys hold
+    every string of match (e.g. "=600 " for npr / ngb = 600, "niw=24").  A chi0 shape with
+    no record ran only accumulating calls, which take 3 slices when no choice was made."""
     if requested:
         return {"chi0": requested, "sigc": requested, "products": {"chi0": requested * (requested + 1) // 2,
                                                                    "sigc": requested * (requested + 1) // 2}}
     rep = lib.autotune_report()
-    pick = lambda pre: max((v for k, v in rep.items() if k.startswith(pre) and "err@" not in k), default=4)
-    ns = {"chi0": pick("chi0_i8 slices"), "sigc": pick("sigc_i8 slices")}
+    mine = lambda k: all(m in k for m in match)
+    pick = lambda pre, dflt: max((v for k, v in rep.items() if k.startswith(pre) and "err@" not in k and mine(k)),
+                                 default=dflt)
+    ns = {"chi0": pick("chi0_i8 slices", 3), "sigc": pick("sigc_i8 slices", 4)}
     ns["products"] = {k: v * (v + 1) // 2 for k, v in list(ns.items())}
-    ns["estimates"] = {k: v for k, v in rep.items() if "err@" in k}
+    ns["estimates"] = {k: v for k, v in rep.items() if "err@" in k and mine(k)}
     return ns
 
 
