@@ -89,6 +89,30 @@ struct Cfg {
   static_assert(NS * BN <= static_cast<int>(TMEM8), "one TMEM accumulator per level");
 };
 
+// The Sigma_c kernel's shared memory: NBUF chunk buffers (NS A' slices and NS B slices of one
+// 64-byte K chunk each), grouped into NST stages of CPS consecutive chunks.  A stage is one
+// full/empty barrier pair: the producer fills its CPS chunks under one expected byte count and the
+// MMA thread waits for it and releases it once, so the fixed cost of a stage (barrier test or
+// wait, commit, TMA bookkeeping) is paid once per CPS chunks.  Two chunks a stage up to 3 slices
+// (3 stages of 64 KB at 2, 2 stages of 96 KB at 3), one at 4 slices (3 stages of 64 KB).
+template <int NS>
+struct SegCfg {
+  static constexpr int CPS = NS <= 3 ? 2 : 1;
+  static constexpr int CHUNK = NS * (SLA8 + SLB8);
+  static constexpr int NBUF = STAGE_BUDGET / CHUNK / CPS * CPS;   // 6, 4, 3 chunk buffers for NS = 2, 3, 4
+  static constexpr int NST = NBUF / CPS;                          // 3, 2, 3 stages
+  static constexpr int OFF_A = 0;                                 // [NBUF][NS] A' slices
+  static constexpr int OFF_B = OFF_A + NBUF * NS * SLA8;          // [NBUF][NS] B slices
+  static constexpr int OFF_W = OFF_B + NBUF * NS * SLB8;          // drain column factors [16][2][32]
+  static constexpr int OFF_BAR = OFF_W + NDW * 64 * 8;
+  static constexpr int NBAR = 2 * NST + 3;                        // full, empty [NST]; accfull, accempty, done
+  static constexpr int OFF_MISC = OFF_BAR + NBAR * 8;
+  static constexpr int SMEM = OFF_MISC + 64 + 1024;
+  static_assert(NST >= 2, "a ring of at least two stages");
+  static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+  static_assert(NBUF * NS * SLA8 >= 8 * 32 * 32 * 8, "the paired tail's cross-half sums fit in the A' buffers");
+};
+
 // kind::i8, A = B = signed 8-bit, D = S32, both K-major, M = 128, N = BN
 constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
                               (static_cast<uint32_t>(BM >> 4) << 24);
@@ -285,8 +309,8 @@ template <int NS, bool PAIRED>
 __global__ void __launch_bounds__(THREADS, 1)
     oz_seg_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                   const __grid_constant__ CUtensorMap mapT, const SegParams p) {
-  using L = Cfg<NS>;
-  constexpr int NST = L::NST;
+  using L = SegCfg<NS>;
+  constexpr int NST = L::NST, CPS = L::CPS;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* sm = align1024(smem_raw);
   unsigned char* sA = sm + L::OFF_A;
@@ -294,8 +318,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   double* sW = reinterpret_cast<double*>(sm + L::OFF_W);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::OFF_BAR);
   uint64_t* full = bar;                  // [NST] TMA -> MMA
-  uint64_t* empty = bar + 2 * NST;       // [NST] MMA -> TMA
-  uint64_t* accfull = bar + 3 * NST;     // MMA -> drain
+  uint64_t* empty = bar + NST;           // [NST] MMA -> TMA
+  uint64_t* accfull = bar + 2 * NST;     // MMA -> drain
   uint64_t* accempty = accfull + 1;      // drain -> MMA
   uint64_t* done = accempty + 1;         // every MMA of the CTA retired
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::OFF_MISC);
@@ -333,7 +357,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (warp == 0 && lane == 0) {
       // ---------------- TMA producer: NS slices of the segment's A' tile and of the B tile
       constexpr uint32_t bytes = NS * (SLA8 + SLB8);
-      int issued = 0, sg = 0, cin = 0, st = 0, ph = 0;
+      int issued = 0, sg = 0, cin = 0, st = 0, ph = 0, sub = 0;   // issued: stages begun
       // this step's slot (paired: the slots of segments 2 sg and 2 sg + 1, the second repeated when absent)
       auto step_slots = [&](int g, int& s0, int& s1) {
         if (!paired) { s0 = s1 = p.seg_slot[seg0 + g]; return; }
@@ -343,13 +367,16 @@ __global__ void __launch_bounds__(THREADS, 1)
       int slot = 0, slot1 = 0;
       step_slots(0, slot, slot1);
       for (int c = 0; c < nchunk; ++c) {
-        if (c >= NST && !mbar_wait(&empty[st], ph ^ 1, abort_flag)) break;
-        issued = c + 1;
-        mbar_expect_tx(&full[st], bytes);
+        if (sub == 0) {                               // a new stage: its CPS chunks (fewer at the end)
+          if (issued >= NST && !mbar_wait(&empty[st], ph ^ 1, abort_flag)) break;
+          ++issued;
+          mbar_expect_tx(&full[st], bytes * static_cast<uint32_t>(min(CPS, nchunk - c)));
+        }
+        const int buf = st * CPS + sub;
         const int x = cin * K8;
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
-          unsigned char* dA = sA + (st * NS + q) * SLA8;
+          unsigned char* dA = sA + (buf * NS + q) * SLA8;
           if constexpr (PAIRED) {                     // rows 0-31 / 32-63 re, 64-95 / 96-127 im
             tma_load_4d(dA, &mapT, &full[st], x, 0, 0, q * p.nslot + slot);
             tma_load_4d(dA + SLA8 / 4, &mapT, &full[st], x, 0, 0, q * p.nslot + slot1);
@@ -358,36 +385,49 @@ __global__ void __launch_bounds__(THREADS, 1)
           } else {
             tma_load_4d(dA, &mapA, &full[st], x, 0, 0, (q * p.nslot + slot) * p.T + mt);
           }
-          tma_load_3d(sB + (st * NS + q) * SLB8, &mapB, &full[st], x, nt * BN, q);
+          tma_load_3d(sB + (buf * NS + q) * SLB8, &mapB, &full[st], x, nt * BN, q);
         }
         if (++cin == p.cps) {
           cin = 0;
           if (++sg < nstep) step_slots(sg, slot, slot1);
         }
-        if (++st == NST) { st = 0; ph ^= 1; }
+        if (++sub == CPS) {
+          sub = 0;
+          if (++st == NST) { st = 0; ph ^= 1; }
+        }
       }
-      for (int c = max(0, issued - NST); c < issued; ++c) mbar_drain(&full[c % NST], (c / NST) & 1);
+      for (int g = max(0, issued - NST); g < issued; ++g) mbar_drain(&full[g % NST], (g / NST) & 1);
     } else if (warp == 1 && lane == 0) {
       // ---------------- MMA issuer: NS level accumulators, one accumulation period per segment
       const uint64_t dA0 = sw64_desc(smem_u32(sA)), dB0 = sw64_desc(smem_u32(sB));
-      int seg = 0, cin = 0, st = 0, ph = 0;
-      uint32_t ready = 0;                            // the chunk's stage was seen full by the last test
+      int seg = 0, cin = 0, st = 0, ph = 0, sub = 0;
+      uint32_t ready = 0;                            // the next stage was seen full by the last test
       for (int c = 0; c < nchunk && !*abort_flag; ++c) {
         const bool first = cin == 0, last = cin == p.cps - 1;
+        const bool stage_end = sub == CPS - 1 || c + 1 == nchunk;
         if (first && seg >= 1 && !mbar_wait(accempty, (seg - 1) & 1, abort_flag)) break;
-        if (!ready && !mbar_wait(&full[st], ph, abort_flag)) break;
+        if (sub == 0 && !ready && !mbar_wait(&full[st], ph, abort_flag)) break;
         tc_fence_after();
-        // the next chunk's stage is tested during this chunk's last MMA
-        const uint32_t nbar = c + 1 < nchunk ? smem_u32(&full[st + 1 == NST ? 0 : st + 1]) : 0u;
+        // the next stage is tested during the last MMA of this stage's last chunk
+        const uint32_t nbar = stage_end && c + 1 < nchunk ? smem_u32(&full[st + 1 == NST ? 0 : st + 1]) : 0u;
         const uint32_t npar = st + 1 == NST ? (ph ^ 1) : ph;
+        const int buf = st * CPS + sub;
 #pragma unroll
-        for (int kk = 0; kk < K8 / 32; ++kk)          // 32 int8 = 32 B along K = 2 descriptor units
-          ready = slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((st * NS * SLA8) >> 4) + 2 * kk,
-                                     dB0 + static_cast<uint32_t>((st * NS * SLB8) >> 4) + 2 * kk, SLA8 >> 4,
-                                     SLB8 >> 4, first && kk == 0, kk == K8 / 32 - 1 ? nbar : 0u, npar);
-        umma_commit(&empty[st]);
+        for (int kk = 0; kk < K8 / 32; ++kk) {        // 32 int8 = 32 B along K = 2 descriptor units
+          const uint32_t r = slice_products<NS>(tmem, dA0 + static_cast<uint32_t>((buf * NS * SLA8) >> 4) + 2 * kk,
+                                                dB0 + static_cast<uint32_t>((buf * NS * SLB8) >> 4) + 2 * kk,
+                                                SLA8 >> 4, SLB8 >> 4, first && kk == 0,
+                                                kk == K8 / 32 - 1 ? nbar : 0u, npar);
+          if (kk == K8 / 32 - 1) ready = nbar ? r : 0u;
+        }
         if (last) umma_commit(accfull);
-        if (++st == NST) { st = 0; ph ^= 1; }
+        if (stage_end) {
+          umma_commit(&empty[st]);
+          sub = 0;
+          if (++st == NST) { st = 0; ph ^= 1; }
+        } else {
+          ++sub;
+        }
         if (++cin == p.cps) { cin = 0; ++seg; }
       }
       umma_commit(done);
@@ -1030,10 +1070,10 @@ template <int NS, bool PAIRED>
 static int launch_seg(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mt, const SegParams& p,
                       dim3 grid, cudaStream_t s) {
   static uint64_t attr = 0;                             // one bit per device
-  int rc = smem_limit_once(reinterpret_cast<const void*>(oz_seg_kernel<NS, PAIRED>), Cfg<NS>::SMEM, attr);
+  int rc = smem_limit_once(reinterpret_cast<const void*>(oz_seg_kernel<NS, PAIRED>), SegCfg<NS>::SMEM, attr);
   if (rc) return rc;
   const int pi = prof_begin("sigc_seg_tc", s);
-  oz_seg_kernel<NS, PAIRED><<<grid, THREADS, Cfg<NS>::SMEM, s>>>(ma, mb, mt, p);
+  oz_seg_kernel<NS, PAIRED><<<grid, THREADS, SegCfg<NS>::SMEM, s>>>(ma, mb, mt, p);
   prof_end(pi, s);
   count_launch();
   QSGW_LAUNCH_CHECK("oz_seg_kernel");
