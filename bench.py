@@ -38,8 +38,8 @@ METRIC = "chi0+Sigma_c time & GFLOP/s on 1 B200, mixed vs FP64 plain, at QP err 
 # (N=600, 40 x 400 states, 25 imaginary slots + real-axis pole columns),
 # measured with ncu on that launch, per kernel of the path.
 # split-i8: the 3-slice launch (base-256 digits), the count the automatic choice makes on
-# this workload: both launches of the task (full row tiles 1.255e9 B, paired last row tile 0.085e9 B).
-SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": 1.340e9}
+# this workload: both launches of the task (full row tiles 1.284e9 B, paired last row tile 0.087e9 B).
+SIGC_TC_TRAFFIC = {"split-f16": 3.315e9, "split-i8": 1.371e9}
 
 
 def load_peaks():
