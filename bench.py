@@ -425,7 +425,7 @@ def main():
     # ---- headline run: one step recorded as a CUDA graph and replayed (eager timing beside it)
     ms_eager = None
     if not args.no_graph:
-        ms_eager, _, _, _ = timed(prec, max(1, min(args.steps, 2)), 1, False)
+        ms_eager, _, _, _ = timed(prec, max(1, min(args.steps, 3)), args.warmup, False)
     ms, kt, launches, clocks = timed(prec, args.steps, args.warmup, True, graph=not args.no_graph)
     value = ws * flops / (ms * 1e-3) / 1e9
     chi_main = chi.clone()
